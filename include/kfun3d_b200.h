@@ -1,0 +1,210 @@
+/*
+ * kfun3d_b200: B200 (sm_100a) implementation of KFUN3D's pseudo-transient
+ * Newton-Krylov solve, exported as a C ABI.
+ *
+ * Part 1 re-exports the reference's own entry points with their exact
+ * signatures, so the reference's C host driver (src/main.c, src/mesh.c and the
+ * set-up files) links against libkfun3d_b200.so in place of src/flux.c,
+ * src/timestep.c, src/fill.c, src/ilu.c, src/sptrsv.c, src/forces.c,
+ * src/utils.c, src/kernel.c and the matrix/ C++ files.  Every call runs on the GPU;
+ * there is no CPU fallback.  Host arrays passed in are copied to device
+ * mirrors kept per GEOMETRY (geometry uploaded once, on first use) and results
+ * are copied back.  Kernel() runs the whole solve on the device.
+ *
+ * Part 2 adds what the fixed ABI cannot express: status, physics and solver
+ * settings, a native mesh loader/generator, a parameterised solve with
+ * per-step history, and device-resident timing hooks.
+ *
+ * Failures: the reference's entry points return void and assert.  Here every
+ * call records a status (kfun3d_gpu_last_status); by default a CUDA error
+ * also aborts the process, as the reference's asserts do.
+ */
+#ifndef KFUN3D_B200_H
+#define KFUN3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "kfun3d_geometry.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ===================================================================== */
+/* Part 1: the reference's entry points                                  */
+/* ===================================================================== */
+
+/* inc/core_kernel.h:9 -> src/fill.c:881-917.  First-order 4x4-block Jacobian
+   at g->q->q with diagonal g->n->cdt, kept on the device behind g->matrix. */
+void ComputeA(GEOMETRY *g);
+
+/* inc/core_kernel.h:12 -> src/timestep.c:156-188.  Writes g->n->cdt. */
+void ComputeTimeStep(const double cfl, GEOMETRY *g);
+
+/* inc/core_kernel.h:15 -> src/flux.c:782-825.  Residual r[4N] of state q[4N];
+   also writes the least-squares gradients grad->x0/x1/x2 [4N]. */
+void ComputeFlux(const GEOMETRY *g, const double *q, GRADIENT *grad, double *r);
+
+/* inc/core_kernel.h:18 -> src/forces.c:101-120.  forces = {lift, drag, moment}. */
+void ComputeForces(const GEOMETRY *g, double *forces);
+
+/* inc/core_kernel.h:21 -> src/ilu.c:271-288 (matrix/ilu.cpp:49-138).
+   Block ILU(0) of the matrix in place, diagonal blocks stored inverted. */
+void ComputeNumericalILU(GEOMETRY *g);
+
+/* inc/core_kernel.h:22 -> src/sptrsv.c:86-105 (matrix/sptrsv.cpp:34-73).
+   x = (LU)^-1 b with the factor of ComputeNumericalILU. */
+void ComputeSparseTriangularSolve(const GEOMETRY *g, const double *b, double *x);
+
+/* inc/utils.h:18 -> src/utils.c:53-67 */
+double Compute2ndNorm(const size_t sz, const double *v);
+/* inc/utils.h:21 -> src/utils.c:69-87: y = a x + y */
+void ComputeAXPY(const size_t sz, const double a, const double *x, double *y);
+/* inc/utils.h:24 -> src/utils.c:89-107: w = a x + y */
+void ComputeNewAXPY(const size_t sz, const double a, const double *x, const double *y, double *w);
+/* inc/utils.h:27 -> src/utils.c:109-122: x /= |x|, returns |x| */
+double Normalize(const size_t sz, double *x);
+/* inc/utils.h:15 -> src/utils.c:5-51 (coloured printf used by src/bench.c) */
+void fun3d_printf(const uint32_t c, const char *format, ...);
+
+/* src/main.c:19 -> src/kernel.c:47-232.  The whole pseudo-transient solve on
+   the device with the reference's constants; updates g->q->q and prints the
+   reference's per-step report unless kfun3d_set_verbose(0). */
+void Kernel(GEOMETRY *g);
+
+/* matrix/wrapper.cpp:23-28.  Creates the opaque matrix handle stored in
+   g->matrix (block pattern of the edge graph plus the diagonal).  No device
+   memory is touched until the first kernel call. */
+void *CXX_Matrix_Init(const size_t nnodes, const size_t nedges, const unsigned int block_size,
+                      const unsigned int nthreads, const unsigned int *n0, const unsigned int *n1);
+/* matrix/wrapper.cpp:30-34 */
+void CXX_Matrix_Delete(void *ptr);
+/* matrix/wrapper.cpp:36-40.  The reference partitions with METIS for its
+   OpenMP threads; the device path does not use the partition, so this assigns
+   contiguous node ranges. */
+void CXX_METIS(const unsigned int nparts, unsigned int *parts, void *ptr);
+/* matrix/wrapper.cpp:13-21: big-endian walkers of the .msh reader */
+void CXX_Walk_Int(char *l, const char *h, const size_t sz, unsigned int *b);
+void CXX_Walk_Double(char *l, const char *h, const size_t sz, double *b);
+
+/* ===================================================================== */
+/* Part 2: extensions (no counterpart in the reference's ABI)            */
+/* ===================================================================== */
+
+enum kfun3d_status {
+  KFUN3D_OK = 0,
+  KFUN3D_ERR_CUDA = 1,        /* a CUDA call failed */
+  KFUN3D_ERR_NONFINITE = 2,   /* NaN or Inf in a residual or norm */
+  KFUN3D_ERR_PIVOT = 3,       /* zero or non-finite pivot block in ILU(0) */
+  KFUN3D_ERR_ARG = 4,         /* invalid argument or unsupported GEOMETRY */
+  KFUN3D_ERR_IO = 5,          /* mesh file error */
+  KFUN3D_ERR_NO_DEVICE = 6,   /* no CUDA device */
+  KFUN3D_ERR_DIVERGED = 7     /* linear or nonlinear solve failed */
+};
+
+/* Status of the most recent call (KFUN3D_OK or an error code) and its text. */
+int kfun3d_gpu_last_status(void);
+const char *kfun3d_gpu_last_error(void);
+void kfun3d_clear_status(void);
+/* 1 (default): a CUDA error aborts the process like the reference's asserts.
+   0: the error is only recorded. */
+void kfun3d_set_abort_on_error(int on);
+
+/* Angle of attack in degrees (inc/phy.h:8-9 hard-codes 3).  Free stream
+   U = cos(a / (180/pi)), V = sin(a / (180/pi)), W = 0, P = 1, beta = 15. */
+void kfun3d_set_aoa(double deg);
+double kfun3d_get_aoa(void);
+void kfun3d_get_freestream(double *u, double *v);
+
+/* Arithmetic of the device kernels.
+   KFUN3D_MODE_EXACT: the reference's operation order everywhere (no fused
+     multiply-add, per-node sums in edge order, reductions in index order);
+     results are bit-identical to the reference at one OpenMP thread.
+   KFUN3D_MODE_FAST: fused multiply-add, tree reductions, reciprocals
+     hoisted; results differ from the reference at rounding level. */
+enum { KFUN3D_MODE_EXACT = 0, KFUN3D_MODE_FAST = 1 };
+void kfun3d_set_mode(int mode);
+int kfun3d_get_mode(void);
+
+/* Preconditioner precision: 0 = FP64 (the reference), 1 = FP32 Jacobian
+   blocks, FP32 ILU(0) factors and FP32-block triangular solves. */
+void kfun3d_set_precision(int p);
+/* 1: residual reconstructed without gradients (first-order flux). */
+void kfun3d_set_first_order(int on);
+/* 0 silences Kernel()'s per-step report. */
+void kfun3d_set_verbose(int on);
+
+typedef struct {
+  int ts_max;          /* Newton steps (src/kernel.c:21: 15) */
+  double stop_ratio;   /* stop once round(|r0|/|r|) >= stop_ratio (kernel.c:22: 1e7) */
+  double gmres_rtol;   /* kernel.c:14: 0.01 */
+  int gmres_restart;   /* kernel.c:15: 30 (at most 30) */
+  int gmres_max_it;    /* kernel.c:17: 10000 */
+  double cfl_init;     /* kernel.c:19: 50 */
+  double cfl_max;      /* kernel.c:20: 1e5 */
+} kfun3d_solver_params;
+
+typedef struct {
+  int step;
+  int gmres_its;
+  double cfl;
+  double fnorm;        /* residual norm before this step's update */
+  double lift, drag, momn;
+  double seconds;      /* device time of the step */
+} kfun3d_step;
+
+/* Reference defaults (src/kernel.c:12-22). */
+void kfun3d_default_params(kfun3d_solver_params *p);
+
+/* Kernel() with parameters: solves from g->q->q (updated in place), records
+   up to max_hist steps, returns the number of steps taken or -1 on error. */
+int kfun3d_solve(GEOMETRY *g, const kfun3d_solver_params *p, kfun3d_step *hist, int max_hist);
+
+/* Native .msh loader: the GEOMETRY the reference's Setup builds at one
+   thread (same edge order, wall colouring and least-squares weights), with
+   the free-stream initial state of the current angle of attack. */
+GEOMETRY *kfun3d_setup_load(const char *path);
+void kfun3d_setup_free(GEOMETRY *g);
+void kfun3d_initial_guess(GEOMETRY *g);
+
+/* Synthetic Kuhn-box mesh writer: n^3 nodes on [0,1]^3, each hex split into
+   six tets, interior nodes jittered by U(+-jitter h), bottom face a slip wall
+   with a Gaussian bump height*exp(-r^2/(2 sigma^2))*(1-z), other faces far
+   field, optional seeded random node numbering.  Returns 0 on success. */
+typedef struct {
+  unsigned int n;
+  double bump_height;
+  double bump_sigma;
+  double jitter;
+  unsigned long long seed;
+  int permute;
+} kfun3d_mesh_spec;
+int kfun3d_mesh_generate(const char *path, const kfun3d_mesh_spec *spec);
+
+/* Device-resident timing: runs kernel family `which` reps times on the
+   device copy of g (state g->q->q uploaded once), returns the mean time of
+   one call in milliseconds measured with CUDA events on the solver's stream,
+   or a negative value on error.  which: 0 flux (gradient + edge flux +
+   boundary), 1 time step, 2 Jacobian fill, 3 ILU(0), 4 triangular solves,
+   5 one GMRES iteration at Arnoldi index 15 (J.v + solve + MGS). */
+double kfun3d_time_kernel(GEOMETRY *g, int which, int reps);
+
+/* Number of kernel launches the library issued since the last reset. */
+unsigned long long kfun3d_launch_count(void);
+void kfun3d_reset_launch_count(void);
+
+/* The device matrix behind g->matrix, for inspection: the block pattern of
+   matrix/init.cpp:7-74 (row pointers nnodes+1, sorted columns nnz) and the
+   4x4 row-major blocks (nnz*16, FP32 blocks widened) as left by the last
+   ComputeA (the Jacobian) or ComputeNumericalILU (the factor, diagonal blocks
+   inverted).  Returns nnz, or -1 on error; NULL outputs are skipped. */
+long kfun3d_matrix_read(const GEOMETRY *g, unsigned int *ia, unsigned int *ja, double *blocks);
+
+/* Release the device mirror of g (also done by CXX_Matrix_Delete). */
+void kfun3d_device_release(GEOMETRY *g);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KFUN3D_B200_H */

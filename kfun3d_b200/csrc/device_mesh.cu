@@ -1,0 +1,415 @@
+// kfun3d_b200: library state, the matrix handle, and the device mirror of a
+// GEOMETRY (built once per GEOMETRY, on its first kernel call).
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+
+#include "internal.h"
+
+// ----------------------------------------------------------------- settings and status
+
+namespace {
+std::atomic<int> g_status{KFUN3D_OK};
+std::string g_error;
+std::mutex g_mu;
+int g_abort = 1;
+double g_aoa = 3.0;
+int g_mode = KFUN3D_MODE_EXACT;
+int g_precision = 0;
+int g_first_order = 0;
+std::atomic<unsigned long long> g_launches{0};
+}  // namespace
+
+int g_kf_verbose = 1;
+
+void kf_set_error(int code, const char *msg)
+{
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_status = code;
+    g_error = msg ? msg : "";
+  }
+  if (code == KFUN3D_ERR_CUDA && g_abort) {
+    fprintf(stderr, "kfun3d_b200: %s\n", msg);
+    abort();
+  }
+}
+
+int kf_mode() { return g_mode; }
+int kf_precision() { return g_precision; }
+int kf_first_order() { return g_first_order; }
+void kf_count_launch(unsigned n) { g_launches += n; }
+
+extern "C" {
+
+int kfun3d_gpu_last_status(void) { return g_status; }
+const char *kfun3d_gpu_last_error(void) { return g_error.c_str(); }
+void kfun3d_clear_status(void)
+{
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_status = KFUN3D_OK;
+  g_error.clear();
+}
+void kfun3d_set_abort_on_error(int on) { g_abort = on; }
+void kfun3d_set_aoa(double deg) { g_aoa = deg; }
+double kfun3d_get_aoa(void) { return g_aoa; }
+// inc/phy.h:8-9
+void kfun3d_get_freestream(double *u, double *v)
+{
+  *u = cos(g_aoa / (180 / M_PI));
+  *v = sin(g_aoa / (180 / M_PI));
+}
+void kfun3d_set_mode(int mode) { g_mode = mode == KFUN3D_MODE_FAST ? KFUN3D_MODE_FAST : KFUN3D_MODE_EXACT; }
+int kfun3d_get_mode(void) { return g_mode; }
+void kfun3d_set_precision(int p) { g_precision = p ? 1 : 0; }
+void kfun3d_set_first_order(int on) { g_first_order = on ? 1 : 0; }
+void kfun3d_set_verbose(int on) { g_kf_verbose = on; }
+unsigned long long kfun3d_launch_count(void) { return g_launches; }
+void kfun3d_reset_launch_count(void) { g_launches = 0; }
+
+// src/utils.c:5-51
+void fun3d_printf(const uint32_t c, const char *format, ...)
+{
+  static const int codes[6] = {31, 32, 33, 34, 35, 36};
+  const int val = c < 6 ? codes[c] : 0;
+  va_list ap;
+  va_start(ap, format);
+  fprintf(stdout, "\x1b[%dm", val);
+  vfprintf(stdout, format, ap);
+  fprintf(stdout, "\x1b[0m");
+  va_end(ap);
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------------------- block pattern
+
+// matrix/init.cpp:7-74 (pattern), 194-274 (level sets) and the reference's
+// fill order (src/fill.c:496-511) for the persistent-L-slot rule.
+void kf_build_pattern(HostPattern &p, size_t N, size_t E, const unsigned int *n0, const unsigned int *n1)
+{
+  p.n = N;
+  p.ia.assign(N + 1, 0);
+  for (size_t e = 0; e < E; e++) { p.ia[n0[e] + 1]++; p.ia[n1[e] + 1]++; }
+  for (size_t i = 0; i < N; i++) p.ia[i + 1] += p.ia[i] + 1;
+  p.nnz = p.ia[N];
+  p.ja.assign(p.nnz, 0);
+  std::vector<uint32_t> fillp(N);
+  for (size_t i = 0; i < N; i++) { p.ja[p.ia[i]] = (uint32_t)i; fillp[i] = p.ia[i] + 1; }
+  for (size_t e = 0; e < E; e++) {
+    p.ja[fillp[n0[e]]++] = n1[e];
+    p.ja[fillp[n1[e]]++] = n0[e];
+  }
+  p.diag.assign(N, 0);
+  p.lpos.assign(N + 1, 0);
+  for (size_t i = 0; i < N; i++) {
+    std::sort(p.ja.begin() + p.ia[i], p.ja.begin() + p.ia[i + 1]);
+    for (uint32_t j = p.ia[i]; j < p.ia[i + 1]; j++)
+      if (p.ja[j] == i) { p.diag[i] = j; break; }
+    p.lpos[i + 1] = p.lpos[i] + (p.diag[i] - p.ia[i]);
+  }
+  auto find = [&](uint32_t row, uint32_t col) -> uint32_t {
+    auto b = p.ja.begin() + p.ia[row], e = p.ja.begin() + p.ia[row + 1];
+    auto it = std::lower_bound(b, e, col);
+    return (it != e && *it == col) ? (uint32_t)(it - p.ja.begin()) : 0xffffffffu;
+  };
+  p.tblk.assign(p.nnz, 0);
+  for (size_t i = 0; i < N; i++)
+    for (uint32_t j = p.ia[i]; j < p.ia[i + 1]; j++) p.tblk[j] = find(p.ja[j], (uint32_t)i);
+  p.last_lower.assign(N, 0xffffffffu);
+  for (size_t e = 0; e < E; e++) {
+    const uint32_t a = n0[e], b = n1[e];
+    if (b < a) p.last_lower[a] = b;
+    if (a < b) p.last_lower[b] = a;
+  }
+  for (size_t i = 0; i < N; i++)
+    if (p.last_lower[i] != 0xffffffffu) p.last_lower[i] = find((uint32_t)i, p.last_lower[i]);
+  // level sets: depth(i) = 1 + max depth over the lower (resp. upper) columns
+  std::vector<uint32_t> depth(N);
+  auto levels = [&](bool lower, std::vector<uint32_t> &rows, std::vector<uint32_t> &ptr) {
+    uint32_t nlev = 1;
+    for (size_t s = 0; s < N; s++) {
+      const size_t i = lower ? s : N - 1 - s;
+      uint32_t d = 1;
+      const uint32_t jb = lower ? p.ia[i] : p.diag[i] + 1, je = lower ? p.diag[i] : p.ia[i + 1];
+      for (uint32_t j = jb; j < je; j++) d = std::max(d, depth[p.ja[j]] + 1);
+      depth[i] = d;
+      nlev = std::max(nlev, d);
+    }
+    ptr.assign(nlev + 1, 0);
+    for (size_t i = 0; i < N; i++) ptr[depth[i]]++;
+    for (uint32_t l = 0; l < nlev; l++) ptr[l + 1] += ptr[l];
+    rows.assign(N, 0);
+    std::vector<uint32_t> top(ptr.begin(), ptr.end() - 1);
+    for (size_t i = 0; i < N; i++) rows[top[depth[i] - 1]++] = (uint32_t)i;
+  };
+  levels(true, p.lev_l, p.lev_l_ptr);
+  levels(false, p.lev_u, p.lev_u_ptr);
+}
+
+// ----------------------------------------------------------------- matrix handle ABI
+
+extern "C" void *CXX_Matrix_Init(const size_t nnodes, const size_t nedges, const unsigned int block_size,
+                                 const unsigned int nthreads, const unsigned int *n0, const unsigned int *n1)
+{
+  (void)nthreads;
+  if (block_size != 4) {
+    kf_set_error(KFUN3D_ERR_ARG, "block size must be 4");
+    return nullptr;
+  }
+  MatrixHandle *h = new MatrixHandle();
+  kf_build_pattern(h->pat, nnodes, nedges, n0, n1);
+  return h;
+}
+
+static void release_device(MatrixHandle *h);
+
+extern "C" void CXX_Matrix_Delete(void *ptr)
+{
+  MatrixHandle *h = (MatrixHandle *)ptr;
+  if (!h || h->magic != 0x4B463344u) return;
+  release_device(h);
+  h->magic = 0;
+  delete h;
+}
+
+extern "C" void CXX_METIS(const unsigned int nparts, unsigned int *parts, void *ptr)
+{
+  MatrixHandle *h = (MatrixHandle *)ptr;
+  if (!h || nparts == 0) return;
+  const size_t N = h->pat.n;
+  for (size_t i = 0; i < N; i++) parts[i] = (unsigned int)((i * nparts) / (N ? N : 1));
+}
+
+MatrixHandle *kf_handle(const GEOMETRY *g)
+{
+  if (!g || !g->matrix) return nullptr;
+  MatrixHandle *h = (MatrixHandle *)g->matrix;
+  return h->magic == 0x4B463344u ? h : nullptr;
+}
+
+// ----------------------------------------------------------------- device mirror
+
+#define KF_CUDA(call)                                                             \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      std::string m_ = std::string(#call) + ": " + cudaGetErrorString(e_);       \
+      kf_set_error(KFUN3D_ERR_CUDA, m_.c_str());                                  \
+      release_device(h);                                                          \
+      return nullptr;                                                             \
+    }                                                                             \
+  } while (0)
+
+template <class T> static cudaError_t upload(T **dst, const T *src, size_t n)
+{
+  cudaError_t e = cudaMalloc((void **)dst, std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess || n == 0) return e;
+  return cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+static void release_device(MatrixHandle *h)
+{
+  DevMesh *m = h->dev;
+  if (!m) return;
+  void *ptrs[] = {m->col, m->egeo, m->xyz, m->inc_ptr, m->inc_oth, m->inc_edge, m->inc_blk, m->inc_w, m->wf_nodes,
+                  m->wf_n, m->s_n, m->f_n, m->bnd_of, m->bnd_node, m->bnd_ptr, m->bnd_ent, m->ia, m->ja,
+                  m->diag, m->tblk, m->lpos, m->last_lower, m->lev_l, m->lev_u, m->A, m->lslot, m->dinv,
+                  m->Af, m->dinvf, m->q, m->r, m->gx, m->gy, m->gz, m->cdt, m->w, m->t, m->x, m->rhs, m->V,
+                  m->red, m->scal, m->forces, m->dscr, m->status};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (m->h_scal) cudaFreeHost(m->h_scal);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+  h->dev = nullptr;
+}
+
+extern "C" void kfun3d_device_release(GEOMETRY *g)
+{
+  MatrixHandle *h = kf_handle(g);
+  if (h) release_device(h);
+}
+
+DevMesh *kf_device(const GEOMETRY *g)
+{
+  MatrixHandle *h = kf_handle(g);
+  if (!h) {
+    kf_set_error(KFUN3D_ERR_ARG, "GEOMETRY::matrix is not a kfun3d_b200 handle (create it with CXX_Matrix_Init)");
+    return nullptr;
+  }
+  if (h->dev) return h->dev;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    kf_set_error(KFUN3D_ERR_NO_DEVICE, "no CUDA device");
+    return nullptr;
+  }
+  if (g->s && g->s->sz > 1) {
+    kf_set_error(KFUN3D_ERR_ARG, "GEOMETRY built for more than one OpenMP thread: set it up with one thread");
+    return nullptr;
+  }
+  const HostPattern &p = h->pat;
+  const uint32_t N = (uint32_t)g->n->sz, E = (uint32_t)g->e->sz;
+  if (p.n != N) {
+    kf_set_error(KFUN3D_ERR_ARG, "matrix handle does not match the GEOMETRY");
+    return nullptr;
+  }
+  const unsigned int *n0 = g->e->eptr->n0, *n1 = g->e->eptr->n1;
+
+  DevMesh *m = new DevMesh();
+  h->dev = m;
+  h->owner = g;
+  KF_CUDA(cudaGetDevice(&m->device));
+  KF_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+  m->N = N;
+  m->E = E;
+  m->Ns = (uint32_t)g->b->s->sz;
+  m->Nf = (uint32_t)g->b->f->sz;
+  m->F = (uint32_t)g->b->fc->sz;
+  m->ncol = (uint32_t)g->t->sz;
+  m->nnz = (uint32_t)p.nnz;
+  m->nlower = p.lpos[N];
+
+  // edge geometry and node coordinates
+  {
+    std::vector<double4> eg(E), xyz(N);
+    for (uint32_t e = 0; e < E; e++)
+      eg[e] = make_double4(g->e->xyzn->x0[e], g->e->xyzn->x1[e], g->e->xyzn->x2[e], g->e->xyzn->x3[e]);
+    for (uint32_t i = 0; i < N; i++)
+      xyz[i] = make_double4(g->n->xyz->x0[i], g->n->xyz->x1[i], g->n->xyz->x2[i], 0.0);
+    KF_CUDA(upload(&m->egeo, eg.data(), E));
+    KF_CUDA(upload(&m->xyz, xyz.data(), N));
+  }
+  // node incidence in edge order, with the least-squares terms seen from the
+  // node (w0 at n0, w1 at n1) and the block of (node, other)
+  {
+    std::vector<uint32_t> ptr(N + 1, 0);
+    for (uint32_t e = 0; e < E; e++) { ptr[n0[e] + 1]++; ptr[n1[e] + 1]++; }
+    for (uint32_t i = 0; i < N; i++) ptr[i + 1] += ptr[i];
+    const size_t ninc = 2 * (size_t)E;
+    std::vector<uint32_t> oth(ninc), edg(ninc), blk(ninc), pos(ptr.begin(), ptr.end() - 1);
+    std::vector<double> w(3 * ninc);
+    const double *w0[3] = {g->e->w->w0->x0, g->e->w->w0->x1, g->e->w->w0->x2};
+    const double *w1[3] = {g->e->w->w1->x0, g->e->w->w1->x1, g->e->w->w1->x2};
+    auto find = [&](uint32_t row, uint32_t col) -> uint32_t {
+      auto b = p.ja.begin() + p.ia[row], en = p.ja.begin() + p.ia[row + 1];
+      return (uint32_t)(std::lower_bound(b, en, col) - p.ja.begin());
+    };
+    for (uint32_t e = 0; e < E; e++) {
+      const uint32_t a = n0[e], b = n1[e];
+      uint32_t k = pos[a]++;
+      oth[k] = b; edg[k] = e; blk[k] = find(a, b);
+      for (int c = 0; c < 3; c++) w[c * ninc + k] = w0[c][e];
+      k = pos[b]++;
+      oth[k] = a; edg[k] = e | 0x80000000u; blk[k] = find(b, a);
+      for (int c = 0; c < 3; c++) w[c * ninc + k] = w1[c][e];
+    }
+    KF_CUDA(upload(&m->inc_ptr, ptr.data(), N + 1));
+    KF_CUDA(upload(&m->inc_oth, oth.data(), ninc));
+    KF_CUDA(upload(&m->inc_edge, edg.data(), ninc));
+    KF_CUDA(upload(&m->inc_blk, blk.data(), ninc));
+    KF_CUDA(upload(&m->inc_w, w.data(), 3 * ninc));
+  }
+  // wall faces (colour order) with normals -(1/6) a x b (src/flux.c:485-508)
+  {
+    const unsigned int *f0 = g->b->fc->fptr->n0, *f1 = g->b->fc->fptr->n1, *f2 = g->b->fc->fptr->n2;
+    const double *X = g->n->xyz->x0, *Y = g->n->xyz->x1, *Z = g->n->xyz->x2;
+    const double MAG0 = 0.5 / 3, MAG1 = -MAG0;
+    std::vector<uint32_t> fn(3 * (size_t)m->F);
+    std::vector<double> nn(3 * (size_t)m->F);
+    for (uint32_t j = 0; j < m->F; j++) {
+      const uint32_t a = f0[j], b = f1[j], d = f2[j];
+      fn[3 * j] = a; fn[3 * j + 1] = b; fn[3 * j + 2] = d;
+      const double ax = X[b] - X[a], ay = Y[b] - Y[a], az = Z[b] - Z[a];
+      const double bx = X[d] - X[a], by = Y[d] - Y[a], bz = Z[d] - Z[a];
+      double xn = ay * bz; xn -= az * by; xn *= MAG1;
+      double yn = ax * bz; yn -= az * bx; yn *= MAG0;
+      double zn = ax * by; zn -= ay * bx; zn *= MAG1;
+      nn[3 * j] = xn; nn[3 * j + 1] = yn; nn[3 * j + 2] = zn;
+    }
+    KF_CUDA(upload(&m->wf_nodes, fn.data(), fn.size()));
+    KF_CUDA(upload(&m->col, g->t->i, (size_t)m->ncol + 1));
+    KF_CUDA(upload(&m->wf_n, nn.data(), nn.size()));
+    std::vector<double> sn(3 * (size_t)m->Ns), fnn(3 * (size_t)m->Nf);
+    for (uint32_t i = 0; i < m->Ns; i++) {
+      sn[3 * i] = g->b->s->xyz->x0[i]; sn[3 * i + 1] = g->b->s->xyz->x1[i]; sn[3 * i + 2] = g->b->s->xyz->x2[i];
+    }
+    for (uint32_t i = 0; i < m->Nf; i++) {
+      fnn[3 * i] = g->b->f->xyz->x0[i]; fnn[3 * i + 1] = g->b->f->xyz->x1[i]; fnn[3 * i + 2] = g->b->f->xyz->x2[i];
+    }
+    KF_CUDA(upload(&m->s_n, sn.data(), sn.size()));
+    KF_CUDA(upload(&m->f_n, fnn.data(), fnn.size()));
+    // per boundary node: wall-face corners (face order = colour order), then
+    // wall-node entries, then far-field entries, each in list order
+    std::vector<std::vector<uint32_t>> ent(N);
+    for (uint32_t j = 0; j < m->F; j++) {
+      ent[f0[j]].push_back(0u << 29 | (3 * j + 0));
+      ent[f1[j]].push_back(0u << 29 | (3 * j + 1));
+      ent[f2[j]].push_back(0u << 29 | (3 * j + 2));
+    }
+    for (uint32_t i = 0; i < m->Ns; i++) ent[g->b->s->nptr[i]].push_back(1u << 29 | i);
+    for (uint32_t i = 0; i < m->Nf; i++) ent[g->b->f->nptr[i]].push_back(2u << 29 | i);
+    std::vector<uint32_t> of(N, 0xffffffffu), nodes, bptr(1, 0), bent;
+    for (uint32_t i = 0; i < N; i++) {
+      if (ent[i].empty()) continue;
+      of[i] = (uint32_t)nodes.size();
+      nodes.push_back(i);
+      bent.insert(bent.end(), ent[i].begin(), ent[i].end());
+      bptr.push_back((uint32_t)bent.size());
+    }
+    m->nb = (uint32_t)nodes.size();
+    KF_CUDA(upload(&m->bnd_of, of.data(), N));
+    KF_CUDA(upload(&m->bnd_node, nodes.data(), nodes.size()));
+    KF_CUDA(upload(&m->bnd_ptr, bptr.data(), bptr.size()));
+    KF_CUDA(upload(&m->bnd_ent, bent.data(), bent.size()));
+  }
+  // block pattern, persistent L slots, level sets
+  KF_CUDA(upload(&m->ia, p.ia.data(), p.ia.size()));
+  KF_CUDA(upload(&m->ja, p.ja.data(), p.ja.size()));
+  KF_CUDA(upload(&m->diag, p.diag.data(), p.diag.size()));
+  KF_CUDA(upload(&m->tblk, p.tblk.data(), p.tblk.size()));
+  KF_CUDA(upload(&m->lpos, p.lpos.data(), p.lpos.size()));
+  KF_CUDA(upload(&m->last_lower, p.last_lower.data(), p.last_lower.size()));
+  KF_CUDA(upload(&m->lev_l, p.lev_l.data(), p.lev_l.size()));
+  KF_CUDA(upload(&m->lev_u, p.lev_u.data(), p.lev_u.size()));
+  m->lev_l_ptr = p.lev_l_ptr;
+  m->lev_u_ptr = p.lev_u_ptr;
+  m->nlev_l = (uint32_t)p.lev_l_ptr.size() - 1;
+  m->nlev_u = (uint32_t)p.lev_u_ptr.size() - 1;
+  const size_t nb16 = 16 * (size_t)m->nnz;
+  KF_CUDA(cudaMalloc(&m->A, nb16 * sizeof(double)));
+  KF_CUDA(cudaMalloc(&m->Af, nb16 * sizeof(float)));
+  KF_CUDA(cudaMalloc(&m->lslot, (16 * (size_t)m->nlower + 16) * sizeof(double)));
+  KF_CUDA(cudaMemset(m->lslot, 0, (16 * (size_t)m->nlower + 16) * sizeof(double)));
+  KF_CUDA(cudaMalloc(&m->dinv, 16 * (size_t)N * sizeof(double)));
+  KF_CUDA(cudaMalloc(&m->dinvf, 16 * (size_t)N * sizeof(float)));
+  KF_CUDA(cudaMalloc(&m->dscr, (16 * (size_t)m->nb + 16) * sizeof(double)));
+  // vectors
+  const size_t dofs = 4 * (size_t)N;
+  double **vecs[] = {&m->q, &m->r, &m->gx, &m->gy, &m->gz, &m->w, &m->t, &m->x, &m->rhs};
+  for (double **v : vecs) {
+    KF_CUDA(cudaMalloc(v, dofs * sizeof(double)));
+    KF_CUDA(cudaMemset(*v, 0, dofs * sizeof(double)));
+  }
+  KF_CUDA(cudaMalloc(&m->cdt, (size_t)N * sizeof(double)));
+  KF_CUDA(cudaMemset(m->cdt, 0, (size_t)N * sizeof(double)));
+  KF_CUDA(cudaMalloc(&m->V, KF_NBASIS * dofs * sizeof(double)));
+  KF_CUDA(cudaMemset(m->V, 0, KF_NBASIS * dofs * sizeof(double)));
+  KF_CUDA(cudaMalloc(&m->red, 4096 * sizeof(double)));
+  KF_CUDA(cudaMalloc(&m->scal, 256 * sizeof(double)));
+  KF_CUDA(cudaMemset(m->scal, 0, 256 * sizeof(double)));
+  KF_CUDA(cudaMalloc(&m->forces, 4 * sizeof(double)));
+  KF_CUDA(cudaMalloc(&m->status, sizeof(int)));
+  KF_CUDA(cudaMemset(m->status, 0, sizeof(int)));
+  KF_CUDA(cudaMallocHost(&m->h_scal, 256 * sizeof(double)));
+  KF_CUDA(cudaDeviceSynchronize());
+  return m;
+}

@@ -1,0 +1,120 @@
+// kfun3d_b200 internals shared by the host and CUDA translation units.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "kfun3d_b200.h"
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#else
+struct double4_host { double x, y, z, w; };
+#endif
+
+void kf_set_error(int code, const char *msg);
+int kf_mode();
+int kf_precision();
+int kf_first_order();
+
+// Host-side block pattern of the edge graph (matrix/init.cpp:7-74): row i
+// holds its diagonal and one block per incident edge, columns sorted.
+struct HostPattern {
+  size_t n = 0, nnz = 0;
+  std::vector<uint32_t> ia, ja, diag;
+  std::vector<uint32_t> tblk;        // block (i,j) -> index of block (j,i)
+  std::vector<uint32_t> lpos;        // first persistent L slot of each row
+  std::vector<uint32_t> last_lower;  // per row: lower block the fill touches last (or ~0)
+  std::vector<uint32_t> lev_l, lev_l_ptr;   // rows by forward level (matrix/init.cpp:194-232)
+  std::vector<uint32_t> lev_u, lev_u_ptr;   // rows by backward level (matrix/init.cpp:234-270)
+};
+
+void kf_build_pattern(HostPattern &p, size_t nnodes, size_t nedges, const unsigned int *n0,
+                      const unsigned int *n1);
+
+struct DevMesh;
+
+// The opaque handle behind GEOMETRY::matrix.
+struct MatrixHandle {
+  uint32_t magic = 0x4B463344u;   // "KF3D"
+  HostPattern pat;
+  DevMesh *dev = nullptr;
+  const GEOMETRY *owner = nullptr;
+};
+
+MatrixHandle *kf_handle(const GEOMETRY *g);
+
+#ifdef __CUDACC__
+
+constexpr int KF_NBASIS = 31;
+
+// Device mirror of one GEOMETRY.  Node-indexed arrays follow the reference's
+// numbering; edge-indexed arrays its (sorted) edge order.
+struct DevMesh {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t N = 0, E = 0, Ns = 0, Nf = 0, F = 0, ncol = 0, nnz = 0, nlower = 0;
+  // static geometry
+  double4 *egeo = nullptr;        // [E] unit normal n0->n1, area
+  double4 *xyz = nullptr;         // [N] coordinates, w = 0
+  uint32_t *inc_ptr = nullptr;    // [N+1] incident edges of each node, in edge order
+  uint32_t *inc_oth = nullptr;    // [2E] the other end point
+  uint32_t *inc_edge = nullptr;   // [2E] edge index | (1u<<31 when the node is n1)
+  uint32_t *inc_blk = nullptr;    // [2E] block index of (node, other)
+  double *inc_w = nullptr;        // [3][2E] least-squares terms seen from the node
+  uint32_t *wf_nodes = nullptr;   // [3F] wall faces in colour order
+  double *wf_n = nullptr;         // [3F] wall-face normals -(1/6) a x b
+  uint32_t *col = nullptr;        // [ncol+1] wall-face colour offsets
+  double *s_n = nullptr;          // [3 Ns] wall-node normals
+  double *f_n = nullptr;          // [3 Nf] far-field node normals
+  uint32_t nb = 0;                // boundary nodes
+  uint32_t *bnd_of = nullptr;     // [N] position in bnd_node, or ~0
+  uint32_t *bnd_node = nullptr;   // [nb]
+  uint32_t *bnd_ptr = nullptr;    // [nb+1]
+  uint32_t *bnd_ent = nullptr;    // entries: kind << 29 | index
+  // block matrix
+  uint32_t *ia = nullptr, *ja = nullptr, *diag = nullptr, *tblk = nullptr;
+  uint32_t *lpos = nullptr, *last_lower = nullptr;
+  uint32_t nlev_l = 0, nlev_u = 0;
+  std::vector<uint32_t> lev_l_ptr, lev_u_ptr;   // host copies of level offsets
+  uint32_t *lev_l = nullptr, *lev_u = nullptr;
+  double *A = nullptr;            // [nnz*16]
+  double *lslot = nullptr;        // [nlower*16] persistent L slots
+  double *dinv = nullptr;         // [N*16] inverse diagonal blocks
+  float *Af = nullptr;            // [nnz*16] FP32 form
+  float *dinvf = nullptr;         // [N*16]
+  // state and work vectors (4N doubles each)
+  double *q = nullptr, *r = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr;
+  double *cdt = nullptr, *w = nullptr, *t = nullptr, *x = nullptr, *rhs = nullptr;
+  double *V = nullptr;            // [KF_NBASIS][4N]
+  double *red = nullptr;          // reduction scratch
+  double *scal = nullptr;         // device scalars
+  double *forces = nullptr;       // [3]
+  double *dscr = nullptr;         // [nb*16] double diagonal blocks of boundary rows (FP32 fill)
+  int *status = nullptr;          // device status word (pivot failures)
+  double *h_scal = nullptr;       // pinned host mirror of scal
+  bool factored = false;
+  bool a_valid = false;
+};
+
+DevMesh *kf_device(const GEOMETRY *g);   // creates and uploads on first use
+
+void kf_count_launch(unsigned n = 1);
+
+// Kernel families, one set per arithmetic mode (kernels_exact.cu, kernels_fast.cu).
+#define KF_DECLARE_KERNELS(NS)                                                          \
+  namespace NS {                                                                        \
+  void gradient(DevMesh &m, const double *q);                                           \
+  void residual(DevMesh &m, const double *q, double *r, int first_order, double u, double v); \
+  void timestep(DevMesh &m, const double *q, double cfl);                               \
+  void fill(DevMesh &m, const double *q, double u, double v, int precision);            \
+  void ilu(DevMesh &m, int precision);                                                  \
+  void sptrsv(DevMesh &m, const double *b, double *x, int precision);                   \
+  void jv_combine(DevMesh &m, double *y, const double *r, const double *w,              \
+                  const double *q, const double *scal, int ia);                          \
+  }
+KF_DECLARE_KERNELS(kf_exact)
+KF_DECLARE_KERNELS(kf_fast)
+
+#endif

@@ -1,0 +1,1092 @@
+// kfun3d_b200 device kernels for the residual, time step, Jacobian fill,
+// ILU(0) and triangular solves.
+//
+// Included twice: kernels_exact.cu (KF_FAST 0, compiled with -fmad=false) and
+// kernels_fast.cu (KF_FAST 1, fused multiply-add allowed).  In the exact build
+// every expression keeps the reference's operation order, and every per-node
+// sum is taken in the reference's order (edges by index, then wall faces by
+// colour, then far-field nodes), which makes the results bit-identical to the
+// reference at one OpenMP thread.  No kernel uses floating-point atomics: each
+// node (or matrix row) is owned by one thread, which gathers its incident
+// edges and recomputes the edge terms it needs, so every run is deterministic.
+//
+// Layout in HBM (DevMesh): node state q, residual r and the three gradient
+// arrays are double4 per node (the reference's q[4*node+var] AoS, one 32-byte
+// sector per gather); edge geometry is a double4 (unit normal, area) per edge;
+// each node's incident edges are a contiguous run of the incidence arrays.
+#include <cstdint>
+
+#include "internal.h"
+
+#ifndef KF_FAST
+#error "define KF_FAST"
+#endif
+
+namespace KF_NS {
+
+constexpr double KB = 15.0;                  // inc/phy.h:6 (beta)
+constexpr double KP = 1.0;                   // inc/phy.h:7
+constexpr double KW = 0.0;                   // inc/phy.h:10
+constexpr double SWITCH = (double)0.95f;     // src/flux.c:181 (a float literal)
+constexpr double MAG0 = 0.5 / 3;             // src/flux.c:11
+constexpr double MAG1 = -MAG0;
+constexpr double INV_B = 1.0 / 15.0;
+
+__device__ __forceinline__ double div_b(double x)
+{
+#if KF_FAST
+  return x * INV_B;
+#else
+  return x / KB;
+#endif
+}
+
+struct Frame { double x1, y1, z1, x2, y2, z2; };
+
+// src/flux.c:173-217: unit tangents completing the unit normal.
+__device__ __forceinline__ Frame tangents(double xn, double yn, double zn)
+{
+  Frame f;
+  double d;
+  if (fabs(xn) < SWITCH) {
+    d = xn;
+    f.x1 = 1.0 - d * xn;
+    f.y1 = -d * yn;
+    f.z1 = -d * zn;
+  } else {
+    d = yn;
+    f.x1 = -d * xn;
+    f.y1 = 1.0 - d * yn;
+    f.z1 = -d * zn;
+  }
+  double s = f.x1 * f.x1;
+  s += f.y1 * f.y1;
+  s += f.z1 * f.z1;
+#if KF_FAST
+  const double is = rsqrt(s);
+  f.x1 *= is;
+  f.y1 *= is;
+  f.z1 *= is;
+#else
+  s = sqrt(s);
+  f.x1 /= s;
+  f.y1 /= s;
+  f.z1 /= s;
+#endif
+  f.x2 = yn * f.z1;
+  f.x2 -= zn * f.y1;
+  f.y2 = zn * f.x1;
+  f.y2 -= xn * f.z1;
+  f.z2 = xn * f.y1;
+  f.z2 -= yn * f.x1;
+  return f;
+}
+
+struct Phi { double p4, p5, p6, p7, p8, p9; };
+
+// src/flux.c:299-324
+__device__ __forceinline__ Phi phis(double xn, double yn, double zn, double u, double v,
+                                    double w, double ubar, const Frame &f)
+{
+  double p1 = xn * KB; p1 += u * ubar;
+  double p2 = yn * KB; p2 += v * ubar;
+  double p3 = zn * KB; p3 += w * ubar;
+  Phi ph;
+  ph.p4 = f.y2 * p3; ph.p4 -= f.z2 * p2;
+  ph.p5 = f.z2 * p1; ph.p5 -= f.x2 * p3;
+  ph.p6 = f.x2 * p2; ph.p6 -= f.y2 * p1;
+  ph.p7 = f.z1 * p2; ph.p7 -= f.y1 * p3;
+  ph.p8 = f.x1 * p3; ph.p8 -= f.z1 * p1;
+  ph.p9 = f.y1 * p1; ph.p9 -= f.x1 * p2;
+  return ph;
+}
+
+__device__ __forceinline__ double4 add4(double4 a, double4 b) { return make_double4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+__device__ __forceinline__ double4 sub4(double4 a, double4 b) { return make_double4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w); }
+
+// Reconstructed state at the edge midpoint, src/flux.c:222-251.
+__device__ __forceinline__ double4 recon(double4 q, double4 gx, double4 gy, double4 gz,
+                                         double rx, double ry, double rz)
+{
+  double4 s;
+  s.x = q.x + gx.x * rx; s.x += gy.x * ry; s.x += gz.x * rz;
+  s.y = q.y + gx.y * rx; s.y += gy.y * ry; s.y += gz.y * rz;
+  s.z = q.z + gx.z * rx; s.z += gy.z * ry; s.z += gz.z * rz;
+  s.w = q.w + gx.w * rx; s.w += gy.w * ry; s.w += gz.w * rz;
+  return s;
+}
+
+// Dissipative edge flux of src/flux.c:159-448 between end points a = n0 and
+// b = n1 (states already reconstructed, sL/sR = p,u,v,w).
+__device__ __forceinline__ double4 edge_flux(double4 geo, double4 sL, double4 sR)
+{
+  const double xn = geo.x, yn = geo.y, zn = geo.z, ln = geo.w;
+  const Frame f = tangents(xn, yn, zn);
+  double ubarL = xn * sL.y; ubarL += yn * sL.z; ubarL += zn * sL.w;
+  double ubarR = xn * sR.y; ubarR += yn * sR.z; ubarR += zn * sR.w;
+  const double u = 0.5 * (sL.y + sR.y);
+  const double v = 0.5 * (sL.z + sR.z);
+  const double w = 0.5 * (sL.w + sR.w);
+  double ubar = xn * u; ubar += yn * v; ubar += zn * w;
+  const Phi ph = phis(xn, yn, zn, u, v, w, ubar, f);
+  const double c2 = ubar * ubar + KB;
+  const double c = sqrt(c2);
+  const double e12 = fabs(ubar), e3 = fabs(ubar + c), e4 = fabs(ubar - c);
+  const double dp = sR.x - sL.x, du = sR.y - sL.y, dv = sR.z - sL.z, dw = sR.w - sL.w;
+
+  double ti11 = u * ph.p4; ti11 += v * ph.p5; ti11 += w * ph.p6; ti11 = div_b(-ti11);
+  double ti21 = u * ph.p7; ti21 += v * ph.p8; ti21 += w * ph.p9; ti21 = div_b(-ti21);
+  double ti31 = 0.5 * (c - ubar); ti31 = div_b(ti31);
+  double ti41 = -0.5 * (c + ubar); ti41 = div_b(ti41);
+
+  double dv1 = ti11 * dp; dv1 += ph.p4 * du; dv1 += ph.p5 * dv; dv1 += ph.p6 * dw;
+  double dv2 = ti21 * dp; dv2 += ph.p7 * du; dv2 += ph.p8 * dv; dv2 += ph.p9 * dw;
+  double dv3 = 2.0 * ti31 * dp; dv3 += xn * du; dv3 += yn * dv; dv3 += zn * dw;
+  double dv4 = 2.0 * ti41 * dp; dv4 += xn * du; dv4 += yn * dv; dv4 += zn * dw;
+#if KF_FAST
+  const double ic2 = 1.0 / c2;
+  dv1 *= ic2;
+  dv2 *= ic2;
+  dv3 *= 0.5 * ic2;
+  dv4 *= 0.5 * ic2;
+#else
+  dv1 /= c2;
+  dv2 /= c2;
+  const double hc2 = 0.5 / c2;
+  dv3 *= hc2;
+  dv4 *= hc2;
+#endif
+  const double r13 = c * KB;
+  double r23 = u * (ubar + c); r23 += xn * KB;
+  double r33 = v * (ubar + c); r33 += yn * KB;
+  double r43 = w * (ubar + c); r43 += zn * KB;
+  const double r14 = -c * KB;
+  double r24 = u * (ubar - c); r24 += xn * KB;
+  double r34 = v * (ubar - c); r34 += yn * KB;
+  double r44 = w * (ubar - c); r44 += zn * KB;
+
+  const double t1 = e3 * r13 * dv3 + e4 * r14 * dv4;
+  double t2 = e12 * f.x1 * dv1 + e12 * f.x2 * dv2;
+  t2 += e3 * r23 * dv3 + e4 * r24 * dv4;
+  double t3 = e12 * f.y1 * dv1 + e12 * f.y2 * dv2;
+  t3 += e3 * r33 * dv3 + e4 * r34 * dv4;
+  double t4 = e12 * f.z1 * dv1 + e12 * f.z2 * dv2;
+  t4 += e3 * r43 * dv3 + e4 * r44 * dv4;
+
+  const double fp1 = ln * KB * ubarL;
+  const double fp2 = ln * (sL.y * ubarL + xn * sL.x);
+  const double fp3 = ln * (sL.z * ubarL + yn * sL.x);
+  const double fp4 = ln * (sL.w * ubarL + zn * sL.x);
+  const double fm1 = ln * KB * ubarR;
+  const double fm2 = ln * (sR.y * ubarR + xn * sR.x);
+  const double fm3 = ln * (sR.z * ubarR + yn * sR.x);
+  const double fm4 = ln * (sR.w * ubarR + zn * sR.x);
+  double4 res;
+  res.x = 0.5 * (fp1 + fm1 - ln * t1);
+  res.y = 0.5 * (fp2 + fm2 - ln * t2);
+  res.z = 0.5 * (fp3 + fm3 - ln * t3);
+  res.w = 0.5 * (fp4 + fm4 - ln * t4);
+  return res;
+}
+
+// Characteristic far-field flux at one node, src/flux.c:552-778.
+__device__ __forceinline__ double4 farfield_flux(double U, double V, double fx, double fy,
+                                                 double fz, double4 qi)
+{
+  double area = fx * fx; area += fy * fy; area += fz * fz; area = sqrt(area);
+  const double xn = fx / area, yn = fy / area, zn = fz / area;
+  const Frame f = tangents(xn, yn, zn);
+  double ubar0 = xn * U; ubar0 += yn * V; ubar0 += zn * KW;
+  const double c20 = ubar0 * ubar0 + KB;
+  const double c0 = sqrt(c20);
+  const Phi ph = phis(xn, yn, zn, U, V, KW, ubar0, f);
+  const double t13 = c0 * KB;
+  double t23 = U * (ubar0 + c0); t23 += xn * KB;
+  double t33 = V * (ubar0 + c0); t33 += yn * KB;
+  double t43 = KW * (ubar0 + c0); t43 += zn * KB;
+  const double t14 = -c0 * KB;
+  double t24 = U * (ubar0 - c0); t24 += xn * KB;
+  double t34 = V * (ubar0 - c0); t34 += yn * KB;
+  double t44 = KW * (ubar0 - c0); t44 += zn * KB;
+  double ti11 = U * ph.p4; ti11 += V * ph.p5; ti11 += KW * ph.p6; ti11 = -ti11 / KB;
+  double ti21 = U * ph.p7; ti21 += V * ph.p8; ti21 += KW * ph.p9; ti21 = -ti21 / KB;
+  double ti31 = 0.5 * (c0 - ubar0); ti31 /= KB;
+  double ti41 = -0.5 * (c0 + ubar0); ti41 /= KB;
+  const double pi = qi.x, ui = qi.y, vi = qi.z, wi = qi.w;
+  double un = xn * ui; un += yn * vi; un += zn * wi;
+  double pr, ur, vr, wr;
+  if (un > 0.0) { pr = pi; ur = ui; vr = vi; wr = wi; }
+  else { pr = KP; ur = U; vr = V; wr = KW; }
+  double rhs1 = ti11 * pr; rhs1 += ph.p4 * ur; rhs1 += ph.p5 * vr; rhs1 += ph.p6 * wr; rhs1 /= c20;
+  double rhs2 = ti21 * pr; rhs2 += ph.p7 * ur; rhs2 += ph.p8 * vr; rhs2 += ph.p9 * wr; rhs2 /= c20;
+  double rhs3 = 2.0 * ti31 * pi; rhs3 += xn * ui; rhs3 += yn * vi; rhs3 += zn * wi;
+  rhs3 = 0.5 * rhs3 / c20;
+  double rhs4 = 2.0 * ti41 * KP; rhs4 += xn * U; rhs4 += yn * V; rhs4 += zn * KW;
+  rhs4 = 0.5 * rhs4 / c20;
+  double pb = t13 * rhs3; pb += t14 * rhs4;
+  double ub = f.x1 * rhs1; ub += f.x2 * rhs2; ub += t23 * rhs3; ub += t24 * rhs4;
+  double vb = f.y1 * rhs1; vb += f.y2 * rhs2; vb += t33 * rhs3; vb += t34 * rhs4;
+  double wb = f.z1 * rhs1; wb += f.z2 * rhs2; wb += t43 * rhs3; wb += t44 * rhs4;
+  double ubar = xn * ub; ubar += yn * vb; ubar += zn * wb;
+  double4 o;
+  o.x = area * KB * ubar;
+  o.y = area * (ub * ubar + xn * pb);
+  o.z = area * (vb * ubar + yn * pb);
+  o.w = area * (wb * ubar + zn * pb);
+  return o;
+}
+
+// ------------------------------------------------------------------ gradient
+
+// src/flux.c:60-145 as a gather: node n sums w.(q[other]-q[n]) over its
+// incident edges in edge order.
+__global__ void __launch_bounds__(256) k_gradient(uint32_t N, const uint32_t *__restrict__ inc_ptr,
+                                                  const uint32_t *__restrict__ inc_oth,
+                                                  const double *__restrict__ inc_w, uint32_t ninc,
+                                                  const double4 *__restrict__ q, double4 *__restrict__ gx,
+                                                  double4 *__restrict__ gy, double4 *__restrict__ gz)
+{
+  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const double4 qn = q[n];
+  double4 ax = make_double4(0, 0, 0, 0), ay = ax, az = ax;
+  const uint32_t k1 = inc_ptr[n + 1];
+  for (uint32_t k = inc_ptr[n]; k < k1; k++) {
+    const double4 qo = q[inc_oth[k]];
+    const double wx = inc_w[k], wy = inc_w[ninc + k], wz = inc_w[2 * (size_t)ninc + k];
+    double dq;
+    dq = qo.x - qn.x; ax.x += wx * dq; ay.x += wy * dq; az.x += wz * dq;
+    dq = qo.y - qn.y; ax.y += wx * dq; ay.y += wy * dq; az.y += wz * dq;
+    dq = qo.z - qn.z; ax.z += wx * dq; ay.z += wy * dq; az.z += wz * dq;
+    dq = qo.w - qn.w; ax.w += wx * dq; ay.w += wy * dq; az.w += wz * dq;
+  }
+  gx[n] = ax;
+  gy[n] = ay;
+  gz[n] = az;
+}
+
+// ------------------------------------------------------------------ residual
+
+// src/flux.c:151-465 as a gather: node n recomputes the flux of each incident
+// edge (end points in the reference's n0/n1 roles) and adds it (n = n0) or
+// subtracts it (n = n1) in edge order.
+template <bool FIRST_ORDER>
+__global__ void __launch_bounds__(128) k_residual(uint32_t N, const uint32_t *__restrict__ inc_ptr,
+                                                  const uint32_t *__restrict__ inc_oth,
+                                                  const uint32_t *__restrict__ inc_edge,
+                                                  const double4 *__restrict__ egeo,
+                                                  const double4 *__restrict__ xyz,
+                                                  const double4 *__restrict__ q,
+                                                  const double4 *__restrict__ gx,
+                                                  const double4 *__restrict__ gy,
+                                                  const double4 *__restrict__ gz, double4 *__restrict__ r)
+{
+  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const double4 qs = q[n], xs = xyz[n];
+  double4 gxs, gys, gzs;
+  if (!FIRST_ORDER) { gxs = gx[n]; gys = gy[n]; gzs = gz[n]; }
+  double4 acc = make_double4(0, 0, 0, 0);
+  const uint32_t k1 = inc_ptr[n + 1];
+  for (uint32_t k = inc_ptr[n]; k < k1; k++) {
+    const uint32_t o = inc_oth[k], ev = inc_edge[k];
+    const bool is_n1 = ev >> 31;
+    const double4 geo = egeo[ev & 0x7fffffffu];
+    const double4 qo = q[o], xo = xyz[o];
+    const double4 xa = is_n1 ? xo : xs, xb = is_n1 ? xs : xo;
+    const double4 qa = is_n1 ? qo : qs, qb = is_n1 ? qs : qo;
+    const double xm = 0.5 * (xa.x + xb.x), ym = 0.5 * (xa.y + xb.y), zm = 0.5 * (xa.z + xb.z);
+    double4 sL, sR;
+    if (FIRST_ORDER) {
+      const double4 z = make_double4(0, 0, 0, 0);
+      sL = recon(qa, z, z, z, xm - xa.x, ym - xa.y, zm - xa.z);
+      sR = recon(qb, z, z, z, xm - xb.x, ym - xb.y, zm - xb.z);
+    } else {
+      const double4 gxo = gx[o], gyo = gy[o], gzo = gz[o];
+      sL = is_n1 ? recon(qa, gxo, gyo, gzo, xm - xa.x, ym - xa.y, zm - xa.z)
+                 : recon(qa, gxs, gys, gzs, xm - xa.x, ym - xa.y, zm - xa.z);
+      sR = is_n1 ? recon(qb, gxs, gys, gzs, xm - xb.x, ym - xb.y, zm - xb.z)
+                 : recon(qb, gxo, gyo, gzo, xm - xb.x, ym - xb.y, zm - xb.z);
+    }
+    const double4 res = edge_flux(geo, sL, sR);
+    acc = is_n1 ? sub4(acc, res) : add4(acc, res);
+  }
+  r[n] = acc;
+}
+
+// Boundary terms, after all edges: wall faces by colour (src/flux.c:467-539),
+// then far-field nodes (src/flux.c:541-779), each node in list order.
+__global__ void k_residual_boundary(uint32_t nb, const uint32_t *__restrict__ bnd_node,
+                                    const uint32_t *__restrict__ bnd_ptr,
+                                    const uint32_t *__restrict__ bnd_ent,
+                                    const uint32_t *__restrict__ wf_nodes,
+                                    const double *__restrict__ wf_n, const double *__restrict__ f_n,
+                                    const double4 *__restrict__ q, double4 *__restrict__ r,
+                                    double U, double V)
+{
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const uint32_t n = bnd_node[b];
+  double4 acc = r[n];
+  for (uint32_t k = bnd_ptr[b]; k < bnd_ptr[b + 1]; k++) {
+    const uint32_t ent = bnd_ent[k], kind = ent >> 29, idx = ent & 0x1fffffffu;
+    if (kind == 0) {
+      const uint32_t f = idx / 3, corner = idx % 3;
+      const double p1 = q[wf_nodes[3 * f]].x, p2 = q[wf_nodes[3 * f + 1]].x, p3 = q[wf_nodes[3 * f + 2]].x;
+      double p;
+      if (corner == 0) { p = 0.125 * (p2 + p3); p += 0.75 * p1; }
+      else if (corner == 1) { p = 0.125 * (p3 + p1); p += 0.75 * p2; }
+      else { p = 0.125 * (p1 + p2); p += 0.75 * p3; }
+      acc.y += wf_n[3 * f] * p;
+      acc.z += wf_n[3 * f + 1] * p;
+      acc.w += wf_n[3 * f + 2] * p;
+    } else if (kind == 2) {
+      const double4 o = farfield_flux(U, V, f_n[3 * idx], f_n[3 * idx + 1], f_n[3 * idx + 2], q[n]);
+      acc.x += o.x;
+      acc.y += o.y;
+      acc.z += o.z;
+      acc.w += o.w;
+    }
+  }
+  r[n] = acc;
+}
+
+// ------------------------------------------------------------------ time step
+
+// src/timestep.c:58-91 as a gather; nodes without boundary terms are divided
+// by the CFL number here, boundary nodes in k_timestep_boundary.
+__global__ void __launch_bounds__(256) k_timestep(uint32_t N, const uint32_t *__restrict__ inc_ptr,
+                                                  const uint32_t *__restrict__ inc_oth,
+                                                  const uint32_t *__restrict__ inc_edge,
+                                                  const double4 *__restrict__ egeo,
+                                                  const double4 *__restrict__ q,
+                                                  const uint32_t *__restrict__ bnd_of, double cfl,
+                                                  double *__restrict__ cdt)
+{
+  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const double4 qs = q[n];
+  double acc = 0.0;
+  const uint32_t k1 = inc_ptr[n + 1];
+  for (uint32_t k = inc_ptr[n]; k < k1; k++) {
+    const uint32_t ev = inc_edge[k];
+    const bool is_n1 = ev >> 31;
+    const double4 geo = egeo[ev & 0x7fffffffu];
+    const double4 qo = q[inc_oth[k]];
+    const double4 qa = is_n1 ? qo : qs, qb = is_n1 ? qs : qo;
+    const double xnorm = geo.x * geo.w, ynorm = geo.y * geo.w, znorm = geo.z * geo.w;
+    const double u = 0.5 * (qa.y + qb.y), v = 0.5 * (qa.z + qb.z), w = 0.5 * (qa.w + qb.w);
+    const double ubar = geo.x * u + geo.y * v + geo.z * w;
+    const double c = sqrt(ubar * ubar + KB);
+    double term = u * xnorm;
+    term += v * ynorm;
+    term += w * znorm;
+    term = fabs(term) + c * geo.w;
+    acc = acc + term;
+  }
+  cdt[n] = (bnd_of[n] == 0xffffffffu) ? acc / cfl : acc;
+}
+
+__device__ __forceinline__ double boundary_rate(double xn, double yn, double zn, double4 qi)
+{
+  // src/timestep.c:98-118 and 126-146
+  const double ln = sqrt(xn * xn + yn * yn + zn * zn);
+  const double ubar = qi.y * xn + qi.z * yn + qi.w * zn;
+  const double ub = ubar / ln;
+  const double c = sqrt(ub * ub + KB);
+  return fabs(ubar) + c * ln;
+}
+
+__global__ void k_timestep_boundary(uint32_t nb, const uint32_t *__restrict__ bnd_node,
+                                    const uint32_t *__restrict__ bnd_ptr,
+                                    const uint32_t *__restrict__ bnd_ent,
+                                    const double *__restrict__ s_n, const double *__restrict__ f_n,
+                                    const double4 *__restrict__ q, double cfl, double *__restrict__ cdt)
+{
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const uint32_t n = bnd_node[b];
+  double acc = cdt[n];
+  const double4 qi = q[n];
+  for (uint32_t k = bnd_ptr[b]; k < bnd_ptr[b + 1]; k++) {
+    const uint32_t ent = bnd_ent[k], kind = ent >> 29, idx = ent & 0x1fffffffu;
+    if (kind == 1) acc += boundary_rate(s_n[3 * idx], s_n[3 * idx + 1], s_n[3 * idx + 2], qi);
+    else if (kind == 2) acc += boundary_rate(f_n[3 * idx], f_n[3 * idx + 1], f_n[3 * idx + 2], qi);
+  }
+  cdt[n] = acc / cfl;
+}
+
+// ------------------------------------------------------------------ Jacobian
+
+// First-order edge Jacobians v0 = (A_L + |A|)/2 and v1 = (A_R - |A|)/2 of
+// src/fill.c:171-494 (row-major 4x4, row = flux component).
+__device__ __forceinline__ void edge_jacobians(double4 geo, double4 qa, double4 qb, double *v0, double *v1)
+{
+  const double xn = geo.x, yn = geo.y, zn = geo.z, ln = geo.w;
+  const Frame f = tangents(xn, yn, zn);
+  const double uL = qa.y, vL = qa.z, wL = qa.w;
+  double ubarL = xn * uL; ubarL += yn * vL; ubarL += zn * wL;
+  const double uR = qb.y, vR = qb.z, wR = qb.w;
+  double ubarR = xn * uR; ubarR += yn * vR; ubarR += zn * wR;
+  const double u = 0.5 * (uL + uR), v = 0.5 * (vL + vR), w = 0.5 * (wL + wR);
+  double ubar = xn * u; ubar += yn * v; ubar += zn * w;
+  const double c2 = ubar * ubar + KB;
+  const double c = sqrt(c2);
+  const double e12 = ln * fabs(ubar), e3 = ln * fabs(ubar + c), e4 = ln * fabs(ubar - c);
+  const Phi ph = phis(xn, yn, zn, u, v, w, ubar, f);
+  const double c2inv = 1.0 / c2;
+  double y1[4], y2[4], y3[4], y4[4];   // rows of T^-1, columns p,u,v,w
+  double t;
+  t = u * ph.p4; t += v * ph.p5; t += w * ph.p6; y1[0] = div_b(-c2inv * t);
+  t = u * ph.p7; t += v * ph.p8; t += w * ph.p9; y2[0] = div_b(-c2inv * t);
+  t = c2inv * (c - ubar); y3[0] = div_b(0.5 * t);
+  t = c2inv * (c + ubar); y4[0] = div_b(-0.5 * t);
+  y1[1] = c2inv * ph.p4; y2[1] = c2inv * ph.p7; y3[1] = c2inv * 0.5 * xn; y4[1] = c2inv * 0.5 * xn;
+  y1[2] = c2inv * ph.p5; y2[2] = c2inv * ph.p8; y3[2] = c2inv * 0.5 * yn; y4[2] = c2inv * 0.5 * yn;
+  y1[3] = c2inv * ph.p6; y2[3] = c2inv * ph.p9; y3[3] = c2inv * 0.5 * zn; y4[3] = c2inv * 0.5 * zn;
+  const double t13 = c * KB;
+  double t23 = u * (ubar + c); t23 += xn * KB;
+  double t33 = v * (ubar + c); t33 += yn * KB;
+  double t43 = w * (ubar + c); t43 += zn * KB;
+  const double t14 = -c * KB;
+  double t24 = u * (ubar - c); t24 += xn * KB;
+  double t34 = v * (ubar - c); t34 += yn * KB;
+  double t44 = w * (ubar - c); t44 += zn * KB;
+  double a[4][4];   // |A| = T |Lambda| T^-1, src/fill.c:367-439
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    double s = e3 * t13 * y3[j];
+    s += e4 * t14 * y4[j];
+    a[0][j] = s;
+    s = e12 * f.x1 * y1[j]; s += e12 * f.x2 * y2[j]; s += e3 * t23 * y3[j]; s += e4 * t24 * y4[j];
+    a[1][j] = s;
+    s = e12 * f.y1 * y1[j]; s += e12 * f.y2 * y2[j]; s += e3 * t33 * y3[j]; s += e4 * t34 * y4[j];
+    a[2][j] = s;
+    s = e12 * f.z1 * y1[j]; s += e12 * f.z2 * y2[j]; s += e3 * t43 * y3[j]; s += e4 * t44 * y4[j];
+    a[3][j] = s;
+  }
+  const double lb = ln * KB, lx = ln * xn, ly = ln * yn, lz = ln * zn;
+  v0[0] = 0.5 * a[0][0];
+  v0[4] = 0.5 * (lx + a[1][0]);
+  v0[8] = 0.5 * (ly + a[2][0]);
+  v0[12] = 0.5 * (lz + a[3][0]);
+  v0[1] = 0.5 * ((lb * xn) + a[0][1]);
+  v0[5] = 0.5 * ((ln * (ubarL + xn * uL)) + a[1][1]);
+  v0[9] = 0.5 * ((lx * vL) + a[2][1]);
+  v0[13] = 0.5 * ((lx * wL) + a[3][1]);
+  v0[2] = 0.5 * ((lb * yn) + a[0][2]);
+  v0[6] = 0.5 * ((ly * uL) + a[1][2]);
+  v0[10] = 0.5 * ((ln * (ubarL + yn * vL)) + a[2][2]);
+  v0[14] = 0.5 * ((ly * wL) + a[3][2]);
+  v0[3] = 0.5 * ((lb * zn) + a[0][3]);
+  v0[7] = 0.5 * ((lz * uL) + a[1][3]);
+  v0[11] = 0.5 * ((lz * vL) + a[2][3]);
+  v0[15] = 0.5 * ((ln * (ubarL + zn * wL)) + a[3][3]);
+  v1[0] = 0.5 * -a[0][0];
+  v1[4] = 0.5 * (lx - a[1][0]);
+  v1[8] = 0.5 * (ly - a[2][0]);
+  v1[12] = 0.5 * (lz - a[3][0]);
+  v1[1] = 0.5 * ((lb * xn) - a[0][1]);
+  v1[5] = 0.5 * ((ln * (ubarR + xn * uR)) - a[1][1]);
+  v1[9] = 0.5 * ((lx * vR) - a[2][1]);
+  v1[13] = 0.5 * ((lx * wR) - a[3][1]);
+  v1[2] = 0.5 * ((lb * yn) - a[0][2]);
+  v1[6] = 0.5 * ((ly * uR) - a[1][2]);
+  v1[10] = 0.5 * ((ln * (ubarR + yn * vR)) - a[2][2]);
+  v1[14] = 0.5 * ((ly * wR) - a[3][2]);
+  v1[3] = 0.5 * ((lb * zn) - a[0][3]);
+  v1[7] = 0.5 * ((lz * uR) - a[1][3]);
+  v1[11] = 0.5 * ((lz * vR) - a[2][3]);
+  v1[15] = 0.5 * ((ln * (ubarR + zn * wR)) - a[3][3]);
+}
+
+// Far-field diagonal block (frozen free-stream T), src/fill.c:527-877.
+__device__ __forceinline__ void farfield_jacobian(double U, double V, double fx, double fy, double fz,
+                                                  double4 qi, double *vb)
+{
+  const double ln = sqrt(fx * fx + fy * fy + fz * fz);
+  const double xn = fx / ln, yn = fy / ln, zn = fz / ln;
+  const Frame f = tangents(xn, yn, zn);
+  double ubar0 = xn * U; ubar0 += yn * V; ubar0 += zn * KW;
+  const double c20 = ubar0 * ubar0 + KB;
+  const double c0 = sqrt(c20);
+  const Phi ph = phis(xn, yn, zn, U, V, KW, ubar0, f);
+  const double t13 = c0 * KB;
+  double t23 = U * (ubar0 + c0); t23 += xn * KB;
+  double t33 = V * (ubar0 + c0); t33 += yn * KB;
+  double t43 = KW * (ubar0 + c0); t43 += zn * KB;
+  const double t14 = -c0 * KB;
+  double t24 = U * (ubar0 - c0); t24 += xn * KB;
+  double t34 = V * (ubar0 - c0); t34 += yn * KB;
+  double t44 = KW * (ubar0 - c0); t44 += zn * KB;
+  double ti11 = U * ph.p4; ti11 += V * ph.p5; ti11 += KW * ph.p6; ti11 = -ti11 / KB / c20;
+  double ti21 = U * ph.p7; ti21 += V * ph.p8; ti21 += KW * ph.p9; ti21 = -ti21 / KB / c20;
+  const double ti31 = (c0 - ubar0) / (2.0 * KB * c20);
+  const double ti41 = -(c0 + ubar0) / (2.0 * KB * c20);
+  const double ti12 = ph.p4 / c20, ti22 = ph.p7 / c20, ti32 = 0.5 * xn / c20, ti42 = 0.5 * xn / c20;
+  const double ti13 = ph.p5 / c20, ti23 = ph.p8 / c20, ti33 = 0.5 * yn / c20, ti43 = 0.5 * yn / c20;
+  const double ti14 = ph.p6 / c20, ti24 = ph.p9 / c20, ti34 = 0.5 * zn / c20, ti44 = 0.5 * zn / c20;
+  const double pi = qi.x, ui = qi.y, vi = qi.z, wi = qi.w;
+  double un = xn * ui; un += yn * vi; un += zn * wi;
+  double pr, prp, ur, uru, vr, vrv, wr, wrw;
+  if (un > 0.0) { pr = pi; prp = 1.0; ur = ui; uru = 1.0; vr = vi; vrv = 1.0; wr = wi; wrw = 1.0; }
+  else { pr = KP; prp = 0.0; ur = U; uru = 0.0; vr = V; vrv = 0.0; wr = KW; wrw = 0.0; }
+  double rhs1 = ti11 * pr; rhs1 += ti12 * ur; rhs1 += ti13 * vr; rhs1 += ti14 * wr;
+  const double r1d[4] = {ti11 * prp, ti12 * uru, ti13 * vrv, ti14 * wrw};
+  double rhs2 = ti21 * pr; rhs2 += ti22 * ur; rhs2 += ti23 * vr; rhs2 += ti24 * wr;
+  const double r2d[4] = {ti21 * prp, ti22 * uru, ti23 * vrv, ti24 * wrw};
+  double rhs3 = ti31 * pi; rhs3 += ti32 * ui; rhs3 += ti33 * vi; rhs3 += ti34 * wi;
+  double rhs4 = ti41 * KP; rhs4 += ti42 * U; rhs4 += ti43 * V; rhs4 += ti44 * KW;
+  double pb = t13 * rhs3; pb += t14 * rhs4;
+  const double tid[4] = {ti31, ti32, ti33, ti34};
+  double ub = f.x1 * rhs1; ub += f.x2 * rhs2; ub += t23 * rhs3; ub += t24 * rhs4;
+  double vb_ = f.y1 * rhs1; vb_ += f.y2 * rhs2; vb_ += t33 * rhs3; vb_ += t34 * rhs4;
+  double wb = f.z1 * rhs1; wb += f.z2 * rhs2; wb += t43 * rhs3; wb += t44 * rhs4;
+  double unb = xn * ub; unb += yn * vb_; unb += zn * wb;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const double pbd = t13 * tid[k];
+    double ubd = f.x1 * r1d[k]; ubd += f.x2 * r2d[k]; ubd += t23 * tid[k];
+    double vbd = f.y1 * r1d[k]; vbd += f.y2 * r2d[k]; vbd += t33 * tid[k];
+    double wbd = f.z1 * r1d[k]; wbd += f.z2 * r2d[k]; wbd += t43 * tid[k];
+    double unbd = xn * ubd; unbd += yn * vbd; unbd += zn * wbd;
+    vb[k] = ln * KB * unbd;
+    vb[4 + k] = ln * (ub * unbd + unb * ubd + xn * pbd);
+    vb[8 + k] = ln * (vb_ * unbd + unb * vbd + yn * pbd);
+    vb[12 + k] = ln * (wb * unbd + unb * wbd + zn * pbd);
+  }
+}
+
+template <typename T> __device__ __forceinline__ void store_block(T *dst, const double *v);
+template <> __device__ __forceinline__ void store_block<double>(double *dst, const double *v)
+{
+  double2 *d2 = reinterpret_cast<double2 *>(dst);
+#pragma unroll
+  for (int i = 0; i < 8; i++) d2[i] = make_double2(v[2 * i], v[2 * i + 1]);
+}
+template <> __device__ __forceinline__ void store_block<float>(float *dst, const double *v)
+{
+  float4 *d4 = reinterpret_cast<float4 *>(dst);
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+    d4[i] = make_float4((float)v[4 * i], (float)v[4 * i + 1], (float)v[4 * i + 2], (float)v[4 * i + 3]);
+}
+
+// One matrix row per thread (src/fill.c:150-512): the diagonal block starts
+// at cdt*I and takes v0 (row = n0) or -v1 (row = n1) of every incident edge
+// in edge order; the off-diagonal block of each edge, v1 in row n0 and -v0 in
+// row n1, is written once.  The row's first persistent L slot receives the
+// last lower block the reference's fill would touch (matrix/matrix.cpp:239).
+template <typename T>
+__global__ void __launch_bounds__(128) k_fill(uint32_t N, const uint32_t *__restrict__ inc_ptr,
+                                              const uint32_t *__restrict__ inc_oth,
+                                              const uint32_t *__restrict__ inc_edge,
+                                              const uint32_t *__restrict__ inc_blk,
+                                              const double4 *__restrict__ egeo,
+                                              const double4 *__restrict__ q,
+                                              const double *__restrict__ cdt,
+                                              const uint32_t *__restrict__ diag,
+                                              const uint32_t *__restrict__ last_lower,
+                                              const uint32_t *__restrict__ lpos, T *__restrict__ A,
+                                              double *__restrict__ lslot,
+                                              const uint32_t *__restrict__ bnd_of, double *__restrict__ dscr)
+{
+  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const double4 qs = q[n];
+  double D[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) D[i] = 0.0;
+  const double c = cdt[n];
+  D[0] += c; D[5] += c; D[10] += c; D[15] += c;
+  const uint32_t ll = last_lower[n];
+  const uint32_t k1 = inc_ptr[n + 1];
+  for (uint32_t k = inc_ptr[n]; k < k1; k++) {
+    const uint32_t ev = inc_edge[k];
+    const bool is_n1 = ev >> 31;
+    const double4 geo = egeo[ev & 0x7fffffffu];
+    const double4 qo = q[inc_oth[k]];
+    double v0[16], v1[16], off[16];
+    edge_jacobians(geo, is_n1 ? qo : qs, is_n1 ? qs : qo, v0, v1);
+    if (is_n1) {
+#pragma unroll
+      for (int i = 0; i < 16; i++) { D[i] += -1.0 * v1[i]; off[i] = 0.0 + -1.0 * v0[i]; }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 16; i++) { D[i] += v0[i]; off[i] = 0.0 + v1[i]; }
+    }
+    const uint32_t blk = inc_blk[k];
+    store_block<T>(A + 16 * (size_t)blk, off);
+    if (lslot != nullptr && blk == ll) store_block<double>(lslot + 16 * (size_t)lpos[n], off);
+  }
+  // FP32 form: boundary rows keep their diagonal in double until the wall and
+  // far-field terms are added, so the block is rounded once.
+  const uint32_t bo = bnd_of[n];
+  if (dscr != nullptr && bo != 0xffffffffu) store_block<double>(dscr + 16 * (size_t)bo, D);
+  else store_block<T>(A + 16 * (size_t)diag[n], D);
+}
+
+// Wall (matrix/matrix.cpp:282-296) and far-field (src/fill.c:527-877) terms
+// on the diagonal blocks of boundary nodes, in list order.
+template <typename T>
+__global__ void k_fill_boundary(uint32_t nb, const uint32_t *__restrict__ bnd_node,
+                                const uint32_t *__restrict__ bnd_ptr, const uint32_t *__restrict__ bnd_ent,
+                                const double *__restrict__ s_n, const double *__restrict__ f_n,
+                                const double4 *__restrict__ q, const uint32_t *__restrict__ diag,
+                                T *__restrict__ A, double U, double V, const double *__restrict__ Dsrc)
+{
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const uint32_t n = bnd_node[b];
+  T *dst = A + 16 * (size_t)diag[n];
+  double D[16];
+  // The FP32 form keeps the double diagonal of the row kernel in Dsrc.
+#pragma unroll
+  for (int i = 0; i < 16; i++) D[i] = Dsrc ? Dsrc[16 * (size_t)b + i] : (double)dst[i];
+  for (uint32_t k = bnd_ptr[b]; k < bnd_ptr[b + 1]; k++) {
+    const uint32_t ent = bnd_ent[k], kind = ent >> 29, idx = ent & 0x1fffffffu;
+    if (kind == 1) {
+      D[4] += s_n[3 * idx];
+      D[8] += s_n[3 * idx + 1];
+      D[12] += s_n[3 * idx + 2];
+    } else if (kind == 2) {
+      double v[16];
+      farfield_jacobian(U, V, f_n[3 * idx], f_n[3 * idx + 1], f_n[3 * idx + 2], q[n], v);
+#pragma unroll
+      for (int i = 0; i < 16; i++) D[i] += v[i];
+    }
+  }
+  store_block<T>(dst, D);
+}
+
+// ------------------------------------------------------------------ ILU(0)
+
+// 4x4 inverse of matrix/inverse.cpp:195-355.
+__device__ void inv4(const double *s, double *dst)
+{
+  double d[16];
+  d[0] = s[5] * s[10] * s[15] - s[5] * s[11] * s[14] - s[9] * s[6] * s[15]
+       + s[9] * s[7] * s[14] + s[13] * s[6] * s[11] - s[13] * s[7] * s[10];
+  d[1] = -s[1] * s[10] * s[15] + s[1] * s[11] * s[14] + s[9] * s[2] * s[15]
+       - s[9] * s[3] * s[14] - s[13] * s[2] * s[11] + s[13] * s[3] * s[10];
+  d[2] = s[1] * s[6] * s[15] - s[1] * s[7] * s[14] - s[5] * s[2] * s[15]
+       + s[5] * s[3] * s[14] + s[13] * s[2] * s[7] - s[13] * s[3] * s[6];
+  d[3] = -s[1] * s[6] * s[11] + s[1] * s[7] * s[10] + s[5] * s[2] * s[11]
+       - s[5] * s[3] * s[10] - s[9] * s[2] * s[7] + s[9] * s[3] * s[6];
+  d[4] = -s[4] * s[10] * s[15] + s[4] * s[11] * s[14] + s[8] * s[6] * s[15]
+       - s[8] * s[7] * s[14] - s[12] * s[6] * s[11] + s[12] * s[7] * s[10];
+  d[5] = s[0] * s[10] * s[15] - s[0] * s[11] * s[14] - s[8] * s[2] * s[15]
+       + s[8] * s[3] * s[14] + s[12] * s[2] * s[11] - s[12] * s[3] * s[10];
+  d[6] = -s[0] * s[6] * s[15] + s[0] * s[7] * s[14] + s[4] * s[2] * s[15]
+       - s[4] * s[3] * s[14] - s[12] * s[2] * s[7] + s[12] * s[3] * s[6];
+  d[7] = s[0] * s[6] * s[11] - s[0] * s[7] * s[10] - s[4] * s[2] * s[11]
+       + s[4] * s[3] * s[10] + s[8] * s[2] * s[7] - s[8] * s[3] * s[6];
+  d[8] = s[4] * s[9] * s[15] - s[4] * s[11] * s[13] - s[8] * s[5] * s[15]
+       + s[8] * s[7] * s[13] + s[12] * s[5] * s[11] - s[12] * s[7] * s[9];
+  d[9] = -s[0] * s[9] * s[15] + s[0] * s[11] * s[13] + s[8] * s[1] * s[15]
+       - s[8] * s[3] * s[13] - s[12] * s[1] * s[11] + s[12] * s[3] * s[9];
+  d[10] = s[0] * s[5] * s[15] - s[0] * s[7] * s[13] - s[4] * s[1] * s[15]
+        + s[4] * s[3] * s[13] + s[12] * s[1] * s[7] - s[12] * s[3] * s[5];
+  d[11] = -s[0] * s[5] * s[11] + s[0] * s[7] * s[9] + s[4] * s[1] * s[11]
+        - s[4] * s[3] * s[9] - s[8] * s[1] * s[7] + s[8] * s[3] * s[5];
+  d[12] = -s[4] * s[9] * s[14] + s[4] * s[10] * s[13] + s[8] * s[5] * s[14]
+        - s[8] * s[6] * s[13] - s[12] * s[5] * s[10] + s[12] * s[6] * s[9];
+  d[13] = s[0] * s[9] * s[14] - s[0] * s[10] * s[13] - s[8] * s[1] * s[14]
+        + s[8] * s[2] * s[13] + s[12] * s[1] * s[10] - s[12] * s[2] * s[9];
+  d[14] = -s[0] * s[5] * s[14] + s[0] * s[6] * s[13] + s[4] * s[1] * s[14]
+        - s[4] * s[2] * s[13] - s[12] * s[1] * s[6] + s[12] * s[2] * s[5];
+  d[15] = s[0] * s[5] * s[10] - s[0] * s[6] * s[9] - s[4] * s[1] * s[10]
+        + s[4] * s[2] * s[9] + s[8] * s[1] * s[6] - s[8] * s[2] * s[5];
+  double det = s[0] * d[0] + s[1] * d[4] + s[2] * d[8] + s[3] * d[12];
+  det = 1.0 / det;
+#pragma unroll
+  for (int k = 0; k < 16; k++) dst[k] = d[k] * det;
+}
+
+// Product of two 4x4 blocks held one entry per lane of a 16-lane group
+// (lane l = 4*row + col); entry (r,c) = sum over t of a(r,t) b(t,c), summed
+// from zero in t order (matrix/init.cpp:105-116).
+__device__ __forceinline__ double gemm_lane(double a, double b, int lane16, unsigned mask, int base)
+{
+  const int r = lane16 >> 2, c = lane16 & 3;
+  double s = 0.0;
+#pragma unroll
+  for (int t = 0; t < 4; t++) {
+    const double at = __shfl_sync(mask, a, base + 4 * r + t);
+    const double bt = __shfl_sync(mask, b, base + 4 * t + c);
+    s += at * bt;
+  }
+  return s;
+}
+
+// One level of the ILU(0) sweep of matrix/ilu.cpp:49-97, 16 lanes per row.
+// For block (i,k) the lanes walk row i's lower columns plus the diagonal
+// against column k of U (row k's lower columns plus k, through tblk),
+// subtracting L(i,m) U(m,k) for every common m; the last product is added back
+// (ilu.cpp:86).  Its L(i,k) factor is the row's persistent slot, the U(i,k)
+// factor the not yet updated block, as in the reference.  Lower blocks are
+// then multiplied by inv(U(k,k)) and stored in lslot; upper blocks are
+// updated in place; the diagonal's inverse goes to dinv.
+__global__ void __launch_bounds__(128) k_ilu_level(uint32_t nrows, const uint32_t *__restrict__ rows,
+                                                   const uint32_t *__restrict__ ia,
+                                                   const uint32_t *__restrict__ ja,
+                                                   const uint32_t *__restrict__ diag,
+                                                   const uint32_t *__restrict__ tblk,
+                                                   const uint32_t *__restrict__ lpos, double *__restrict__ A,
+                                                   double *__restrict__ lslot, double *__restrict__ dinv,
+                                                   int *__restrict__ status)
+{
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t grp = gid >> 4;
+  const int lane = threadIdx.x & 31, l16 = lane & 15, base = lane & 16;
+  const unsigned mask = 0xffffu << base;
+  if (grp >= nrows) return;   // both halves of a warp exit together or stay
+  const uint32_t i = rows[grp];
+  const uint32_t j0 = ia[i], jd = diag[i], j1 = ia[i + 1];
+  const double ident = ((l16 >> 2) == (l16 & 3)) ? 1.0 : 0.0;
+  for (uint32_t j = j0; j < j1; j++) {
+    const uint32_t k = ja[j];
+    double a = A[16 * (size_t)j + l16];
+    double d = 0.0;
+    // merge L row i (columns ja[j0..jd]) with U column k (rows ja[ia[k]..diag[k]])
+    uint32_t pl = j0, pu = ia[k];
+    const uint32_t pu_end = diag[k];
+    while (pl <= jd && pu <= pu_end) {
+      const uint32_t cl = ja[pl], cu = ja[pu];
+      if (cl == cu) {
+        const double lv = (cl == i) ? ident : lslot[16 * (size_t)(lpos[i] + (pl - j0)) + l16];
+        const double uv = A[16 * (size_t)tblk[pu] + l16];
+        d = gemm_lane(lv, uv, l16, mask, base);
+        a = -1.0 * d + a;
+      }
+      if (cl <= cu) pl++;
+      if (cl >= cu) pu++;
+    }
+    a = 1.0 * d + a;
+    if (k < i) {
+      const double dk = dinv[16 * (size_t)k + l16];
+      const double lv = gemm_lane(a, dk, l16, mask, base);
+      lslot[16 * (size_t)(lpos[i] + (j - j0)) + l16] = lv;
+    } else {
+      A[16 * (size_t)j + l16] = a;
+      if (k == i) {
+        __syncwarp(mask);
+        if (l16 == 0) {
+          double s[16], o[16];
+          for (int t = 0; t < 16; t++) s[t] = A[16 * (size_t)j + t];
+          inv4(s, o);
+          bool bad = false;
+          for (int t = 0; t < 16; t++) {
+            dinv[16 * (size_t)i + t] = o[t];
+            bad |= !isfinite(o[t]);
+          }
+          if (bad) atomicExch(status, KFUN3D_ERR_PIVOT);
+        }
+        __syncwarp(mask);
+      }
+    }
+  }
+}
+
+// matrix/ilu.cpp:115-136: the factor over A, lower blocks from the L slots,
+// diagonal blocks inverted.
+__global__ void k_ilu_finish(uint32_t N, const uint32_t *__restrict__ ia, const uint32_t *__restrict__ diag,
+                             const uint32_t *__restrict__ lpos, const double *__restrict__ lslot,
+                             const double *__restrict__ dinv, double *__restrict__ A)
+{
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t i = gid >> 4, l = gid & 15;
+  if (i >= N) return;
+  const uint32_t j0 = ia[i], jd = diag[i];
+  for (uint32_t j = j0; j < jd; j++) A[16 * (size_t)j + l] = lslot[16 * (size_t)(lpos[i] + (j - j0)) + l];
+  A[16 * (size_t)jd + l] = dinv[16 * (size_t)i + l];
+}
+
+// FP32 form: plain block ILU(0) in natural order on float blocks (no
+// persistent slots); L(i,k) = (A(i,k) - sum L(i,m) U(m,k)) inv(U(k,k)),
+// U(i,k) = A(i,k) - sum L(i,m) U(m,k), inverses formed in double and rounded.
+__device__ __forceinline__ float gemm_lane_f(float a, float b, int lane16, unsigned mask, int base)
+{
+  const int r = lane16 >> 2, c = lane16 & 3;
+  float s = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 4; t++) s += __shfl_sync(mask, a, base + 4 * r + t) * __shfl_sync(mask, b, base + 4 * t + c);
+  return s;
+}
+
+__global__ void __launch_bounds__(128) k_ilu_level_f32(uint32_t nrows, const uint32_t *__restrict__ rows,
+                                                       const uint32_t *__restrict__ ia,
+                                                       const uint32_t *__restrict__ ja,
+                                                       const uint32_t *__restrict__ diag,
+                                                       const uint32_t *__restrict__ tblk, float *__restrict__ A,
+                                                       float *__restrict__ dinv, int *__restrict__ status)
+{
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t grp = gid >> 4;
+  const int lane = threadIdx.x & 31, l16 = lane & 15, base = lane & 16;
+  const unsigned mask = 0xffffu << base;
+  if (grp >= nrows) return;
+  const uint32_t i = rows[grp];
+  const uint32_t j0 = ia[i], jd = diag[i], j1 = ia[i + 1];
+  for (uint32_t j = j0; j < j1; j++) {
+    const uint32_t k = ja[j];
+    float a = A[16 * (size_t)j + l16];
+    // sum over m < min(i,k): row i's lower columns against U(m,k)
+    uint32_t pl = j0, pu = ia[k];
+    const uint32_t pu_end = diag[k];
+    while (pl < jd && pu < pu_end) {
+      const uint32_t cl = ja[pl], cu = ja[pu];
+      if (cl == cu) {
+        const float lv = A[16 * (size_t)pl + l16];
+        const float uv = A[16 * (size_t)tblk[pu] + l16];
+        a -= gemm_lane_f(lv, uv, l16, mask, base);
+      }
+      if (cl <= cu) pl++;
+      if (cl >= cu) pu++;
+    }
+    if (k < i) {
+      A[16 * (size_t)j + l16] = gemm_lane_f(a, dinv[16 * (size_t)k + l16], l16, mask, base);
+    } else {
+      A[16 * (size_t)j + l16] = a;
+      if (k == i) {
+        __syncwarp(mask);
+        if (l16 == 0) {
+          double s[16], o[16];
+          for (int t = 0; t < 16; t++) s[t] = A[16 * (size_t)j + t];
+          inv4(s, o);
+          bool bad = false;
+          for (int t = 0; t < 16; t++) {
+            dinv[16 * (size_t)i + t] = (float)o[t];
+            bad |= !isfinite(o[t]);
+          }
+          if (bad) atomicExch(status, KFUN3D_ERR_PIVOT);
+        }
+        __syncwarp(mask);
+      }
+    }
+  }
+}
+
+__global__ void k_ilu_finish_f32(uint32_t N, const uint32_t *__restrict__ diag, const float *__restrict__ dinv,
+                                 float *__restrict__ A)
+{
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t i = gid >> 4, l = gid & 15;
+  if (i >= N) return;
+  A[16 * (size_t)diag[i] + l] = dinv[16 * (size_t)i + l];
+}
+
+// ------------------------------------------------------------------ SpTRSV
+
+// Forward level of matrix/sptrsv.cpp:173-189, 4 lanes per row (lane = block
+// row): x_r = b_r - sum over lower blocks of A x, each block product summed
+// from zero in column order, then subtracted, in column order.
+template <typename T>
+__global__ void __launch_bounds__(128) k_trsv_lower(uint32_t nrows, const uint32_t *__restrict__ rows,
+                                                    const uint32_t *__restrict__ ia,
+                                                    const uint32_t *__restrict__ ja,
+                                                    const uint32_t *__restrict__ diag, const T *__restrict__ A,
+                                                    const double *__restrict__ b, double *__restrict__ x)
+{
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t g = gid >> 2, rr = gid & 3;
+  if (g >= nrows) return;
+  const uint32_t i = rows[g];
+  double xi = b[4 * (size_t)i + rr];
+  const uint32_t jd = diag[i];
+  for (uint32_t j = ia[i]; j < jd; j++) {
+    const T *blk = A + 16 * (size_t)j + 4 * rr;
+    const double4 xc = reinterpret_cast<const double4 *>(x)[ja[j]];
+    double t = 0.0;
+    t += (double)blk[0] * xc.x;
+    t += (double)blk[1] * xc.y;
+    t += (double)blk[2] * xc.z;
+    t += (double)blk[3] * xc.w;
+    xi = -1.0 * t + xi;
+  }
+  x[4 * (size_t)i + rr] = xi;
+}
+
+// Backward level of matrix/sptrsv.cpp:191-209: x_r -= sum over upper blocks,
+// then x_r = inv(U_rr) x_r.
+template <typename T>
+__global__ void __launch_bounds__(128) k_trsv_upper(uint32_t nrows, const uint32_t *__restrict__ rows,
+                                                    const uint32_t *__restrict__ ia,
+                                                    const uint32_t *__restrict__ ja,
+                                                    const uint32_t *__restrict__ diag, const T *__restrict__ A,
+                                                    double *__restrict__ x)
+{
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t g = gid >> 2, rr = gid & 3;
+  const unsigned mask = 0xfu << (threadIdx.x & 28);
+  if (g >= nrows) return;
+  const uint32_t i = rows[g];
+  double xi = x[4 * (size_t)i + rr];
+  const uint32_t jd = diag[i], j1 = ia[i + 1];
+  for (uint32_t j = jd + 1; j < j1; j++) {
+    const T *blk = A + 16 * (size_t)j + 4 * rr;
+    const double4 xc = reinterpret_cast<const double4 *>(x)[ja[j]];
+    double t = 0.0;
+    t += (double)blk[0] * xc.x;
+    t += (double)blk[1] * xc.y;
+    t += (double)blk[2] * xc.z;
+    t += (double)blk[3] * xc.w;
+    xi = -1.0 * t + xi;
+  }
+  const int b4 = threadIdx.x & 28;
+  const double x0 = __shfl_sync(mask, xi, b4 + 0), x1 = __shfl_sync(mask, xi, b4 + 1);
+  const double x2 = __shfl_sync(mask, xi, b4 + 2), x3 = __shfl_sync(mask, xi, b4 + 3);
+  const T *dblk = A + 16 * (size_t)jd + 4 * rr;
+  double t = 0.0;
+  t += (double)dblk[0] * x0;
+  t += (double)dblk[1] * x1;
+  t += (double)dblk[2] * x2;
+  t += (double)dblk[3] * x3;
+  x[4 * (size_t)i + rr] = t;
+}
+
+// ------------------------------------------------------------------ J.v
+
+// src/kernel.c:35-44: y = (y - r + cdt (w - q)) * a, a = |x| / h from the
+// device scalars (scal[ia] = |x|, scal[ia+1] = h).
+__global__ void k_jv_combine(uint32_t N, double *__restrict__ y, const double *__restrict__ r,
+                             const double *__restrict__ w, const double *__restrict__ q,
+                             const double *__restrict__ cdt, const double *__restrict__ scal, int ia)
+{
+  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const double a = scal[ia] / scal[ia + 1];
+  const double c = cdt[n];
+  const double4 yy = reinterpret_cast<double4 *>(y)[n];
+  const double4 rr = reinterpret_cast<const double4 *>(r)[n];
+  const double4 ww = reinterpret_cast<const double4 *>(w)[n];
+  const double4 qq = reinterpret_cast<const double4 *>(q)[n];
+  double4 o;
+  o.x = (yy.x - rr.x + c * (ww.x - qq.x)) * a;
+  o.y = (yy.y - rr.y + c * (ww.y - qq.y)) * a;
+  o.z = (yy.z - rr.z + c * (ww.z - qq.z)) * a;
+  o.w = (yy.w - rr.w + c * (ww.w - qq.w)) * a;
+  reinterpret_cast<double4 *>(y)[n] = o;
+}
+
+// ------------------------------------------------------------------ launchers
+
+inline unsigned blocks(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+void gradient(DevMesh &m, const double *q)
+{
+  k_gradient<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_w, 2 * m.E,
+                                                      (const double4 *)q, (double4 *)m.gx,
+                                                      (double4 *)m.gy, (double4 *)m.gz);
+  kf_count_launch();
+}
+
+void residual(DevMesh &m, const double *q, double *r, int first_order, double u, double v)
+{
+  if (first_order)
+    k_residual<true><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo, m.xyz,
+                                                            (const double4 *)q, nullptr, nullptr, nullptr,
+                                                            (double4 *)r);
+  else
+    k_residual<false><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo, m.xyz,
+                                                             (const double4 *)q, (const double4 *)m.gx,
+                                                             (const double4 *)m.gy, (const double4 *)m.gz,
+                                                             (double4 *)r);
+  kf_count_launch();
+  if (m.nb) {
+    k_residual_boundary<<<blocks(m.nb, 64), 64, 0, m.stream>>>(m.nb, m.bnd_node, m.bnd_ptr, m.bnd_ent, m.wf_nodes,
+                                                               m.wf_n, m.f_n, (const double4 *)q, (double4 *)r, u, v);
+    kf_count_launch();
+  }
+}
+
+void timestep(DevMesh &m, const double *q, double cfl)
+{
+  k_timestep<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo,
+                                                      (const double4 *)q, m.bnd_of, cfl, m.cdt);
+  kf_count_launch();
+  if (m.nb) {
+    k_timestep_boundary<<<blocks(m.nb, 64), 64, 0, m.stream>>>(m.nb, m.bnd_node, m.bnd_ptr, m.bnd_ent, m.s_n,
+                                                               m.f_n, (const double4 *)q, cfl, m.cdt);
+    kf_count_launch();
+  }
+}
+
+void fill(DevMesh &m, const double *q, double u, double v, int precision)
+{
+  if (precision == 0) {
+    k_fill<double><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_edge, m.inc_blk, m.egeo,
+                                                          (const double4 *)q, m.cdt, m.diag, m.last_lower,
+                                                          m.lpos, m.A, m.lslot, m.bnd_of, nullptr);
+    kf_count_launch();
+    if (m.nb) {
+      k_fill_boundary<double><<<blocks(m.nb, 64), 64, 0, m.stream>>>(m.nb, m.bnd_node, m.bnd_ptr, m.bnd_ent, m.s_n,
+                                                                     m.f_n, (const double4 *)q, m.diag, m.A, u, v,
+                                                                     nullptr);
+      kf_count_launch();
+    }
+  } else {
+    k_fill<float><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_edge, m.inc_blk, m.egeo,
+                                                         (const double4 *)q, m.cdt, m.diag, m.last_lower, m.lpos,
+                                                         m.Af, nullptr, m.bnd_of, m.dscr);
+    kf_count_launch();
+    if (m.nb) {
+      k_fill_boundary<float><<<blocks(m.nb, 64), 64, 0, m.stream>>>(m.nb, m.bnd_node, m.bnd_ptr, m.bnd_ent, m.s_n,
+                                                                    m.f_n, (const double4 *)q, m.diag, m.Af, u, v,
+                                                                    m.dscr);
+      kf_count_launch();
+    }
+  }
+}
+
+void ilu(DevMesh &m, int precision)
+{
+  int *status = m.status;
+  for (uint32_t l = 0; l < m.nlev_l; l++) {
+    const uint32_t r0 = m.lev_l_ptr[l], nr = m.lev_l_ptr[l + 1] - r0;
+    if (precision == 0)
+      k_ilu_level<<<blocks((size_t)nr * 16, 128), 128, 0, m.stream>>>(nr, m.lev_l + r0, m.ia, m.ja, m.diag, m.tblk,
+                                                                      m.lpos, m.A, m.lslot, m.dinv, status);
+    else
+      k_ilu_level_f32<<<blocks((size_t)nr * 16, 128), 128, 0, m.stream>>>(nr, m.lev_l + r0, m.ia, m.ja, m.diag,
+                                                                          m.tblk, m.Af, m.dinvf, status);
+    kf_count_launch();
+  }
+  if (precision == 0)
+    k_ilu_finish<<<blocks((size_t)m.N * 16, 256), 256, 0, m.stream>>>(m.N, m.ia, m.diag, m.lpos, m.lslot, m.dinv, m.A);
+  else
+    k_ilu_finish_f32<<<blocks((size_t)m.N * 16, 256), 256, 0, m.stream>>>(m.N, m.diag, m.dinvf, m.Af);
+  kf_count_launch();
+}
+
+void sptrsv(DevMesh &m, const double *b, double *x, int precision)
+{
+  for (uint32_t l = 0; l < m.nlev_l; l++) {
+    const uint32_t r0 = m.lev_l_ptr[l], nr = m.lev_l_ptr[l + 1] - r0;
+    if (precision == 0)
+      k_trsv_lower<double><<<blocks((size_t)nr * 4, 128), 128, 0, m.stream>>>(nr, m.lev_l + r0, m.ia, m.ja, m.diag,
+                                                                             m.A, b, x);
+    else
+      k_trsv_lower<float><<<blocks((size_t)nr * 4, 128), 128, 0, m.stream>>>(nr, m.lev_l + r0, m.ia, m.ja, m.diag,
+                                                                            m.Af, b, x);
+    kf_count_launch();
+  }
+  for (uint32_t l = 0; l < m.nlev_u; l++) {
+    const uint32_t r0 = m.lev_u_ptr[l], nr = m.lev_u_ptr[l + 1] - r0;
+    if (precision == 0)
+      k_trsv_upper<double><<<blocks((size_t)nr * 4, 128), 128, 0, m.stream>>>(nr, m.lev_u + r0, m.ia, m.ja, m.diag,
+                                                                             m.A, x);
+    else
+      k_trsv_upper<float><<<blocks((size_t)nr * 4, 128), 128, 0, m.stream>>>(nr, m.lev_u + r0, m.ia, m.ja, m.diag,
+                                                                            m.Af, x);
+    kf_count_launch();
+  }
+}
+
+void jv_combine(DevMesh &m, double *y, const double *r, const double *w, const double *q, const double *scal, int ia)
+{
+  k_jv_combine<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, y, r, w, q, m.cdt, scal, ia);
+  kf_count_launch();
+}
+
+}  // namespace KF_NS

@@ -1,0 +1,776 @@
+// kfun3d_b200: BLAS-1 reductions, wall forces, the reference's C entry points
+// and the device-resident pseudo-transient Newton / GMRES(30) driver.
+//
+// Compiled with -fmad=false: in exact mode every reduction sums in index
+// order (as the reference at one OpenMP thread) and every scalar update keeps
+// its operation order; fast mode uses explicit fma() and fixed-shape tree
+// reductions (deterministic run to run).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+extern int g_kf_verbose;
+
+namespace {
+
+constexpr double JV_EPS = 1.490116119384766e-08;   // src/kernel.c:12
+constexpr int RED_BLOCKS = 296;                    // 2 x 148 SMs
+constexpr int S_XN = 40, S_H = 41, S_QN = 42, S_FN = 43, S_T0 = 44;
+
+inline unsigned nblk(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// ------------------------------------------------------------------ reductions
+
+// Sum of a[i]*b[i] in index order (src/utils.c:53-67, src/kernel.c:131-134):
+// one warp loads 32 products at a time and every lane adds them in order.
+__global__ void k_dot_seq(size_t n, const double *__restrict__ a, const double *__restrict__ b,
+                          double *__restrict__ out, int op)
+{
+  const int lane = threadIdx.x;
+  double s = 0.0;
+  for (size_t base = 0; base < n; base += 32) {
+    const size_t i = base + lane;
+    const double p = (i < n) ? a[i] * b[i] : 0.0;
+    const int cnt = (n - base) < 32 ? (int)(n - base) : 32;
+    for (int l = 0; l < cnt; l++) s += __shfl_sync(0xffffffffu, p, l);
+  }
+  if (lane == 0) {
+    if (op == 0) *out = s;
+    else if (op == 1) *out = sqrt(s);
+    else *out = sqrt(1.0 + sqrt(s));   // src/kernel.c:95
+  }
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Fast form: fixed grid, fixed tree, so the result is run-to-run identical.
+__global__ void __launch_bounds__(256) k_dot_partial(size_t n, const double *__restrict__ a,
+                                                     const double *__restrict__ b, double *__restrict__ part)
+{
+  __shared__ double sm[8];
+  double s = 0.0;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t n2 = n / 2;
+  const double2 *a2 = reinterpret_cast<const double2 *>(a), *b2 = reinterpret_cast<const double2 *>(b);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += stride) {
+    const double2 x = a2[i], y = b2[i];
+    s = fma(x.x, y.x, s);
+    s = fma(x.y, y.y, s);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && (n & 1)) s = fma(a[n - 1], b[n - 1], s);
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < 8 ? sm[threadIdx.x] : 0.0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) part[blockIdx.x] = v;
+  }
+}
+
+__global__ void k_dot_final(const double *__restrict__ part, int np, double *__restrict__ out, int op)
+{
+  __shared__ double sm[8];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) s += part[i];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += sm[w];
+    if (op == 0) *out = v;
+    else if (op == 1) *out = sqrt(v);
+    else *out = sqrt(1.0 + sqrt(v));
+  }
+}
+
+// y = (mult * coef[0]) * x + y with the coefficient on the device
+__global__ void k_axpy_dev(size_t n, const double *__restrict__ coef, double mult, const double *__restrict__ x,
+                           double *__restrict__ y, int fast)
+{
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a = mult * coef[0];
+  y[i] = fast ? fma(a, x[i], y[i]) : a * x[i] + y[i];
+}
+
+// y = a x + y (src/utils.c:69-87)
+__global__ void k_axpy(size_t n, double a, const double *__restrict__ x, double *__restrict__ y, int fast)
+{
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  y[i] = fast ? fma(a, x[i], y[i]) : a * x[i] + y[i];
+}
+
+// w = a x + y (src/utils.c:89-107)
+__global__ void k_waxpy(size_t n, double a, const double *__restrict__ x, const double *__restrict__ y,
+                        double *__restrict__ w, int fast)
+{
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  w[i] = fast ? fma(a, x[i], y[i]) : a * x[i] + y[i];
+}
+
+// x *= 1/|x| with |x| on the device (src/utils.c:109-122)
+__global__ void k_scale_inv(size_t n, const double *__restrict__ nrm, double *__restrict__ x)
+{
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] *= (1.0 / nrm[0]);
+}
+
+// J.v set-up, src/kernel.c:27-30: h = eps * qnorm; w = (h/|x|) x + q
+__global__ void k_jv_shift(size_t n, const double *__restrict__ scal, const double *__restrict__ x,
+                           const double *__restrict__ q, double *__restrict__ w, int fast)
+{
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double h = JV_EPS * scal[S_QN];
+  const double a = h / scal[S_XN];
+  w[i] = fast ? fma(a, x[i], q[i]) : a * x[i] + q[i];
+}
+
+__global__ void k_set_h(double *scal)
+{
+  scal[S_H] = JV_EPS * scal[S_QN];
+}
+
+// src/forces.c:8-120 in the reference's order: per colour an OpenMP
+// reduction from zero, added to the running total.
+__global__ void k_forces(uint32_t ncol, const uint32_t *__restrict__ col, const uint32_t *__restrict__ wf,
+                         const double4 *__restrict__ xyz, const double4 *__restrict__ q, double U, double V,
+                         double *__restrict__ out)
+{
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double lift = 0.0, drag = 0.0, momn = 0.0;
+  for (uint32_t c = 0; c < ncol; c++) {
+    double l = 0.0, d = 0.0, m = 0.0;
+    for (uint32_t j = col[c]; j < col[c + 1]; j++) {
+      const uint32_t a = wf[3 * j], b = wf[3 * j + 1], e = wf[3 * j + 2];
+      const double4 pa = xyz[a], pb = xyz[b], pe = xyz[e];
+      const double ax = pb.x - pa.x, ay = pb.y - pa.y, az = pb.z - pa.z;
+      const double bx = pe.x - pa.x, by = pe.y - pa.y, bz = pe.z - pa.z;
+      double xnorm = ay * bz; xnorm -= az * by; xnorm = -0.5 * xnorm;
+      double ynorm = ax * bz; ynorm -= az * bx; ynorm = 0.5 * ynorm;
+      const double press = (q[a].x + q[b].x + q[e].x) / 3.0;
+      const double cp = 2.0 * (press - 1.0);
+      const double dcx = cp * xnorm, dcy = cp * ynorm;
+      const double xmid = pa.x + pb.x + pe.x;
+      const double ymid = pa.y + pb.y + pe.y;
+      l = l - dcx * V + dcy * U;
+      d = d + dcx * U + dcy * V;
+      m = m + (xmid - 0.25) * dcy - ymid * dcx;
+    }
+    lift += l;
+    drag += d;
+    momn += m;
+  }
+  out[0] = lift;
+  out[1] = drag;
+  out[2] = momn;
+}
+
+// ------------------------------------------------------------------ helpers
+
+bool check_cuda(const char *what)
+{
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    std::string s = std::string(what) + ": " + cudaGetErrorString(e);
+    kf_set_error(KFUN3D_ERR_CUDA, s.c_str());
+    return false;
+  }
+  return true;
+}
+
+#define CK(call)                                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      std::string s_ = std::string(#call) + ": " + cudaGetErrorString(e_);        \
+      kf_set_error(KFUN3D_ERR_CUDA, s_.c_str());                                   \
+    }                                                                              \
+  } while (0)
+
+// Kernel set of the current arithmetic mode.
+struct Ops {
+  bool fast;
+  void gradient(DevMesh &m, const double *q) const { fast ? kf_fast::gradient(m, q) : kf_exact::gradient(m, q); }
+  void residual(DevMesh &m, const double *q, double *r, int fo, double u, double v) const
+  {
+    fast ? kf_fast::residual(m, q, r, fo, u, v) : kf_exact::residual(m, q, r, fo, u, v);
+  }
+  void timestep(DevMesh &m, const double *q, double cfl) const
+  {
+    fast ? kf_fast::timestep(m, q, cfl) : kf_exact::timestep(m, q, cfl);
+  }
+  void fill(DevMesh &m, const double *q, double u, double v, int p) const
+  {
+    fast ? kf_fast::fill(m, q, u, v, p) : kf_exact::fill(m, q, u, v, p);
+  }
+  void ilu(DevMesh &m, int p) const { fast ? kf_fast::ilu(m, p) : kf_exact::ilu(m, p); }
+  void sptrsv(DevMesh &m, const double *b, double *x, int p) const
+  {
+    fast ? kf_fast::sptrsv(m, b, x, p) : kf_exact::sptrsv(m, b, x, p);
+  }
+  void jv_combine(DevMesh &m, double *y, const double *r, const double *w, const double *q) const
+  {
+    fast ? kf_fast::jv_combine(m, y, r, w, q, m.scal, S_XN) : kf_exact::jv_combine(m, y, r, w, q, m.scal, S_XN);
+  }
+};
+
+Ops ops() { return Ops{kf_mode() == KFUN3D_MODE_FAST}; }
+
+// dot / norm into a device scalar: op 0 = sum, 1 = sqrt(sum), 2 = sqrt(1 + sqrt(sum))
+void dev_reduce(DevMesh &m, const double *a, const double *b, double *out, int op, bool fast)
+{
+  const size_t n = 4 * (size_t)m.N;
+  if (fast) {
+    k_dot_partial<<<RED_BLOCKS, 256, 0, m.stream>>>(n, a, b, m.red);
+    k_dot_final<<<1, 256, 0, m.stream>>>(m.red, RED_BLOCKS, out, op);
+    kf_count_launch(2);
+  } else {
+    k_dot_seq<<<1, 32, 0, m.stream>>>(n, a, b, out, op);
+    kf_count_launch();
+  }
+}
+
+void fetch(DevMesh &m, int first, int count)
+{
+  CK(cudaMemcpyAsync(m.h_scal + first, m.scal + first, count * sizeof(double), cudaMemcpyDeviceToHost, m.stream));
+  CK(cudaStreamSynchronize(m.stream));
+}
+
+// Residual of state q into r (gradient first unless first order).
+void dev_residual(DevMesh &m, const Ops &o, const double *q, double *r)
+{
+  double u, v;
+  kfun3d_get_freestream(&u, &v);
+  const int fo = kf_first_order();
+  if (!fo) o.gradient(m, q);
+  o.residual(m, q, r, fo, u, v);
+}
+
+// iJacVec, src/kernel.c:24-45: y = (F(q + h x/|x|) - r + cdt (w - q)) |x| / h
+void dev_jacvec(DevMesh &m, const Ops &o, const double *x, double *y)
+{
+  const size_t n = 4 * (size_t)m.N;
+  dev_reduce(m, x, x, m.scal + S_XN, 1, o.fast);
+  k_set_h<<<1, 1, 0, m.stream>>>(m.scal);
+  k_jv_shift<<<nblk(n, 256), 256, 0, m.stream>>>(n, m.scal, x, m.q, m.w, o.fast);
+  kf_count_launch(2);
+  dev_residual(m, o, m.w, y);
+  o.jv_combine(m, y, m.r, m.w, m.q);
+}
+
+void dev_axpy(DevMesh &m, double a, const double *x, double *y, bool fast)
+{
+  const size_t n = 4 * (size_t)m.N;
+  k_axpy<<<nblk(n, 256), 256, 0, m.stream>>>(n, a, x, y, fast);
+  kf_count_launch();
+}
+
+double *Vb(DevMesh &m, int k) { return m.V + (size_t)k * 4 * m.N; }
+
+void dev_normalize(DevMesh &m, double *x, double *nrm, bool fast)
+{
+  const size_t n = 4 * (size_t)m.N;
+  dev_reduce(m, x, x, nrm, 1, fast);
+  k_scale_inv<<<nblk(n, 256), 256, 0, m.stream>>>(n, nrm, x);
+  kf_count_launch();
+}
+
+// One Arnoldi step k (src/kernel.c:123-141): V[k+1] = M^-1 J V[k],
+// modified Gram-Schmidt against V[0..k], normalised; h in scal[0..k+1].
+void arnoldi_step(DevMesh &m, const Ops &o, int k, int prec)
+{
+  const size_t n = 4 * (size_t)m.N;
+  dev_jacvec(m, o, Vb(m, k), m.t);
+  o.sptrsv(m, m.t, Vb(m, k + 1), prec);
+  for (int v = 0; v <= k; v++) {
+    dev_reduce(m, Vb(m, k + 1), Vb(m, v), m.scal + v, 0, o.fast);
+    k_axpy_dev<<<nblk(n, 256), 256, 0, m.stream>>>(n, m.scal + v, -1.0, Vb(m, v), Vb(m, k + 1), o.fast);
+    kf_count_launch();
+  }
+  dev_normalize(m, Vb(m, k + 1), m.scal + k + 1, o.fast);
+}
+
+int device_status(DevMesh &m)
+{
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, m.status, sizeof(int), cudaMemcpyDeviceToHost, m.stream));
+  CK(cudaStreamSynchronize(m.stream));
+  if (st) {
+    CK(cudaMemsetAsync(m.status, 0, sizeof(int), m.stream));
+  }
+  return st;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ solve
+
+extern "C" void kfun3d_default_params(kfun3d_solver_params *p)
+{
+  p->ts_max = 15;
+  p->stop_ratio = 10000000.0;
+  p->gmres_rtol = 0.01;
+  p->gmres_restart = 30;
+  p->gmres_max_it = 10000;
+  p->cfl_init = 50.0;
+  p->cfl_max = 100000.0;
+}
+
+// The device-resident solve of src/kernel.c:47-232 (parameters as data).
+// The state stays on the device; the host keeps the small GMRES scalars and
+// reads one column of the Hessenberg matrix per Arnoldi step.
+static int solve_device(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_params *p, kfun3d_step *hist,
+                        int max_hist, bool print)
+{
+  const Ops o = ops();
+  const int prec = kf_precision();
+  const size_t n = 4 * (size_t)m.N;
+  const int restart = std::min(std::max(p->gmres_restart, 1), 30);
+  double u, v;
+  kfun3d_get_freestream(&u, &v);
+  double ghh[KF_NBASIS * (KF_NBASIS + 1)] = {0};
+  double cs[KF_NBASIS], sn[KF_NBASIS], rs[KF_NBASIS];
+  double fnorm0 = 0.0, cfl = p->cfl_init;
+  int nrec = 0, steps = 0;
+  cudaEvent_t ev0, ev1;
+  CK(cudaEventCreate(&ev0));
+  CK(cudaEventCreate(&ev1));
+  for (int its = 0; its < p->ts_max; its++) {
+    CK(cudaEventRecord(ev0, m.stream));
+    dev_residual(m, o, m.q, m.r);
+    dev_reduce(m, m.r, m.r, m.scal + S_FN, 1, o.fast);
+    fetch(m, S_FN, 1);
+    const double fnorm = m.h_scal[S_FN];
+    if (!std::isfinite(fnorm)) {
+      kf_set_error(KFUN3D_ERR_NONFINITE, "residual norm is not finite");
+      steps = -1;
+      break;
+    }
+    if (its == 0) fnorm0 = fnorm;
+    else {
+      double cfl0 = 1.1 * p->cfl_init * fnorm0;   // src/kernel.c:86-88
+      cfl0 /= fnorm;
+      cfl = (cfl0 < p->cfl_max) ? cfl0 : p->cfl_max;
+    }
+    o.timestep(m, m.q, cfl);
+    o.fill(m, m.q, u, v, prec);
+    dev_reduce(m, m.q, m.q, m.scal + S_QN, 2, o.fast);
+    CK(cudaMemsetAsync(m.x, 0, n * sizeof(double), m.stream));
+    o.ilu(m, prec);
+    o.sptrsv(m, m.r, Vb(m, 0), prec);
+    if (device_status(m) == KFUN3D_ERR_PIVOT) {
+      kf_set_error(KFUN3D_ERR_PIVOT, "singular or non-finite pivot block in ILU(0)");
+      steps = -1;
+      break;
+    }
+
+    double tol = 0.0;
+    unsigned int total = 0;
+    bool done = false;
+    while (total <= (unsigned)p->gmres_max_it) {     // src/kernel.c:107-196
+      if (total > 0) {
+        dev_jacvec(m, o, m.x, m.t);
+        k_waxpy<<<nblk(n, 256), 256, 0, m.stream>>>(n, -1.0, m.t, m.r, m.w, o.fast);
+        kf_count_launch();
+        o.sptrsv(m, m.w, Vb(m, 0), prec);
+      }
+      dev_normalize(m, Vb(m, 0), m.scal + S_T0, o.fast);
+      fetch(m, S_T0, 1);
+      rs[0] = m.h_scal[S_T0];
+      if (!std::isfinite(rs[0])) {
+        kf_set_error(KFUN3D_ERR_NONFINITE, "preconditioned residual is not finite");
+        done = false;
+        steps = -1;
+        break;
+      }
+      if (total == 0) tol = p->gmres_rtol * rs[0];
+      int k = 0;
+      while (k < restart) {
+        arnoldi_step(m, o, k, prec);
+        fetch(m, 0, k + 2);
+        double *hh = ghh + k * (KF_NBASIS + 1);
+        for (int i = 0; i <= k + 1; i++) hh[i] = m.h_scal[i];
+        for (int i = 0; i < k; i++) {               // src/kernel.c:143-149
+          const double tt = hh[i];
+          hh[i] = cs[i] * hh[i] + sn[i] * hh[i + 1];
+          hh[i + 1] = cs[i] * hh[i + 1] - sn[i] * tt;
+        }
+        const double tt = sqrt(hh[k] * hh[k] + hh[k + 1] * hh[k + 1]);
+        const double c = hh[k] / tt, s = hh[k + 1] / tt;
+        cs[k] = c;
+        sn[k] = s;
+        rs[k + 1] = -(s * rs[k]);
+        rs[k] = c * rs[k];
+        hh[k] = c * hh[k] + s * hh[k + 1];
+        const double res = fabs(rs[k + 1]);
+        k++;
+        if (res <= tol) { done = true; break; }
+        if (!std::isfinite(res)) break;
+      }
+      total += k;
+      rs[k - 1] /= ghh[(k - 1) * (KF_NBASIS + 1) + (k - 1)];   // src/kernel.c:178-188
+      for (int i = 1; i <= k - 1; i++) {
+        const int mm = (k - 1) - i;
+        double tt = rs[mm];
+        for (int j = mm + 1; j <= k - 1; j++) tt -= ghh[j * (KF_NBASIS + 1) + mm] * rs[j];
+        rs[mm] = tt / ghh[mm * (KF_NBASIS + 1) + mm];
+      }
+      for (int vv = 0; vv < k; vv++) dev_axpy(m, rs[vv], Vb(m, vv), m.x, o.fast);
+      if (print && k == restart) fun3d_printf(5, ">> GMRES: COMPLETED ONE CYCLE\n");
+      if (done) break;
+    }
+    if (steps < 0) break;
+    if (print) fun3d_printf(5, ">> GMRES: TOTAL ITERATIONS %d\n", total);
+    dev_axpy(m, -1.0, m.x, m.q, o.fast);                           // src/kernel.c:200
+    k_forces<<<1, 32, 0, m.stream>>>(m.ncol, m.col, m.wf_nodes, m.xyz, (const double4 *)m.q, u, v, m.forces);
+    kf_count_launch();
+    CK(cudaEventRecord(ev1, m.stream));
+    CK(cudaMemcpyAsync(m.h_scal + 48, m.forces, 3 * sizeof(double), cudaMemcpyDeviceToHost, m.stream));
+    CK(cudaStreamSynchronize(m.stream));
+    if (!check_cuda("solve")) { steps = -1; break; }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    const double lift = m.h_scal[48], drag = m.h_scal[49], momn = m.h_scal[50];
+    if (print) {
+      printf("STEP: %d ", its);
+      printf("CFL: %g ", cfl);
+      printf("NORM: %g\n", fnorm);
+      printf("LIFT: %g DRAG: %g MOMN: %g\n", lift, drag, momn);
+    }
+    if (hist && nrec < max_hist) {
+      hist[nrec] = kfun3d_step{its, (int)total, cfl, fnorm, lift, drag, momn, ms * 1e-3};
+      nrec++;
+    }
+    steps = its + 1;
+    if (round(fnorm0 / fnorm) >= p->stop_ratio) break;   // src/kernel.c:214
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  return steps < 0 ? -1 : nrec;
+}
+
+// ------------------------------------------------------------------ entry points
+
+namespace {
+
+DevMesh *dev_or_fail(const GEOMETRY *g)
+{
+  DevMesh *m = kf_device(g);
+  return m;
+}
+
+void h2d(DevMesh &m, double *dst, const double *src, size_t n)
+{
+  CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, m.stream));
+}
+
+void d2h(DevMesh &m, double *dst, const double *src, size_t n)
+{
+  CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, m.stream));
+}
+
+bool finish(DevMesh &m, const char *what)
+{
+  CK(cudaStreamSynchronize(m.stream));
+  return check_cuda(what);
+}
+
+}  // namespace
+
+extern "C" void ComputeFlux(const GEOMETRY *g, const double *q, GRADIENT *grad, double *r)
+{
+  DevMesh *m = dev_or_fail(g);
+  if (!m) return;
+  const size_t n = 4 * (size_t)m->N;
+  h2d(*m, m->w, q, n);
+  const Ops o = ops();
+  if (kf_first_order()) {
+    CK(cudaMemsetAsync(m->gx, 0, n * sizeof(double), m->stream));
+    CK(cudaMemsetAsync(m->gy, 0, n * sizeof(double), m->stream));
+    CK(cudaMemsetAsync(m->gz, 0, n * sizeof(double), m->stream));
+  }
+  dev_residual(*m, o, m->w, m->t);
+  d2h(*m, grad->x0, m->gx, n);
+  d2h(*m, grad->x1, m->gy, n);
+  d2h(*m, grad->x2, m->gz, n);
+  d2h(*m, r, m->t, n);
+  finish(*m, "ComputeFlux");
+}
+
+extern "C" void ComputeTimeStep(const double cfl, GEOMETRY *g)
+{
+  DevMesh *m = dev_or_fail(g);
+  if (!m) return;
+  h2d(*m, m->q, g->q->q, 4 * (size_t)m->N);
+  ops().timestep(*m, m->q, cfl);
+  d2h(*m, g->n->cdt, m->cdt, m->N);
+  finish(*m, "ComputeTimeStep");
+}
+
+extern "C" void ComputeA(GEOMETRY *g)
+{
+  DevMesh *m = dev_or_fail(g);
+  if (!m) return;
+  double u, v;
+  kfun3d_get_freestream(&u, &v);
+  h2d(*m, m->q, g->q->q, 4 * (size_t)m->N);
+  h2d(*m, m->cdt, g->n->cdt, m->N);
+  ops().fill(*m, m->q, u, v, kf_precision());
+  m->a_valid = true;
+  m->factored = false;
+  finish(*m, "ComputeA");
+}
+
+extern "C" void ComputeNumericalILU(GEOMETRY *g)
+{
+  DevMesh *m = dev_or_fail(g);
+  if (!m) return;
+  ops().ilu(*m, kf_precision());
+  m->factored = true;
+  if (!finish(*m, "ComputeNumericalILU")) return;
+  if (device_status(*m) == KFUN3D_ERR_PIVOT)
+    kf_set_error(KFUN3D_ERR_PIVOT, "singular or non-finite pivot block in ILU(0)");
+}
+
+extern "C" void ComputeSparseTriangularSolve(const GEOMETRY *g, const double *b, double *x)
+{
+  DevMesh *m = dev_or_fail(g);
+  if (!m) return;
+  const size_t n = 4 * (size_t)m->N;
+  h2d(*m, m->rhs, b, n);
+  ops().sptrsv(*m, m->rhs, m->t, kf_precision());
+  d2h(*m, x, m->t, n);
+  finish(*m, "ComputeSparseTriangularSolve");
+}
+
+extern "C" void ComputeForces(const GEOMETRY *g, double *forces)
+{
+  DevMesh *m = dev_or_fail(g);
+  if (!m) return;
+  double u, v;
+  kfun3d_get_freestream(&u, &v);
+  h2d(*m, m->q, g->q->q, 4 * (size_t)m->N);
+  k_forces<<<1, 32, 0, m->stream>>>(m->ncol, m->col, m->wf_nodes, m->xyz, (const double4 *)m->q, u, v, m->forces);
+  kf_count_launch();
+  d2h(*m, forces, m->forces, 3);
+  finish(*m, "ComputeForces");
+}
+
+// ---- BLAS-1 on host arrays (inc/utils.h): staged through a device buffer
+
+namespace {
+
+struct Scratch {
+  double *buf = nullptr;
+  size_t cap = 0;
+  cudaStream_t stream = nullptr;
+  double *ensure(size_t n)
+  {
+    if (!stream) CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    if (n > cap) {
+      if (buf) cudaFree(buf);
+      cap = std::max(n, (size_t)1 << 16);
+      CK(cudaMalloc(&buf, (3 * cap + 4096) * sizeof(double)));
+    }
+    return buf;
+  }
+} g_scr;
+
+double blas_reduce(size_t sz, const double *hv, int op)
+{
+  double *d = g_scr.ensure(sz);
+  if (!d) return NAN;
+  cudaStream_t s = g_scr.stream;
+  double *red = d + 3 * g_scr.cap, out = 0.0;
+  CK(cudaMemcpyAsync(d, hv, sz * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (kf_mode() == KFUN3D_MODE_FAST) {
+    k_dot_partial<<<RED_BLOCKS, 256, 0, s>>>(sz, d, d, red + 8);
+    k_dot_final<<<1, 256, 0, s>>>(red + 8, RED_BLOCKS, red, op);
+    kf_count_launch(2);
+  } else {
+    k_dot_seq<<<1, 32, 0, s>>>(sz, d, d, red, op);
+    kf_count_launch();
+  }
+  CK(cudaMemcpyAsync(&out, red, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  check_cuda("Compute2ndNorm");
+  return out;
+}
+
+}  // namespace
+
+extern "C" double Compute2ndNorm(const size_t sz, const double *v) { return blas_reduce(sz, v, 1); }
+
+extern "C" void ComputeAXPY(const size_t sz, const double a, const double *x, double *y)
+{
+  double *d = g_scr.ensure(sz);
+  if (!d) return;
+  cudaStream_t s = g_scr.stream;
+  CK(cudaMemcpyAsync(d, x, sz * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d + g_scr.cap, y, sz * sizeof(double), cudaMemcpyHostToDevice, s));
+  k_axpy<<<nblk(sz, 256), 256, 0, s>>>(sz, a, d, d + g_scr.cap, kf_mode() == KFUN3D_MODE_FAST);
+  kf_count_launch();
+  CK(cudaMemcpyAsync(y, d + g_scr.cap, sz * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  check_cuda("ComputeAXPY");
+}
+
+extern "C" void ComputeNewAXPY(const size_t sz, const double a, const double *x, const double *y, double *w)
+{
+  double *d = g_scr.ensure(sz);
+  if (!d) return;
+  cudaStream_t s = g_scr.stream;
+  CK(cudaMemcpyAsync(d, x, sz * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d + g_scr.cap, y, sz * sizeof(double), cudaMemcpyHostToDevice, s));
+  k_waxpy<<<nblk(sz, 256), 256, 0, s>>>(sz, a, d, d + g_scr.cap, d + 2 * g_scr.cap, kf_mode() == KFUN3D_MODE_FAST);
+  kf_count_launch();
+  CK(cudaMemcpyAsync(w, d + 2 * g_scr.cap, sz * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  check_cuda("ComputeNewAXPY");
+}
+
+extern "C" double Normalize(const size_t sz, double *x)
+{
+  double *d = g_scr.ensure(sz);
+  if (!d) return NAN;
+  cudaStream_t s = g_scr.stream;
+  double *red = d + 3 * g_scr.cap, nrm = 0.0;
+  CK(cudaMemcpyAsync(d, x, sz * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (kf_mode() == KFUN3D_MODE_FAST) {
+    k_dot_partial<<<RED_BLOCKS, 256, 0, s>>>(sz, d, d, red + 8);
+    k_dot_final<<<1, 256, 0, s>>>(red + 8, RED_BLOCKS, red, 1);
+    kf_count_launch(2);
+  } else {
+    k_dot_seq<<<1, 32, 0, s>>>(sz, d, d, red, 1);
+    kf_count_launch();
+  }
+  k_scale_inv<<<nblk(sz, 256), 256, 0, s>>>(sz, red, d);
+  kf_count_launch();
+  CK(cudaMemcpyAsync(x, d, sz * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&nrm, red, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  check_cuda("Normalize");
+  return nrm;
+}
+
+// ---- whole solves
+
+extern "C" int kfun3d_solve(GEOMETRY *g, const kfun3d_solver_params *p, kfun3d_step *hist, int max_hist)
+{
+  DevMesh *m = dev_or_fail(g);
+  if (!m) return -1;
+  kfun3d_solver_params def;
+  if (!p) { kfun3d_default_params(&def); p = &def; }
+  h2d(*m, m->q, g->q->q, 4 * (size_t)m->N);
+  CK(cudaMemsetAsync(m->lslot, 0, (16 * (size_t)m->nlower + 16) * sizeof(double), m->stream));
+  const int n = solve_device(*m, g, p, hist, max_hist, false);
+  d2h(*m, g->q->q, m->q, 4 * (size_t)m->N);
+  d2h(*m, g->n->cdt, m->cdt, m->N);
+  finish(*m, "kfun3d_solve");
+  return n;
+}
+
+extern "C" void Kernel(GEOMETRY *g)
+{
+  DevMesh *m = dev_or_fail(g);
+  if (!m) return;
+  kfun3d_solver_params p;
+  kfun3d_default_params(&p);
+  h2d(*m, m->q, g->q->q, 4 * (size_t)m->N);
+  solve_device(*m, g, &p, nullptr, 0, g_kf_verbose != 0);
+  d2h(*m, g->q->q, m->q, 4 * (size_t)m->N);
+  d2h(*m, g->n->cdt, m->cdt, m->N);
+  finish(*m, "Kernel");
+}
+
+// ---- device-resident timing
+
+extern "C" double kfun3d_time_kernel(GEOMETRY *g, int which, int reps)
+{
+  DevMesh *m = dev_or_fail(g);
+  if (!m || reps < 1) return -1.0;
+  const Ops o = ops();
+  const int prec = kf_precision();
+  const size_t n = 4 * (size_t)m->N;
+  double u, v;
+  kfun3d_get_freestream(&u, &v);
+  h2d(*m, m->q, g->q->q, n);
+  // a consistent state for the preconditioner and the Krylov vectors
+  dev_residual(*m, o, m->q, m->r);
+  o.timestep(*m, m->q, 50.0);
+  o.fill(*m, m->q, u, v, prec);
+  o.ilu(*m, prec);
+  dev_reduce(*m, m->q, m->q, m->scal + S_QN, 2, o.fast);
+  for (int k = 0; k <= 16; k++) {
+    CK(cudaMemcpyAsync(Vb(*m, k), m->r, n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream));
+    dev_normalize(*m, Vb(*m, k), m->scal + S_T0, o.fast);
+  }
+  auto run = [&]() {
+    switch (which) {
+      case 0: dev_residual(*m, o, m->q, m->r); break;
+      case 1: o.timestep(*m, m->q, 50.0); break;
+      case 2: o.fill(*m, m->q, u, v, prec); break;
+      case 3: o.fill(*m, m->q, u, v, prec); o.ilu(*m, prec); break;
+      case 4: o.sptrsv(*m, m->r, m->t, prec); break;
+      case 5: arnoldi_step(*m, o, 15, prec); break;
+      default: break;
+    }
+  };
+  for (int i = 0; i < 2; i++) run();
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, m->stream));
+  for (int i = 0; i < reps; i++) run();
+  CK(cudaEventRecord(e1, m->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!finish(*m, "kfun3d_time_kernel")) return -1.0;
+  return (double)ms / reps;
+}
+
+extern "C" long kfun3d_matrix_read(const GEOMETRY *g, unsigned int *ia, unsigned int *ja, double *blocks)
+{
+  MatrixHandle *h = kf_handle(g);
+  if (!h) {
+    kf_set_error(KFUN3D_ERR_ARG, "GEOMETRY::matrix is not a kfun3d_b200 handle");
+    return -1;
+  }
+  const HostPattern &p = h->pat;
+  if (ia) memcpy(ia, p.ia.data(), p.ia.size() * sizeof(unsigned int));
+  if (ja) memcpy(ja, p.ja.data(), p.ja.size() * sizeof(unsigned int));
+  if (blocks) {
+    DevMesh *m = dev_or_fail(g);
+    if (!m) return -1;
+    const size_t nv = 16 * p.nnz;
+    if (kf_precision() == 0) {
+      d2h(*m, blocks, m->A, nv);
+    } else {
+      std::vector<float> tmp(nv);
+      CK(cudaMemcpyAsync(tmp.data(), m->Af, nv * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+      CK(cudaStreamSynchronize(m->stream));
+      for (size_t i = 0; i < nv; i++) blocks[i] = tmp[i];
+    }
+    if (!finish(*m, "kfun3d_matrix_read")) return -1;
+  }
+  return (long)p.nnz;
+}

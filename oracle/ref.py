@@ -88,6 +88,7 @@ class RefMesh:
         self.aoa = aoa_deg
         self.g = L.ref_setup(os.fsencode(path), threads)
         self.view = GeometryView(self.g)
+        self.view.owner = self
 
     def close(self):
         if self.g:
