@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""One-line benchmark of the kfun3d_b200 hot path (pseudo-transient Newton-Krylov).
+
+Workload (N = 1): the config-1 solve — the 70^3 seeded Kuhn-box mesh (343,000
+nodes, 2,342,619 edges, bump 0.1, jitter 0.2h, random numbering), AoA 3.06,
+second-order residual, FP64 ILU(0)-GMRES(30), SER CFL from 50, at most 20
+Newton steps, stopped at a 1e-8 drop of the residual norm.  A step is one such
+solve from the free-stream state.  The metric is BASELINE.json's: seconds to
+the 1e-8 drop (lower is better), with flux edges/s and the other kernel
+throughputs reported beside it.
+
+value    device-resident: state and mesh already in HBM, CUDA events on the
+         solver's stream around each solve, max over ranks.
+e2e      the same solve through the C ABI with host buffers (kfun3d_solve:
+         state uploaded, solved, state and time step downloaded), wall clock.
+roofline the kernel family with the largest share of one GMRES iteration,
+         algorithmic bytes (per-kernel formulas below) / its CUDA-event time,
+         against MEASURED_PEAKS.json's HBM copy bandwidth.
+cpu_baseline / --impl reference: the reference itself (oracle/_ref, built from
+         its own sources) on all host cores, timed on a bounded sample.
+
+Multi-GPU: replicas (one independent mesh per GPU, no collective on the data
+path); `scaling` is weak.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s to 1e-8 residual drop: mixed+learned vs plain FP64 on 1 B200; flux edges/s"
+
+CONFIGS = {
+    0: dict(workload="config0: 25^3 Kuhn box, first-order flux, FP64 exact arithmetic, 20 Newton steps",
+            n=25, seed=0, bump=0.1, aoa=3.06, precision=0, mode="exact", first_order=True,
+            ts_max=20, stop_ratio=1e30),
+    1: dict(workload="config1: 70^3 Kuhn box, second-order flux, plain FP64, solve to 1e-8 drop",
+            n=70, seed=1, bump=0.1, aoa=3.06, precision=0, mode="fast", first_order=False,
+            ts_max=20, stop_ratio=1e8),
+    2: dict(workload="config2: 70^3 Kuhn box, FP32 Jacobian/ILU(0)/SpTRSV, FP64 residual and GMRES, to 1e-8 drop",
+            n=70, seed=1, bump=0.1, aoa=3.06, precision=1, mode="fast", first_order=False,
+            ts_max=20, stop_ratio=1e8),
+    4: dict(workload="config4: 120^3 Kuhn box (bump 0.12, AoA 4.5), FP32 preconditioner, to 1e-8 drop",
+            n=120, seed=4, bump=0.12, aoa=4.5, precision=1, mode="fast", first_order=False,
+            ts_max=20, stop_ratio=1e8),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- algorithmic bytes
+def alg_bytes(N, E, Fs, Ns, Nf, nnzb, prec, j=15):
+    """Per-call algorithmic bytes of each kernel family (f64 = 8 B, u32 = 4 B;
+    node arrays counted once per pass; w = 8 for FP64 blocks, 4 for FP32)."""
+    w = 4 if prec else 8
+    b = {}
+    b["gradient"] = 56 * E + 128 * N
+    b["edge_flux"] = 40 * E + 184 * N + 12 * Fs + 28 * Nf
+    b["flux"] = b["gradient"] + b["edge_flux"]                       # 96E + 312N + 12Fs + 28Nf
+    b["timestep"] = 40 * E + 40 * N + 28 * (Ns + Nf)
+    b["fill"] = (296 * E + 168 * N if not prec else 168 * E + 104 * N) + 28 * (Ns + Nf)
+    b["ilu"] = nnzb * (32 * w + 4) + 8 * (N + 1)
+    b["sptrsv"] = nnzb * (16 * w + 4) + 8 * (N + 1) + 96 * N
+    b["mgs"] = (5 * (j + 1) + 3) * 32 * N                             # j+1 dot/axpy pairs + normalise
+    b["gmres_iter"] = b["flux"] + 296 * N + b["sptrsv"] + b["mgs"]
+    return b
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpus):
+        self.gpus = gpus
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", ",".join(str(g) for g in self.gpus), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception as e:   # no nvidia-smi: report no clock data
+            log("clock sampler unavailable:", e)
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            t = [x.strip() for x in line.split(",")]
+            if len(t) < 9:
+                continue
+            try:
+                sm.append(float(t[1]))
+                mx = max(mx, float(t[2]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if t[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- distributed plumbing
+class Dist:
+    def __init__(self, gpus):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import torch
+            import torch.distributed as dist
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            import datetime
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+            self.backend = backend
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        import torch
+        dev = "cuda" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+
+
+def cuda_sync():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
+    except Exception:
+        pass
+
+
+# ---------------------------------------------------------------- the reference on the host cores
+class CStdoutToStderr:
+    """Routes C-level stdout (the reference prints METIS statistics) to stderr,
+    so this script's stdout carries only the JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_sample(path, cfg, total_its, threads):
+    """Time the reference (oracle/_ref) on a bounded sample of the solve: its
+    first two Newton steps on the same mesh and settings, at `threads` OpenMP
+    threads.  Seconds to the 1e-8 drop are extrapolated by GMRES iterations:
+    sample_time * total_its / sample_its (the per-iteration work of this solver
+    is the same at every step)."""
+    from oracle import ref
+    m = ref.RefMesh(path, cfg["aoa"], threads)
+    v = m.view
+    q0 = v.q.copy()
+    # ComputeFlux throughput (edges/s): a few calls
+    t0 = time.perf_counter()
+    nflux = 3
+    for _ in range(nflux):
+        m.flux(q0)
+    t_flux = (time.perf_counter() - t0) / nflux
+    t0 = time.perf_counter()
+    hist = m.solve(ts_max=2, stop_ratio=cfg["stop_ratio"])
+    t_sample = time.perf_counter() - t0
+    its = sum(h["gmres_its"] for h in hist)
+    m.close()
+    return dict(seconds=t_sample * total_its / max(its, 1), sample_seconds=t_sample, sample_its=its,
+                flux_edges_per_s=v.nedges / t_flux)
+
+
+def run_reference_arm(args, cfg):
+    # Under torchrun only rank 0 times the reference; the other ranks have no work.
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libkfun3d_ref.so was not built"}))
+        return
+    import kfun3d_b200 as kf
+    path = mesh_path(cfg)
+    threads = host_cores()
+    total_its = args.ref_total_its
+    # Warm-up: one untimed ComputeFlux pass per requested warm-up step (page-in
+    # of the mesh and OpenMP thread start); each timed step is a full sample.
+    if args.warmup:
+        with CStdoutToStderr():
+            m = ref.RefMesh(path, cfg["aoa"], threads)
+            for _ in range(args.warmup):
+                m.flux(m.view.q.copy())
+            m.close()
+    vals = []
+    t_all = time.perf_counter()
+    with CStdoutToStderr():
+        for _ in range(args.steps):
+            vals.append(reference_sample(path, cfg, total_its, threads))
+    wall = time.perf_counter() - t_all
+    value = statistics.mean(v["seconds"] for v in vals)
+    sample = (f"first 2 Newton steps ({vals[-1]['sample_its']} GMRES iterations, "
+              f"{vals[-1]['sample_seconds']:.2f} s) of the workload, extrapolated to {total_its} iterations")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": cfg["workload"], "threads": threads},
+            "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "reference",
+                             "sample": sample, "flux_edges_per_s": vals[-1]["flux_edges_per_s"]},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------- the GPU arm
+def mesh_path(cfg):
+    import kfun3d_b200 as kf
+    d = os.environ.get("KFUN3D_MESH_DIR", os.path.join(tempfile.gettempdir(), "kfun3d_meshes"))
+    os.makedirs(d, exist_ok=True)
+    p = os.path.join(d, f"box{cfg['n']}_s{cfg['seed']}_b{cfg['bump']}.msh")
+    if not os.path.exists(p):
+        tmp = p + f".{os.getpid()}.tmp"
+        kf.generate_mesh(tmp, cfg["n"], bump_height=cfg["bump"], seed=cfg["seed"])
+        os.replace(tmp, p)
+    return p
+
+
+def configure(kf, cfg):
+    kf.set_mode(cfg["mode"])
+    kf.set_precision(cfg["precision"])
+    kf.set_first_order(cfg["first_order"])
+    kf.set_aoa(cfg["aoa"])
+    kf.set_verbose(False)
+
+
+def run_gpu_arm(args, cfg):
+    dist = Dist(list(range(args.gpus)))
+    import torch
+    if torch.cuda.is_available():
+        torch.cuda.set_device(dist.local)
+    import kfun3d_b200 as kf
+    configure(kf, cfg)
+    path = mesh_path(cfg)
+    m = kf.Mesh(path)
+    v = m.view
+    N, E = v.nnodes, v.nedges
+    params = dict(ts_max=cfg["ts_max"], stop_ratio=cfg["stop_ratio"])
+
+    # warm-up (uploads the mesh, builds the device mirror)
+    m.time_solve(reps=args.warmup, **params)
+    cuda_sync()
+    dist.barrier()
+    cuda_sync()
+    sampler = ClockSampler([dist.local]) if dist.rank == 0 else None
+    if sampler:
+        sampler.start()
+    kf.reset_launch_count()
+    t_wall = time.perf_counter()
+    t_solve, hist = m.time_solve(reps=args.steps, **params)
+    cuda_sync()
+    launches = kf.launch_count()
+    dist.barrier()
+    cuda_sync()
+    wall = time.perf_counter() - t_wall
+    clocks = sampler.stop() if sampler else None
+    value = dist.max(t_solve)
+    gmres_its = sum(h["gmres_its"] for h in hist)
+    drop = hist[-1]["fnorm"] / hist[0]["fnorm"] if hist else float("nan")
+
+    # end to end through the C ABI, host buffers
+    q0 = v.q.copy()
+    e2e = []
+    for _ in range(max(1, min(args.steps, 3))):
+        v.q[:] = q0
+        t0 = time.perf_counter()
+        m.solve(**params)
+        e2e.append(time.perf_counter() - t0)
+    v.q[:] = q0
+    e2e_value = dist.max(statistics.mean(e2e))
+
+    # per-kernel live timing (CUDA events on the solver's stream)
+    peak, peak_kind = peaks()
+    Fs, Ns, Nf = v.nfaces, v.ns, v.nf
+    nnzb = N + 2 * E
+    B = alg_bytes(N, E, Fs, Ns, Nf, nnzb, cfg["precision"])
+    t = {}
+    for name in ("flux", "gradient", "edge_flux", "timestep", "fill", "sptrsv", "mgs", "gmres_iter"):
+        t[name] = m.time_kernel(name, 20 if name not in ("gmres_iter",) else 10)
+    t["ilu"] = max(m.time_kernel("ilu", 3) - t["fill"], 1e-6)
+    kernels = {k: {"ms": round(t[k], 5), "gbs": round(B[k] / (t[k] * 1e-3) / 1e9, 1),
+                   "frac": round(B[k] / (t[k] * 1e-3) / 1e9 / peak, 4)} for k in t}
+    share = {k: t[k] for k in ("flux", "sptrsv", "mgs")}
+    dominant = max(share, key=share.get)
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", f"traffic_config{args.config}.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(dominant)
+    achieved = B[dominant] / (t[dominant] * 1e-3) / 1e9
+    roofline = {"kernel": dominant, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                "peak_kind": peak_kind, "algorithmic_bytes": B[dominant]}
+
+    cpu = None
+    if dist.rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available():
+            threads = host_cores()
+            with CStdoutToStderr():
+                s = reference_sample(path, cfg, gmres_its, threads)
+            cpu = {"value": s["seconds"], "unit": "s", "cores": threads, "kind": "reference",
+                   "sample": (f"reference (oracle/_ref) first 2 Newton steps of this workload: "
+                              f"{s['sample_its']} GMRES iterations in {s['sample_seconds']:.2f} s at "
+                              f"{threads} threads, extrapolated to this solve's {gmres_its} iterations"),
+                   "flux_edges_per_s": s["flux_edges_per_s"]}
+    if dist.rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if cfg["precision"] == 0 else "f64/f32",
+            "data": "synthetic (seeded Kuhn-box mesh generated on the box)",
+            "config": {"workload": cfg["workload"], "nodes": N, "edges": E, "nnz_blocks": nnzb,
+                       "newton_steps": len(hist), "gmres_its": gmres_its, "residual_drop": drop,
+                       "mode": cfg["mode"], "precision": "fp64" if cfg["precision"] == 0 else "fp32-precond",
+                       "parallelism": f"replicas x{args.gpus}",
+                       "l2": "working set (matrix + vectors) larger than the 126 MB L2"},
+            "e2e": {"value": e2e_value, "unit": "s", "h2d_bytes_per_step": 32 * N,
+                    "d2h_bytes_per_step": 32 * N + 8 * N},
+            "roofline": roofline,
+            "kernels": kernels,
+            "flux_edges_per_s": E / (t["flux"] * 1e-3),
+            "fill_edges_per_s": E / (t["fill"] * 1e-3),
+            "gmres_iterations_per_s": gmres_its / value,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+            "wall_s": wall,
+        }
+        print(json.dumps(line))
+    m.close()
+    dist.close()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=1, choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-total-its", type=int, default=741,
+                    help="GMRES iterations of the full solve used to extrapolate the reference sample")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference_arm(args, cfg)
+    else:
+        run_gpu_arm(args, cfg)
+
+
+if __name__ == "__main__":
+    main()

@@ -187,8 +187,17 @@ int kfun3d_mesh_generate(const char *path, const kfun3d_mesh_spec *spec);
    one call in milliseconds measured with CUDA events on the solver's stream,
    or a negative value on error.  which: 0 flux (gradient + edge flux +
    boundary), 1 time step, 2 Jacobian fill, 3 ILU(0), 4 triangular solves,
-   5 one GMRES iteration at Arnoldi index 15 (J.v + solve + MGS). */
+   5 one GMRES iteration at Arnoldi index 15 (J.v + solve + MGS),
+   6 modified Gram-Schmidt and normalisation alone at Arnoldi index 15,
+   7 the gradient alone, 8 the edge flux and boundary terms alone. */
 double kfun3d_time_kernel(GEOMETRY *g, int which, int reps);
+
+/* Device-resident solve timing: the initial state g->q->q is uploaded once;
+   each of reps solves restarts from it on the device and runs kfun3d_solve's
+   algorithm.  Returns the mean seconds per solve (CUDA events on the solver's
+   stream) and fills hist with the last solve's steps; negative on error. */
+double kfun3d_time_solve(GEOMETRY *g, const kfun3d_solver_params *p, int reps, kfun3d_step *hist,
+                         int max_hist, int *nsteps);
 
 /* Number of kernel launches the library issued since the last reset. */
 unsigned long long kfun3d_launch_count(void);

@@ -90,6 +90,7 @@ def lib():
         "kfun3d_reset_launch_count": (None, []),
         "kfun3d_device_release": (None, [G]),
         "kfun3d_matrix_read": (C.c_long, [G, P(C.c_uint), P(C.c_uint), D]),
+        "kfun3d_time_solve": (C.c_double, [G, P(SolverParams), C.c_int, P(Step), C.c_int, P(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -273,7 +274,8 @@ class Mesh:
                      drag=h.drag, momn=h.momn, seconds=h.seconds) for h in hist[:n]]
 
     def time_kernel(self, which, reps=10):
-        names = {"flux": 0, "timestep": 1, "fill": 2, "ilu": 3, "sptrsv": 4, "gmres_iter": 5}
+        names = {"flux": 0, "timestep": 1, "fill": 2, "ilu": 3, "sptrsv": 4, "gmres_iter": 5,
+                 "mgs": 6, "gradient": 7, "edge_flux": 8}
         w = names.get(which, which)
         ms = lib().kfun3d_time_kernel(self.g, int(w), int(reps))
         if ms < 0:
@@ -292,6 +294,18 @@ class Mesh:
         if rc < 0:
             raise RuntimeError(f"kfun3d_matrix_read failed: {last_error()}")
         return ia, ja, blocks.reshape(-1, 4, 4)
+
+    def time_solve(self, reps=1, **params):
+        """Mean device seconds per solve from the current state, and the last history."""
+        p = default_params(**params)
+        hist = (Step * 64)()
+        ns = C.c_int(0)
+        t = lib().kfun3d_time_solve(self.g, C.byref(p), int(reps), hist, 64, C.byref(ns))
+        if t < 0:
+            raise RuntimeError(f"kfun3d_time_solve failed: {last_error()}")
+        steps = [dict(step=h.step, gmres_its=h.gmres_its, cfl=h.cfl, fnorm=h.fnorm, lift=h.lift,
+                      drag=h.drag, momn=h.momn, seconds=h.seconds) for h in hist[:ns.value]]
+        return t, steps
 
     def release_device(self):
         lib().kfun3d_device_release(self.g)

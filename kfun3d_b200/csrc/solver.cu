@@ -729,6 +729,16 @@ extern "C" double kfun3d_time_kernel(GEOMETRY *g, int which, int reps)
       case 3: o.fill(*m, m->q, u, v, prec); o.ilu(*m, prec); break;
       case 4: o.sptrsv(*m, m->r, m->t, prec); break;
       case 5: arnoldi_step(*m, o, 15, prec); break;
+      case 6:
+        for (int vv = 0; vv <= 15; vv++) {
+          dev_reduce(*m, Vb(*m, 16), Vb(*m, vv), m->scal + vv, 0, o.fast);
+          k_axpy_dev<<<nblk(n, 256), 256, 0, m->stream>>>(n, m->scal + vv, -1.0, Vb(*m, vv), Vb(*m, 16), o.fast);
+          kf_count_launch();
+        }
+        dev_normalize(*m, Vb(*m, 16), m->scal + 16, o.fast);
+        break;
+      case 7: o.gradient(*m, m->q); break;
+      case 8: o.residual(*m, m->q, m->r, kf_first_order(), u, v); break;
       default: break;
     }
   };
@@ -773,4 +783,42 @@ extern "C" long kfun3d_matrix_read(const GEOMETRY *g, unsigned int *ia, unsigned
     if (!finish(*m, "kfun3d_matrix_read")) return -1;
   }
   return (long)p.nnz;
+}
+
+extern "C" double kfun3d_time_solve(GEOMETRY *g, const kfun3d_solver_params *p, int reps, kfun3d_step *hist,
+                                    int max_hist, int *nsteps)
+{
+  DevMesh *m = dev_or_fail(g);
+  if (!m || reps < 1) return -1.0;
+  kfun3d_solver_params def;
+  if (!p) { kfun3d_default_params(&def); p = &def; }
+  const size_t n = 4 * (size_t)m->N;
+  double *q0 = nullptr;
+  CK(cudaMalloc(&q0, n * sizeof(double)));
+  if (!q0) return -1.0;
+  h2d(*m, q0, g->q->q, n);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  double total = 0.0;
+  int ns = 0;
+  for (int r = 0; r < reps; r++) {
+    CK(cudaMemcpyAsync(m->q, q0, n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream));
+    CK(cudaMemsetAsync(m->lslot, 0, (16 * (size_t)m->nlower + 16) * sizeof(double), m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    CK(cudaEventRecord(e0, m->stream));
+    ns = solve_device(*m, g, p, hist, max_hist, false);
+    CK(cudaEventRecord(e1, m->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    total += ms * 1e-3;
+    if (ns < 0) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(q0);
+  if (nsteps) *nsteps = ns;
+  if (!finish(*m, "kfun3d_time_solve") || ns < 0) return -1.0;
+  return total / reps;
 }
