@@ -100,7 +100,8 @@ enum kfun3d_status {
   KFUN3D_ERR_ARG = 4,         /* invalid argument or unsupported GEOMETRY */
   KFUN3D_ERR_IO = 5,          /* mesh file error */
   KFUN3D_ERR_NO_DEVICE = 6,   /* no CUDA device */
-  KFUN3D_ERR_DIVERGED = 7     /* linear or nonlinear solve failed */
+  KFUN3D_ERR_DIVERGED = 7,    /* linear or nonlinear solve failed */
+  KFUN3D_ERR_TIMEOUT = 8      /* a device-side wait exceeded its bound (results invalid) */
 };
 
 /* Status of the most recent call (KFUN3D_OK or an error code) and its text. */

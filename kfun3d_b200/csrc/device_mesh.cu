@@ -46,6 +46,7 @@ int kf_mode() { return g_mode; }
 int kf_precision() { return g_precision; }
 int kf_first_order() { return g_first_order; }
 void kf_count_launch(unsigned n) { g_launches += n; }
+void kfun3d_reset_launch_count_by(unsigned long long n) { g_launches -= n; }
 
 extern "C" {
 
@@ -152,6 +153,27 @@ void kf_build_pattern(HostPattern &p, size_t N, size_t E, const unsigned int *n0
   };
   levels(true, p.lev_l, p.lev_l_ptr);
   levels(false, p.lev_u, p.lev_u_ptr);
+  // ILU(0) product lists: for block (i,k) merge row i's columns up to the
+  // diagonal with row k's columns up to the diagonal (= U's column k)
+  p.pair_ptr.assign(p.nnz + 1, 0);
+  p.pairs.clear();
+  p.pairs.reserve(p.nnz * 10);
+  for (size_t i = 0; i < N; i++) {
+    for (uint32_t j = p.ia[i]; j < p.ia[i + 1]; j++) {
+      const uint32_t k = p.ja[j];
+      uint32_t pl = p.ia[i], pu = p.ia[k];
+      while (pl <= p.diag[i] && pu <= p.diag[k]) {
+        const uint32_t cl = p.ja[pl], cu = p.ja[pu];
+        if (cl == cu) {
+          p.pairs.push_back(cl == i ? 0xffffffffu : p.lpos[i] + (pl - p.ia[i]));
+          p.pairs.push_back(p.tblk[pu]);
+        }
+        if (cl <= cu) pl++;
+        if (cl >= cu) pu++;
+      }
+      p.pair_ptr[j + 1] = (uint32_t)(p.pairs.size() / 2);
+    }
+  }
 }
 
 // ----------------------------------------------------------------- matrix handle ABI
@@ -223,10 +245,14 @@ static void release_device(MatrixHandle *h)
                   m->wf_n, m->s_n, m->f_n, m->bnd_of, m->bnd_node, m->bnd_ptr, m->bnd_ent, m->ia, m->ja,
                   m->diag, m->tblk, m->lpos, m->last_lower, m->lev_l, m->lev_u, m->A, m->lslot, m->dinv,
                   m->Af, m->dinvf, m->q, m->r, m->gx, m->gy, m->gz, m->cdt, m->w, m->t, m->x, m->rhs, m->V,
-                  m->red, m->scal, m->forces, m->dscr, m->status};
+                  m->red, m->scal, m->forces, m->dscr, m->status, m->flags, m->ticket, m->part, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->s0, m->pair_ptr, m->pairs};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (m->h_scal) cudaFreeHost(m->h_scal);
+  for (auto &a : m->arnoldi)
+    for (auto &b : a)
+      for (auto &g : b)
+        if (g) cudaGraphExecDestroy(g);
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
   h->dev = nullptr;
@@ -318,6 +344,29 @@ DevMesh *kf_device(const GEOMETRY *g)
     KF_CUDA(upload(&m->inc_blk, blk.data(), ninc));
     KF_CUDA(upload(&m->inc_w, w.data(), 3 * ninc));
   }
+  // two-pass residual structure: edges sorted by n0 with n0 < n1 everywhere
+  {
+    bool ok = true;
+    for (uint32_t e = 0; e < E && ok; e++) {
+      if (n0[e] >= n1[e]) ok = false;
+      if (e && n0[e] < n0[e - 1]) ok = false;
+    }
+    const char *env = getenv("KFUN3D_RESIDUAL");
+    m->two_pass = ok && !(env && strcmp(env, "gather") == 0);
+    if (m->two_pass) {
+      std::vector<uint32_t> eoff(N + 1, 0), iptr(N + 1, 0), iedge(E);
+      for (uint32_t e = 0; e < E; e++) { eoff[n0[e] + 1]++; iptr[n1[e] + 1]++; }
+      for (uint32_t i = 0; i < N; i++) { eoff[i + 1] += eoff[i]; iptr[i + 1] += iptr[i]; }
+      std::vector<uint32_t> pos(iptr.begin(), iptr.end() - 1);
+      for (uint32_t e = 0; e < E; e++) iedge[pos[n1[e]]++] = e;
+      KF_CUDA(upload(&m->eoff, eoff.data(), N + 1));
+      KF_CUDA(upload(&m->n1, n1, E));
+      KF_CUDA(upload(&m->in1_ptr, iptr.data(), N + 1));
+      KF_CUDA(upload(&m->in1_edge, iedge.data(), E));
+      KF_CUDA(cudaMalloc(&m->eres, std::max<size_t>(E, 1) * sizeof(double4)));
+      KF_CUDA(cudaMalloc(&m->s0, std::max<size_t>(N, 1) * sizeof(double4)));
+    }
+  }
   // wall faces (colour order) with normals -(1/6) a x b (src/flux.c:485-508)
   {
     const unsigned int *f0 = g->b->fc->fptr->n0, *f1 = g->b->fc->fptr->n1, *f2 = g->b->fc->fptr->n2;
@@ -378,6 +427,8 @@ DevMesh *kf_device(const GEOMETRY *g)
   KF_CUDA(upload(&m->tblk, p.tblk.data(), p.tblk.size()));
   KF_CUDA(upload(&m->lpos, p.lpos.data(), p.lpos.size()));
   KF_CUDA(upload(&m->last_lower, p.last_lower.data(), p.last_lower.size()));
+  KF_CUDA(upload(&m->pair_ptr, p.pair_ptr.data(), p.pair_ptr.size()));
+  KF_CUDA(upload(&m->pairs, reinterpret_cast<const uint2 *>(p.pairs.data()), p.pairs.size() / 2));
   KF_CUDA(upload(&m->lev_l, p.lev_l.data(), p.lev_l.size()));
   KF_CUDA(upload(&m->lev_u, p.lev_u.data(), p.lev_u.size()));
   m->lev_l_ptr = p.lev_l_ptr;
@@ -407,8 +458,38 @@ DevMesh *kf_device(const GEOMETRY *g)
   KF_CUDA(cudaMalloc(&m->scal, 256 * sizeof(double)));
   KF_CUDA(cudaMemset(m->scal, 0, 256 * sizeof(double)));
   KF_CUDA(cudaMalloc(&m->forces, 4 * sizeof(double)));
-  KF_CUDA(cudaMalloc(&m->status, sizeof(int)));
-  KF_CUDA(cudaMemset(m->status, 0, sizeof(int)));
+  KF_CUDA(cudaMalloc(&m->status, 4 * sizeof(int)));
+  KF_CUDA(cudaMemset(m->status, 0, 4 * sizeof(int)));
+  KF_CUDA(cudaMalloc(&m->flags, (size_t)N * sizeof(uint32_t)));
+  KF_CUDA(cudaMemset(m->flags, 0, (size_t)N * sizeof(uint32_t)));
+  KF_CUDA(cudaMalloc(&m->ticket, sizeof(unsigned long long)));
+  KF_CUDA(cudaMemset(m->ticket, 0, sizeof(unsigned long long)));
+  {
+    int nsm = 0;
+    KF_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device));
+    // cooperative grid: 4 blocks of 256 threads per SM (the kernel's launch
+    // bounds guarantee they fit); the runtime refuses the launch otherwise
+    m->trsv_grid = (unsigned)nsm * 4;
+    std::vector<uint4> dl(N), du(N);
+    for (uint32_t s = 0; s < N; s++) {
+      const uint32_t i = p.lev_l[s];
+      dl[s] = make_uint4(i, p.ia[i], p.diag[i], 0);
+      const uint32_t k = p.lev_u[s];
+      du[s] = make_uint4(k, p.diag[k] + 1, p.ia[k + 1], 0);
+    }
+    KF_CUDA(upload(&m->desc_l, dl.data(), N));
+    KF_CUDA(upload(&m->desc_u, du.data(), N));
+    // triangular-solve schedule: "levels16" (default: one launch per level,
+    // 16 lanes per row), "syncfree" (per-row flags, no level barriers) or
+    // "levels" (one launch per level, 4 lanes per row)
+    const char *env = getenv("KFUN3D_SPTRSV");
+    m->trsv_mode = 2;
+    if (env && strcmp(env, "syncfree") == 0) m->trsv_mode = 1;
+    if (env && strcmp(env, "levels") == 0) m->trsv_mode = 0;
+    m->syncfree = m->trsv_mode == 1;
+    const char *genv = getenv("KFUN3D_GRAPHS");
+    m->use_graphs = !(genv && strcmp(genv, "0") == 0);
+  }
   KF_CUDA(cudaMallocHost(&m->h_scal, 256 * sizeof(double)));
   KF_CUDA(cudaDeviceSynchronize());
   return m;

@@ -28,6 +28,11 @@ struct HostPattern {
   std::vector<uint32_t> last_lower;  // per row: lower block the fill touches last (or ~0)
   std::vector<uint32_t> lev_l, lev_l_ptr;   // rows by forward level (matrix/init.cpp:194-232)
   std::vector<uint32_t> lev_u, lev_u_ptr;   // rows by backward level (matrix/init.cpp:234-270)
+  // ILU(0) products of block j = (i,k) in merge order (matrix/ilu.cpp:71-84):
+  // pairs [pair_ptr[j], pair_ptr[j+1]) of (L slot index or ~0 for the
+  // identity, block index of U(m,k)); the last pair is the product the
+  // reference adds back.
+  std::vector<uint32_t> pair_ptr, pairs;
 };
 
 void kf_build_pattern(HostPattern &p, size_t nnodes, size_t nedges, const unsigned int *n0,
@@ -63,6 +68,14 @@ struct DevMesh {
   uint32_t *inc_edge = nullptr;   // [2E] edge index | (1u<<31 when the node is n1)
   uint32_t *inc_blk = nullptr;    // [2E] block index of (node, other)
   double *inc_w = nullptr;        // [3][2E] least-squares terms seen from the node
+  // two-pass residual (every edge has n0 < n1)
+  bool two_pass = false;
+  uint32_t *eoff = nullptr;       // [N+1] edges with n0 = node (contiguous: edges are sorted by n0)
+  uint32_t *n1 = nullptr;         // [E]
+  uint32_t *in1_ptr = nullptr;    // [N+1] edges with n1 = node, in edge order
+  uint32_t *in1_edge = nullptr;   // [E]
+  double4 *eres = nullptr;        // [E] edge fluxes
+  double4 *s0 = nullptr;          // [N] n0-side sums (fast build)
   uint32_t *wf_nodes = nullptr;   // [3F] wall faces in colour order
   double *wf_n = nullptr;         // [3F] wall-face normals -(1/6) a x b
   uint32_t *col = nullptr;        // [ncol+1] wall-face colour offsets
@@ -79,6 +92,8 @@ struct DevMesh {
   uint32_t nlev_l = 0, nlev_u = 0;
   std::vector<uint32_t> lev_l_ptr, lev_u_ptr;   // host copies of level offsets
   uint32_t *lev_l = nullptr, *lev_u = nullptr;
+  uint32_t *pair_ptr = nullptr;   // [nnz+1]
+  uint2 *pairs = nullptr;         // [npairs] (L slot or ~0, U block)
   double *A = nullptr;            // [nnz*16]
   double *lslot = nullptr;        // [nlower*16] persistent L slots
   double *dinv = nullptr;         // [N*16] inverse diagonal blocks
@@ -92,7 +107,22 @@ struct DevMesh {
   double *scal = nullptr;         // device scalars
   double *forces = nullptr;       // [3]
   double *dscr = nullptr;         // [nb*16] double diagonal blocks of boundary rows (FP32 fill)
-  int *status = nullptr;          // device status word (pivot failures)
+  int *status = nullptr;          // device status words: [0] pivot failure, [1] wait timeout
+  // sync-free triangular solves
+  bool syncfree = true;
+  int trsv_mode = 1;               // 0 levels (4 lanes/row), 1 sync-free, 2 levels (16 lanes/row)
+  unsigned trsv_grid = 0;          // persistent grid (whole blocks resident on every SM)
+  uint32_t *flags = nullptr;       // [N] per-row completion epoch
+  unsigned long long *ticket = nullptr;   // unused (kept zero)
+  uint4 *desc_l = nullptr, *desc_u = nullptr;   // [N] (row, first block, end block) in level order
+  // fast mode: one CUDA graph per Arnoldi index (jacobian-vector product,
+  // triangular solves, Gram-Schmidt, read-back of the Hessenberg column)
+  cudaGraphExec_t arnoldi[2][2][KF_NBASIS] = {};   // [precision][first order][k]
+  unsigned arnoldi_nodes[2][2][KF_NBASIS] = {};
+  double graph_aoa = 0.0;
+  bool use_graphs = true;
+  unsigned mgs_grid = 0;          // cooperative grid for the Gram-Schmidt kernel
+  double *part = nullptr;         // [2][mgs_grid] block partial sums
   double *h_scal = nullptr;       // pinned host mirror of scal
   bool factored = false;
   bool a_valid = false;
@@ -101,6 +131,7 @@ struct DevMesh {
 DevMesh *kf_device(const GEOMETRY *g);   // creates and uploads on first use
 
 void kf_count_launch(unsigned n = 1);
+void kfun3d_reset_launch_count_by(unsigned long long n);   // undo counts taken during graph capture
 
 // Kernel families, one set per arithmetic mode (kernels_exact.cu, kernels_fast.cu).
 #define KF_DECLARE_KERNELS(NS)                                                          \

@@ -314,6 +314,74 @@ __global__ void __launch_bounds__(128) k_residual(uint32_t N, const uint32_t *__
   r[n] = acc;
 }
 
+// Two-pass residual, used when every edge has n0 < n1 (edges sorted by n0).
+// Then a node's edges as n1 all precede its edges as n0 in edge order, so the
+// reference's per-node sum in edge order is: subtract the n1-side fluxes in
+// edge order, then add the n0-side fluxes in edge order.  Pass 1 evaluates
+// each edge's flux once (thread per n0 node over its contiguous edges) and
+// stores it; in the fast build it also keeps the n0-side sum.  Pass 2 gathers.
+template <bool FIRST_ORDER, bool FAST>
+__global__ void __launch_bounds__(128) k_flux_edges(uint32_t N, const uint32_t *__restrict__ eoff,
+                                                    const uint32_t *__restrict__ n1,
+                                                    const double4 *__restrict__ egeo,
+                                                    const double4 *__restrict__ xyz,
+                                                    const double4 *__restrict__ q,
+                                                    const double4 *__restrict__ gx,
+                                                    const double4 *__restrict__ gy,
+                                                    const double4 *__restrict__ gz, double4 *__restrict__ res,
+                                                    double4 *__restrict__ s0)
+{
+  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const uint32_t e0 = eoff[n], e1 = eoff[n + 1];
+  double4 acc = make_double4(0, 0, 0, 0);
+  if (e0 < e1) {
+    const double4 qa = q[n], xa = xyz[n];
+    double4 gxa, gya, gza;
+    if (!FIRST_ORDER) { gxa = gx[n]; gya = gy[n]; gza = gz[n]; }
+    for (uint32_t e = e0; e < e1; e++) {
+      const uint32_t o = n1[e];
+      const double4 geo = egeo[e];
+      const double4 qb = q[o], xb = xyz[o];
+      const double xm = 0.5 * (xa.x + xb.x), ym = 0.5 * (xa.y + xb.y), zm = 0.5 * (xa.z + xb.z);
+      double4 sL, sR;
+      if (FIRST_ORDER) {
+        const double4 z = make_double4(0, 0, 0, 0);
+        sL = recon(qa, z, z, z, xm - xa.x, ym - xa.y, zm - xa.z);
+        sR = recon(qb, z, z, z, xm - xb.x, ym - xb.y, zm - xb.z);
+      } else {
+        sL = recon(qa, gxa, gya, gza, xm - xa.x, ym - xa.y, zm - xa.z);
+        sR = recon(qb, gx[o], gy[o], gz[o], xm - xb.x, ym - xb.y, zm - xb.z);
+      }
+      const double4 f = edge_flux(geo, sL, sR);
+      res[e] = f;
+      if (FAST) acc = add4(acc, f);
+    }
+  }
+  if (FAST) s0[n] = acc;
+}
+
+template <bool FAST>
+__global__ void __launch_bounds__(256) k_flux_nodes(uint32_t N, const uint32_t *__restrict__ in1_ptr,
+                                                    const uint32_t *__restrict__ in1_edge,
+                                                    const uint32_t *__restrict__ eoff,
+                                                    const double4 *__restrict__ res,
+                                                    const double4 *__restrict__ s0, double4 *__restrict__ r)
+{
+  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double4 acc = make_double4(0, 0, 0, 0);
+  const uint32_t k1 = in1_ptr[n + 1];
+  for (uint32_t k = in1_ptr[n]; k < k1; k++) acc = sub4(acc, res[in1_edge[k]]);
+  if (FAST) {
+    acc = add4(s0[n], acc);
+  } else {
+    const uint32_t e1 = eoff[n + 1];
+    for (uint32_t e = eoff[n]; e < e1; e++) acc = add4(acc, res[e]);
+  }
+  r[n] = acc;
+}
+
 // Boundary terms, after all edges: wall faces by colour (src/flux.c:467-539),
 // then far-field nodes (src/flux.c:541-779), each node in list order.
 __global__ void k_residual_boundary(uint32_t nb, const uint32_t *__restrict__ bnd_node,
@@ -788,6 +856,79 @@ __global__ void __launch_bounds__(128) k_ilu_level(uint32_t nrows, const uint32_
   }
 }
 
+// Same sweep with the merge precomputed: the products of block (i,k) come from
+// its pair list (L slot or identity, U block) in merge order, so all loads of
+// a product are issued at once instead of walking two index lists.  Lane l16
+// owns entry l16 of every block, so the L slots this row wrote earlier are
+// read back by the lane that wrote them.
+__global__ void __launch_bounds__(128) k_ilu_level_pairs(uint32_t nrows, const uint32_t *__restrict__ rows,
+                                                         const uint32_t *__restrict__ ia,
+                                                         const uint32_t *__restrict__ ja,
+                                                         const uint32_t *__restrict__ diag,
+                                                         const uint32_t *__restrict__ pair_ptr,
+                                                         const uint2 *__restrict__ pairs,
+                                                         const uint32_t *__restrict__ lpos, double *__restrict__ A,
+                                                         double *__restrict__ lslot, double *__restrict__ dinv,
+                                                         int *__restrict__ status)
+{
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t grp = gid >> 4;
+  const int lane = threadIdx.x & 31, l16 = lane & 15, base = lane & 16;
+  const unsigned mask = 0xffffu << base;
+  if (grp >= nrows) return;
+  const uint32_t i = rows[grp];
+  const uint32_t j0 = ia[i], j1 = ia[i + 1];
+  const double ident = ((l16 >> 2) == (l16 & 3)) ? 1.0 : 0.0;
+  for (uint32_t j = j0; j < j1; j++) {
+    const uint32_t k = ja[j];
+    double a = A[16 * (size_t)j + l16];
+    double d = 0.0;
+    const uint32_t p0 = pair_ptr[j], p1 = pair_ptr[j + 1];
+    for (uint32_t pb = p0; pb < p1; pb += 8) {
+      double lv[8], uv[8];
+      const uint32_t cnt = (p1 - pb) < 8 ? (p1 - pb) : 8;
+#pragma unroll
+      for (int t = 0; t < 8; t++) {
+        lv[t] = 0.0;
+        uv[t] = 0.0;
+        if ((uint32_t)t < cnt) {
+          const uint2 pr = pairs[pb + t];
+          lv[t] = pr.x == 0xffffffffu ? ident : lslot[16 * (size_t)pr.x + l16];
+          uv[t] = A[16 * (size_t)pr.y + l16];
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < 8; t++) {
+        if ((uint32_t)t >= cnt) break;
+        d = gemm_lane(lv[t], uv[t], l16, mask, base);
+        a = -1.0 * d + a;
+      }
+    }
+    a = 1.0 * d + a;
+    if (k < i) {
+      const double dk = dinv[16 * (size_t)k + l16];
+      lslot[16 * (size_t)(lpos[i] + (j - j0)) + l16] = gemm_lane(a, dk, l16, mask, base);
+    } else {
+      A[16 * (size_t)j + l16] = a;
+      if (k == i) {
+        __syncwarp(mask);
+        if (l16 == 0) {
+          double s[16], o[16];
+          for (int t = 0; t < 16; t++) s[t] = A[16 * (size_t)j + t];
+          inv4(s, o);
+          bool bad = false;
+          for (int t = 0; t < 16; t++) {
+            dinv[16 * (size_t)i + t] = o[t];
+            bad |= !isfinite(o[t]);
+          }
+          if (bad) atomicExch(status, KFUN3D_ERR_PIVOT);
+        }
+        __syncwarp(mask);
+      }
+    }
+  }
+}
+
 // matrix/ilu.cpp:115-136: the factor over A, lower blocks from the L slots,
 // diagonal blocks inverted.
 __global__ void k_ilu_finish(uint32_t N, const uint32_t *__restrict__ ia, const uint32_t *__restrict__ diag,
@@ -945,6 +1086,181 @@ __global__ void __launch_bounds__(128) k_trsv_upper(uint32_t nrows, const uint32
   x[4 * (size_t)i + rr] = t;
 }
 
+// Level-synchronous sweep, one launch per level: 16 lanes per row
+// (lane = 4*block + component); every load of a row (its blocks, their
+// columns, and the already final x of those columns) is issued at once, then
+// the products are subtracted in column order exactly as in
+// matrix/sptrsv.cpp:173-209.  desc holds (row, first block, end block) in
+// level order; rows [s0, s1) are this level.
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(256) k_trsv_level16(uint32_t s0, uint32_t s1, const uint4 *__restrict__ desc,
+                                                      const uint32_t *__restrict__ ja, const T *__restrict__ A,
+                                                      const double *__restrict__ b, double *__restrict__ x)
+{
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t slot = s0 + (gid >> 4);
+  const int lane = threadIdx.x & 31, half = lane >> 4, l16 = lane & 15, jj = l16 >> 2, r = l16 & 3;
+  const unsigned hmask = 0xffffu << (16 * half);
+  if (slot >= s1) return;
+  const uint4 d = desc[slot];
+  const uint32_t i = d.x, jb = d.y, je = d.z;
+  double xi = UPPER ? x[4 * (size_t)i + r] : b[4 * (size_t)i + r];
+  for (uint32_t c0 = jb; c0 < je; c0 += 16) {
+    double t[4];
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const uint32_t j = c0 + 4 * p + jj;
+      t[p] = 0.0;
+      if (j < je) {
+        const uint32_t col = ja[j];
+        const T *blk = A + 16 * (size_t)j + 4 * r;
+        const double4 xc = reinterpret_cast<const double4 *>(x)[col];
+        double s = 0.0;
+        s += (double)blk[0] * xc.x;
+        s += (double)blk[1] * xc.y;
+        s += (double)blk[2] * xc.z;
+        s += (double)blk[3] * xc.w;
+        t[p] = s;
+      }
+    }
+    const uint32_t cnt = (je - c0) < 16u ? (je - c0) : 16u;
+#pragma unroll
+    for (int p = 0; p < 4; p++)
+      for (uint32_t q = 0; q < 4; q++) {
+        if (4 * p + q >= cnt) break;
+        xi = -1.0 * __shfl_sync(hmask, t[p], 16 * half + 4 * q + r) + xi;
+      }
+  }
+  if (UPPER) {
+    const int b4 = 16 * half;
+    const double x0 = __shfl_sync(hmask, xi, b4 + 0), x1 = __shfl_sync(hmask, xi, b4 + 1);
+    const double x2 = __shfl_sync(hmask, xi, b4 + 2), x3 = __shfl_sync(hmask, xi, b4 + 3);
+    const T *dg = A + 16 * (size_t)(jb - 1) + 4 * r;
+    double y = 0.0;
+    y += (double)dg[0] * x0;
+    y += (double)dg[1] * x1;
+    y += (double)dg[2] * x2;
+    y += (double)dg[3] * x3;
+    xi = y;
+  }
+  if (l16 < 4) x[4 * (size_t)i + r] = xi;
+}
+
+// ------------------------------------------------------------------ sync-free SpTRSV
+
+// Bounded wait for a row's completion flag (device scope, acquire).
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p)
+{
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release(uint32_t *p, uint32_t v)
+{
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+constexpr uint32_t KF_SPIN_LIMIT = 1u << 20;   // polls (about 0.1-0.5 s) before a wait is declared failed
+
+// One triangular sweep without level barriers (matrix/sptrsv.cpp:34-73).
+// Launched cooperatively, so every block of the grid is resident at once.
+// Half-warp h (of H) owns the rows at level-order positions h, h+H, h+2H, ...
+// and works them in that order.  desc[slot] = (row, first block, end block)
+// in level order.  For a row, the 16 lanes (lane = 4*block + component) first
+// load all of the row's blocks (up to KF_TRSV_MAXB, four per pass), then wait
+// until each block's column row has published its result (flag == epoch),
+// form the block-vector products, and subtract them from x_i in column order;
+// every row's arithmetic is the reference's (products summed from zero in
+// column order, subtracted in block order), only the schedule differs.
+// Deadlock-free: the unfinished row with the smallest position has all its
+// dependencies done, and its owner, being resident and having finished its
+// earlier rows, is working on it.  A wait that exceeds KF_SPIN_LIMIT polls
+// records an error in *err, after which every other wait gives up too.
+constexpr int KF_TRSV_MAXB = 16;   // blocks per row held in registers (longer rows loop)
+
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(256, 4) k_trsv_syncfree(uint32_t N, const uint4 *__restrict__ desc,
+                                                          const uint32_t *__restrict__ ja,
+                                                          const T *__restrict__ A, const double *__restrict__ b,
+                                                          double *x, uint32_t *flags, uint32_t epoch, int *err)
+{
+  const int lane = threadIdx.x & 31, half = lane >> 4, l16 = lane & 15, jj = l16 >> 2, r = l16 & 3;
+  const unsigned hmask = 0xffffu << (16 * half);
+  const uint32_t H = gridDim.x * (blockDim.x >> 4);
+  const uint32_t h = blockIdx.x * (blockDim.x >> 4) + (threadIdx.x >> 4);
+  for (uint32_t slot = h; slot < N; slot += H) {
+    const uint4 d = desc[slot];
+    const uint32_t i = d.x, jb = d.y, je = d.z;
+    double xi = UPPER ? __ldcg(x + 4 * (size_t)i + r) : b[4 * (size_t)i + r];
+    for (uint32_t c0 = jb; c0 < je; c0 += KF_TRSV_MAXB) {
+      // 1. all loads that do not depend on other rows
+      double a[4][4];
+      uint32_t col[4];
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        const uint32_t j = c0 + 4 * p + jj;
+        col[p] = 0xffffffffu;
+        a[p][0] = a[p][1] = a[p][2] = a[p][3] = 0.0;
+        if (j < je) {
+          col[p] = ja[j];
+          const T *blk = A + 16 * (size_t)j + 4 * r;
+          a[p][0] = (double)blk[0]; a[p][1] = (double)blk[1];
+          a[p][2] = (double)blk[2]; a[p][3] = (double)blk[3];
+        }
+      }
+      // 2. wait for the column rows, then the products
+      double t[4];
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        t[p] = 0.0;
+        if (col[p] != 0xffffffffu) {
+          uint32_t spins = 0;
+          while (ld_acquire(flags + col[p]) != epoch) {
+            if (++spins > KF_SPIN_LIMIT) { atomicExch(err, 1); break; }
+            if ((spins & 63) == 0 && *(volatile int *)err) break;
+          }
+          const double2 x01 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)col[p]);
+          const double2 x23 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)col[p] + 1);
+          double s = 0.0;
+          s += a[p][0] * x01.x;
+          s += a[p][1] * x01.y;
+          s += a[p][2] * x23.x;
+          s += a[p][3] * x23.y;
+          t[p] = s;
+        }
+      }
+      // 3. subtract in column order
+      const uint32_t cnt = (je - c0) < (uint32_t)KF_TRSV_MAXB ? (je - c0) : (uint32_t)KF_TRSV_MAXB;
+#pragma unroll
+      for (int p = 0; p < 4; p++)
+        for (uint32_t q = 0; q < 4; q++) {
+          if (4 * p + q >= cnt) break;
+          const double tq = __shfl_sync(hmask, t[p], 16 * half + 4 * q + r);
+          xi = -1.0 * tq + xi;
+        }
+    }
+    if (UPPER) {
+      const int b4 = 16 * half;
+      const double x0 = __shfl_sync(hmask, xi, b4 + 0), x1 = __shfl_sync(hmask, xi, b4 + 1);
+      const double x2 = __shfl_sync(hmask, xi, b4 + 2), x3 = __shfl_sync(hmask, xi, b4 + 3);
+      const T *dg = A + 16 * (size_t)(jb - 1) + 4 * r;
+      double y = 0.0;
+      y += (double)dg[0] * x0;
+      y += (double)dg[1] * x1;
+      y += (double)dg[2] * x2;
+      y += (double)dg[3] * x3;
+      xi = y;
+    }
+    if (l16 < 4) {
+      __stcg(x + 4 * (size_t)i + r, xi);
+      __threadfence();
+    }
+    __syncwarp(hmask);
+    if (l16 == 0) st_release(flags + i, epoch);
+  }
+}
+
 // ------------------------------------------------------------------ J.v
 
 // src/kernel.c:35-44: y = (y - r + cdt (w - q)) * a, a = |x| / h from the
@@ -983,7 +1299,18 @@ void gradient(DevMesh &m, const double *q)
 
 void residual(DevMesh &m, const double *q, double *r, int first_order, double u, double v)
 {
-  if (first_order)
+  if (m.two_pass) {
+    const double4 *G[3] = {(const double4 *)m.gx, (const double4 *)m.gy, (const double4 *)m.gz};
+    if (first_order)
+      k_flux_edges<true, KF_FAST><<<blocks(m.N, 128), 128, 0, m.stream>>>(
+          m.N, m.eoff, m.n1, m.egeo, m.xyz, (const double4 *)q, nullptr, nullptr, nullptr, m.eres, m.s0);
+    else
+      k_flux_edges<false, KF_FAST><<<blocks(m.N, 128), 128, 0, m.stream>>>(
+          m.N, m.eoff, m.n1, m.egeo, m.xyz, (const double4 *)q, G[0], G[1], G[2], m.eres, m.s0);
+    k_flux_nodes<KF_FAST><<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.in1_ptr, m.in1_edge, m.eoff, m.eres, m.s0,
+                                                                  (double4 *)r);
+    kf_count_launch(2);
+  } else if (first_order)
     k_residual<true><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo, m.xyz,
                                                             (const double4 *)q, nullptr, nullptr, nullptr,
                                                             (double4 *)r);
@@ -992,7 +1319,7 @@ void residual(DevMesh &m, const double *q, double *r, int first_order, double u,
                                                              (const double4 *)q, (const double4 *)m.gx,
                                                              (const double4 *)m.gy, (const double4 *)m.gz,
                                                              (double4 *)r);
-  kf_count_launch();
+  if (!m.two_pass) kf_count_launch();
   if (m.nb) {
     k_residual_boundary<<<blocks(m.nb, 64), 64, 0, m.stream>>>(m.nb, m.bnd_node, m.bnd_ptr, m.bnd_ent, m.wf_nodes,
                                                                m.wf_n, m.f_n, (const double4 *)q, (double4 *)r, u, v);
@@ -1044,7 +1371,11 @@ void ilu(DevMesh &m, int precision)
   int *status = m.status;
   for (uint32_t l = 0; l < m.nlev_l; l++) {
     const uint32_t r0 = m.lev_l_ptr[l], nr = m.lev_l_ptr[l + 1] - r0;
-    if (precision == 0)
+    if (precision == 0 && m.pairs)
+      k_ilu_level_pairs<<<blocks((size_t)nr * 16, 128), 128, 0, m.stream>>>(nr, m.lev_l + r0, m.ia, m.ja, m.diag,
+                                                                            m.pair_ptr, m.pairs, m.lpos, m.A,
+                                                                            m.lslot, m.dinv, status);
+    else if (precision == 0)
       k_ilu_level<<<blocks((size_t)nr * 16, 128), 128, 0, m.stream>>>(nr, m.lev_l + r0, m.ia, m.ja, m.diag, m.tblk,
                                                                       m.lpos, m.A, m.lslot, m.dinv, status);
     else
@@ -1061,6 +1392,58 @@ void ilu(DevMesh &m, int precision)
 
 void sptrsv(DevMesh &m, const double *b, double *x, int precision)
 {
+  if (m.trsv_mode == 2) {
+    for (int pass = 0; pass < 2; pass++) {
+      const std::vector<uint32_t> &ptr = pass == 0 ? m.lev_l_ptr : m.lev_u_ptr;
+      const uint4 *desc = pass == 0 ? m.desc_l : m.desc_u;
+      for (size_t l = 0; l + 1 < ptr.size(); l++) {
+        const uint32_t s0 = ptr[l], s1 = ptr[l + 1];
+        const unsigned nb = blocks((size_t)(s1 - s0) * 16, 256);
+        if (precision == 0) {
+          if (pass == 0) k_trsv_level16<double, false><<<nb, 256, 0, m.stream>>>(s0, s1, desc, m.ja, m.A, b, x);
+          else k_trsv_level16<double, true><<<nb, 256, 0, m.stream>>>(s0, s1, desc, m.ja, m.A, b, x);
+        } else {
+          if (pass == 0) k_trsv_level16<float, false><<<nb, 256, 0, m.stream>>>(s0, s1, desc, m.ja, m.Af, b, x);
+          else k_trsv_level16<float, true><<<nb, 256, 0, m.stream>>>(s0, s1, desc, m.ja, m.Af, b, x);
+        }
+        kf_count_launch();
+      }
+    }
+    return;
+  }
+  if (m.syncfree) {
+    // flags restart from zero on every solve (graph-capturable); epoch 1
+    // marks rows done in the lower sweep, 2 in the upper sweep
+    cudaMemsetAsync(m.flags, 0, (size_t)m.N * sizeof(uint32_t), m.stream);
+    const double *bb = b;
+    uint32_t N = m.N, eL = 1, eU = 2;
+    int *err = m.status + 1;
+    auto launch = [&](const void *fn, const uint4 *desc, uint32_t *e) {
+      const void *Ap = precision == 0 ? (const void *)m.A : (const void *)m.Af;
+      void *args[] = {&N, (void *)&desc, (void *)&m.ja, (void *)&Ap, (void *)&bb, (void *)&x, (void *)&m.flags,
+                      e, (void *)&err};
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(m.trsv_grid);
+      cfg.blockDim = dim3(256);
+      cfg.stream = m.stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeCooperative;
+      attr[0].val.cooperative = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      const cudaError_t e2 = cudaLaunchKernelExC(&cfg, fn, args);
+      if (e2 != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e2));
+    };
+    if (precision == 0) {
+      launch((const void *)k_trsv_syncfree<double, false>, m.desc_l, &eL);
+      launch((const void *)k_trsv_syncfree<double, true>, m.desc_u, &eU);
+    } else {
+      launch((const void *)k_trsv_syncfree<float, false>, m.desc_l, &eL);
+      launch((const void *)k_trsv_syncfree<float, true>, m.desc_u, &eU);
+    }
+    kf_count_launch(2);
+    return;
+  }
   for (uint32_t l = 0; l < m.nlev_l; l++) {
     const uint32_t r0 = m.lev_l_ptr[l], nr = m.lev_l_ptr[l + 1] - r0;
     if (precision == 0)

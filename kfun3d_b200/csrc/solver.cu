@@ -13,7 +13,11 @@
 #include <string>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "internal.h"
+
+namespace cg = cooperative_groups;
 
 extern int g_kf_verbose;
 
@@ -95,6 +99,94 @@ __global__ void k_dot_final(const double *__restrict__ part, int np, double *__r
   }
 }
 
+// Fast-mode modified Gram-Schmidt of V[k+1] against V[0..k] and its
+// normalisation (src/kernel.c:129-141) in one cooperative launch.  Pass v
+// applies the previous projection, w -= h[v-1] V[v-1], and forms the block
+// partial sums of w.V[v] in the same sweep; after a grid-wide barrier every
+// block adds the partial sums in the same fixed order, so all blocks hold the
+// identical h[v] (run-to-run deterministic).  Partial sums alternate between
+// two buffers, so one barrier per projection suffices.
+__device__ __forceinline__ double block_sum(double v, double *sm)
+{
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) sm[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x < 32) {
+    t = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0.0;
+    t = warp_sum(t);
+  }
+  __syncthreads();
+  return t;   // valid in thread 0
+}
+
+__device__ __forceinline__ double grid_total(const double *part, int np, double *sm)
+{
+  double v = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) v += part[i];
+  v = block_sum(v, sm);
+  if (threadIdx.x == 0) sm[32] = v;
+  __syncthreads();
+  const double t = sm[32];
+  __syncthreads();
+  return t;
+}
+
+__global__ void __launch_bounds__(256) k_mgs_coop(size_t n, double *__restrict__ V, int k,
+                                                  double *__restrict__ h, double *__restrict__ part)
+{
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sm[40];
+  const int G = gridDim.x;
+  const size_t n2 = n / 2;
+  double2 *w = reinterpret_cast<double2 *>(V + (size_t)(k + 1) * n);
+  const size_t stride = (size_t)G * blockDim.x;
+  const size_t i0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double hprev = 0.0;
+  for (int v = 0; v <= k + 1; v++) {
+    const double2 *prev = v > 0 ? reinterpret_cast<const double2 *>(V + (size_t)(v - 1) * n) : nullptr;
+    const double2 *cur = v <= k ? reinterpret_cast<const double2 *>(V + (size_t)v * n) : nullptr;
+    double s = 0.0;
+    for (size_t i = i0; i < n2; i += stride) {
+      double2 a = w[i];
+      if (prev) {
+        const double2 p = prev[i];
+        a.x = fma(-hprev, p.x, a.x);
+        a.y = fma(-hprev, p.y, a.y);
+        w[i] = a;
+      }
+      if (cur) {
+        const double2 c = __ldcs(cur + i);
+        s = fma(a.x, c.x, s);
+        s = fma(a.y, c.y, s);
+      } else {
+        s = fma(a.x, a.x, s);
+        s = fma(a.y, a.y, s);
+      }
+    }
+    double *pb = part + (v & 1) * G;
+    const double bs = block_sum(s, sm);
+    if (threadIdx.x == 0) pb[blockIdx.x] = bs;
+    grid.sync();
+    const double tot = grid_total(pb, G, sm);
+    if (v <= k) {
+      hprev = tot;
+      if (blockIdx.x == 0 && threadIdx.x == 0) h[v] = tot;
+    } else {
+      const double nrm = sqrt(tot);
+      if (blockIdx.x == 0 && threadIdx.x == 0) h[k + 1] = nrm;
+      const double sc = 1.0 / nrm;
+      for (size_t i = i0; i < n2; i += stride) {
+        double2 a = w[i];
+        a.x *= sc;
+        a.y *= sc;
+        w[i] = a;
+      }
+    }
+  }
+}
+
 // y = (mult * coef[0]) * x + y with the coefficient on the device
 __global__ void k_axpy_dev(size_t n, const double *__restrict__ coef, double mult, const double *__restrict__ x,
                            double *__restrict__ y, int fast)
@@ -147,41 +239,73 @@ __global__ void k_set_h(double *scal)
 }
 
 // src/forces.c:8-120 in the reference's order: per colour an OpenMP
-// reduction from zero, added to the running total.
-__global__ void k_forces(uint32_t ncol, const uint32_t *__restrict__ col, const uint32_t *__restrict__ wf,
-                         const double4 *__restrict__ xyz, const double4 *__restrict__ q, double U, double V,
-                         double *__restrict__ out)
+// reduction from zero over the colour's faces in face order, each colour's sum
+// then added to the running total.  One warp per colour: the lanes form 32
+// faces' products at once, then every lane applies them to the running sums
+// in face order (lift = (lift - dcx V) + dcy U, drag = (drag + dcx U) + dcy V,
+// momn = (momn + (xmid - 1/4) dcy) - ymid dcx), so the arithmetic is the
+// reference's.  The colour sums are added in colour order by one thread.
+__global__ void __launch_bounds__(1024) k_forces(uint32_t ncol, const uint32_t *__restrict__ col,
+                                                 const uint32_t *__restrict__ wf, const double4 *__restrict__ xyz,
+                                                 const double4 *__restrict__ q, double U, double V,
+                                                 double *__restrict__ out)
 {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double lift = 0.0, drag = 0.0, momn = 0.0;
-  for (uint32_t c = 0; c < ncol; c++) {
+  __shared__ double part[3 * 1024];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (uint32_t c = warp; c < ncol; c += nw) {
     double l = 0.0, d = 0.0, m = 0.0;
-    for (uint32_t j = col[c]; j < col[c + 1]; j++) {
-      const uint32_t a = wf[3 * j], b = wf[3 * j + 1], e = wf[3 * j + 2];
-      const double4 pa = xyz[a], pb = xyz[b], pe = xyz[e];
-      const double ax = pb.x - pa.x, ay = pb.y - pa.y, az = pb.z - pa.z;
-      const double bx = pe.x - pa.x, by = pe.y - pa.y, bz = pe.z - pa.z;
-      double xnorm = ay * bz; xnorm -= az * by; xnorm = -0.5 * xnorm;
-      double ynorm = ax * bz; ynorm -= az * bx; ynorm = 0.5 * ynorm;
-      const double press = (q[a].x + q[b].x + q[e].x) / 3.0;
-      const double cp = 2.0 * (press - 1.0);
-      const double dcx = cp * xnorm, dcy = cp * ynorm;
-      const double xmid = pa.x + pb.x + pe.x;
-      const double ymid = pa.y + pb.y + pe.y;
-      l = l - dcx * V + dcy * U;
-      d = d + dcx * U + dcy * V;
-      m = m + (xmid - 0.25) * dcy - ymid * dcx;
+    for (uint32_t base = col[c]; base < col[c + 1]; base += 32) {
+      const uint32_t j = base + lane;
+      double a1 = 0, a2 = 0, b1 = 0, b2 = 0, c1 = 0, c2 = 0;
+      if (j < col[c + 1]) {
+        const uint32_t a = wf[3 * j], b = wf[3 * j + 1], e = wf[3 * j + 2];
+        const double4 pa = xyz[a], pb = xyz[b], pe = xyz[e];
+        const double ax = pb.x - pa.x, ay = pb.y - pa.y, az = pb.z - pa.z;
+        const double bx = pe.x - pa.x, by = pe.y - pa.y, bz = pe.z - pa.z;
+        double xnorm = ay * bz; xnorm -= az * by; xnorm = -0.5 * xnorm;
+        double ynorm = ax * bz; ynorm -= az * bx; ynorm = 0.5 * ynorm;
+        const double press = (q[a].x + q[b].x + q[e].x) / 3.0;
+        const double cp = 2.0 * (press - 1.0);
+        const double dcx = cp * xnorm, dcy = cp * ynorm;
+        const double xmid = pa.x + pb.x + pe.x;
+        const double ymid = pa.y + pb.y + pe.y;
+        a1 = dcx * V; a2 = dcy * U;
+        b1 = dcx * U; b2 = dcy * V;
+        c1 = (xmid - 0.25) * dcy; c2 = ymid * dcx;
+      }
+      const uint32_t cnt = min(32u, col[c + 1] - base);
+      for (uint32_t k = 0; k < cnt; k++) {
+        l = l - __shfl_sync(0xffffffffu, a1, k);
+        l = l + __shfl_sync(0xffffffffu, a2, k);
+        d = d + __shfl_sync(0xffffffffu, b1, k);
+        d = d + __shfl_sync(0xffffffffu, b2, k);
+        m = m + __shfl_sync(0xffffffffu, c1, k);
+        m = m - __shfl_sync(0xffffffffu, c2, k);
+      }
     }
-    lift += l;
-    drag += d;
-    momn += m;
+    if (lane == 0 && c < 1024) {
+      part[3 * c] = l;
+      part[3 * c + 1] = d;
+      part[3 * c + 2] = m;
+    }
   }
-  out[0] = lift;
-  out[1] = drag;
-  out[2] = momn;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double lift = 0.0, drag = 0.0, momn = 0.0;
+    for (uint32_t c = 0; c < ncol && c < 1024; c++) {
+      lift += part[3 * c];
+      drag += part[3 * c + 1];
+      momn += part[3 * c + 2];
+    }
+    out[0] = lift;
+    out[1] = drag;
+    out[2] = momn;
+  }
 }
 
 // ------------------------------------------------------------------ helpers
+
+unsigned forces_threads(uint32_t ncol) { return 32u * std::min<uint32_t>(std::max<uint32_t>(ncol, 1u), 32u); }
 
 bool check_cuda(const char *what)
 {
@@ -291,6 +415,36 @@ void dev_normalize(DevMesh &m, double *x, double *nrm, bool fast)
   kf_count_launch();
 }
 
+void mgs_coop_prepare(DevMesh &m)
+{
+  if (!m.mgs_grid) {
+    int nsm = 0, per = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m.device));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mgs_coop, 256, 0));
+    m.mgs_grid = (unsigned)nsm * (unsigned)std::min(std::max(per, 1), 2);
+    CK(cudaMalloc(&m.part, 2 * m.mgs_grid * sizeof(double)));
+  }
+}
+
+void mgs_coop(DevMesh &m, int k)
+{
+  mgs_coop_prepare(m);
+  size_t n = 4 * (size_t)m.N;
+  double *V = m.V, *h = m.scal, *part = m.part;
+  void *args[] = {&n, &V, &k, &h, &part};
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(m.mgs_grid);
+  cfg.blockDim = dim3(256);
+  cfg.stream = m.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelExC(&cfg, (const void *)k_mgs_coop, args));
+  kf_count_launch();
+}
+
 // One Arnoldi step k (src/kernel.c:123-141): V[k+1] = M^-1 J V[k],
 // modified Gram-Schmidt against V[0..k], normalised; h in scal[0..k+1].
 void arnoldi_step(DevMesh &m, const Ops &o, int k, int prec)
@@ -298,6 +452,10 @@ void arnoldi_step(DevMesh &m, const Ops &o, int k, int prec)
   const size_t n = 4 * (size_t)m.N;
   dev_jacvec(m, o, Vb(m, k), m.t);
   o.sptrsv(m, m.t, Vb(m, k + 1), prec);
+  if (o.fast && (n % 2) == 0) {
+    mgs_coop(m, k);
+    return;
+  }
   for (int v = 0; v <= k; v++) {
     dev_reduce(m, Vb(m, k + 1), Vb(m, v), m.scal + v, 0, o.fast);
     k_axpy_dev<<<nblk(n, 256), 256, 0, m.stream>>>(n, m.scal + v, -1.0, Vb(m, v), Vb(m, k + 1), o.fast);
@@ -306,15 +464,62 @@ void arnoldi_step(DevMesh &m, const Ops &o, int k, int prec)
   dev_normalize(m, Vb(m, k + 1), m.scal + k + 1, o.fast);
 }
 
+// Fast mode: the Arnoldi step and the read-back of its Hessenberg column as
+// one CUDA graph per (precision, first order, k), captured on first use.
+void arnoldi_step_graph(DevMesh &m, const Ops &o, int k, int prec)
+{
+  const int fo = kf_first_order();
+  double u, v;
+  kfun3d_get_freestream(&u, &v);
+  if (m.graph_aoa != kfun3d_get_aoa()) {
+    for (auto &a : m.arnoldi)
+      for (auto &b : a)
+        for (auto &g : b)
+          if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    m.graph_aoa = kfun3d_get_aoa();
+  }
+  cudaGraphExec_t &ge = m.arnoldi[prec][fo][k];
+  if (!ge) {
+    mgs_coop_prepare(m);
+    const unsigned long long before = kfun3d_launch_count();
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(m.stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      arnoldi_step(m, o, k, prec);
+      cudaMemcpyAsync(m.h_scal, m.scal, (k + 2) * sizeof(double), cudaMemcpyDeviceToHost, m.stream);
+      e = cudaStreamEndCapture(m.stream, &graph);
+    }
+    const unsigned nodes = (unsigned)(kfun3d_launch_count() - before);
+    kfun3d_reset_launch_count_by(nodes);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&ge, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      // capture not available: run this solve without graphs
+      cudaGetLastError();
+      ge = nullptr;
+      m.use_graphs = false;
+      arnoldi_step(m, o, k, prec);
+      fetch(m, 0, k + 2);
+      return;
+    }
+    m.arnoldi_nodes[prec][fo][k] = nodes;
+  }
+  CK(cudaGraphLaunch(ge, m.stream));
+  kf_count_launch(m.arnoldi_nodes[prec][fo][k]);
+  CK(cudaStreamSynchronize(m.stream));
+}
+
+// Device status words: [0] pivot failure in ILU(0), [1] a bounded wait gave up.
 int device_status(DevMesh &m)
 {
-  int st = 0;
-  CK(cudaMemcpyAsync(&st, m.status, sizeof(int), cudaMemcpyDeviceToHost, m.stream));
+  int st[2] = {0, 0};
+  CK(cudaMemcpyAsync(st, m.status, 2 * sizeof(int), cudaMemcpyDeviceToHost, m.stream));
   CK(cudaStreamSynchronize(m.stream));
-  if (st) {
-    CK(cudaMemsetAsync(m.status, 0, sizeof(int), m.stream));
+  if (st[0] || st[1]) {
+    CK(cudaMemsetAsync(m.status, 0, 2 * sizeof(int), m.stream));
   }
-  return st;
+  if (st[1]) return KFUN3D_ERR_TIMEOUT;
+  return st[0];
 }
 
 }  // namespace
@@ -374,10 +579,18 @@ static int solve_device(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_param
     CK(cudaMemsetAsync(m.x, 0, n * sizeof(double), m.stream));
     o.ilu(m, prec);
     o.sptrsv(m, m.r, Vb(m, 0), prec);
-    if (device_status(m) == KFUN3D_ERR_PIVOT) {
-      kf_set_error(KFUN3D_ERR_PIVOT, "singular or non-finite pivot block in ILU(0)");
-      steps = -1;
-      break;
+    {
+      const int st = device_status(m);
+      if (st == KFUN3D_ERR_PIVOT) {
+        kf_set_error(KFUN3D_ERR_PIVOT, "singular or non-finite pivot block in ILU(0)");
+        steps = -1;
+        break;
+      }
+      if (st == KFUN3D_ERR_TIMEOUT) {
+        kf_set_error(KFUN3D_ERR_TIMEOUT, "a triangular-solve wait exceeded its bound");
+        steps = -1;
+        break;
+      }
     }
 
     double tol = 0.0;
@@ -402,8 +615,12 @@ static int solve_device(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_param
       if (total == 0) tol = p->gmres_rtol * rs[0];
       int k = 0;
       while (k < restart) {
-        arnoldi_step(m, o, k, prec);
-        fetch(m, 0, k + 2);
+        if (o.fast && m.use_graphs) {
+          arnoldi_step_graph(m, o, k, prec);
+        } else {
+          arnoldi_step(m, o, k, prec);
+          fetch(m, 0, k + 2);
+        }
         double *hh = ghh + k * (KF_NBASIS + 1);
         for (int i = 0; i <= k + 1; i++) hh[i] = m.h_scal[i];
         for (int i = 0; i < k; i++) {               // src/kernel.c:143-149
@@ -438,12 +655,17 @@ static int solve_device(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_param
     if (steps < 0) break;
     if (print) fun3d_printf(5, ">> GMRES: TOTAL ITERATIONS %d\n", total);
     dev_axpy(m, -1.0, m.x, m.q, o.fast);                           // src/kernel.c:200
-    k_forces<<<1, 32, 0, m.stream>>>(m.ncol, m.col, m.wf_nodes, m.xyz, (const double4 *)m.q, u, v, m.forces);
+    k_forces<<<1, forces_threads(m.ncol), 0, m.stream>>>(m.ncol, m.col, m.wf_nodes, m.xyz, (const double4 *)m.q, u, v, m.forces);
     kf_count_launch();
     CK(cudaEventRecord(ev1, m.stream));
     CK(cudaMemcpyAsync(m.h_scal + 48, m.forces, 3 * sizeof(double), cudaMemcpyDeviceToHost, m.stream));
     CK(cudaStreamSynchronize(m.stream));
     if (!check_cuda("solve")) { steps = -1; break; }
+    if (device_status(m) == KFUN3D_ERR_TIMEOUT) {
+      kf_set_error(KFUN3D_ERR_TIMEOUT, "a triangular-solve wait exceeded its bound");
+      steps = -1;
+      break;
+    }
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev0, ev1);
     const double lift = m.h_scal[48], drag = m.h_scal[49], momn = m.h_scal[50];
@@ -556,7 +778,9 @@ extern "C" void ComputeSparseTriangularSolve(const GEOMETRY *g, const double *b,
   h2d(*m, m->rhs, b, n);
   ops().sptrsv(*m, m->rhs, m->t, kf_precision());
   d2h(*m, x, m->t, n);
-  finish(*m, "ComputeSparseTriangularSolve");
+  if (!finish(*m, "ComputeSparseTriangularSolve")) return;
+  if (device_status(*m) == KFUN3D_ERR_TIMEOUT)
+    kf_set_error(KFUN3D_ERR_TIMEOUT, "a triangular-solve wait exceeded its bound");
 }
 
 extern "C" void ComputeForces(const GEOMETRY *g, double *forces)
@@ -566,7 +790,7 @@ extern "C" void ComputeForces(const GEOMETRY *g, double *forces)
   double u, v;
   kfun3d_get_freestream(&u, &v);
   h2d(*m, m->q, g->q->q, 4 * (size_t)m->N);
-  k_forces<<<1, 32, 0, m->stream>>>(m->ncol, m->col, m->wf_nodes, m->xyz, (const double4 *)m->q, u, v, m->forces);
+  k_forces<<<1, forces_threads(m->ncol), 0, m->stream>>>(m->ncol, m->col, m->wf_nodes, m->xyz, (const double4 *)m->q, u, v, m->forces);
   kf_count_launch();
   d2h(*m, forces, m->forces, 3);
   finish(*m, "ComputeForces");
