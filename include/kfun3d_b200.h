@@ -211,6 +211,21 @@ void kfun3d_reset_launch_count(void);
    inverted).  Returns nnz, or -1 on error; NULL outputs are skipped. */
 long kfun3d_matrix_read(const GEOMETRY *g, unsigned int *ia, unsigned int *ja, double *blocks);
 
+/* No counterpart in the reference.  Allocation-free triangular solve, for
+   callers that cannot allocate device memory: code that applies the
+   preconditioner from inside a CUDA stream capture (cudaMalloc is not allowed
+   there) or a framework that owns every device allocation.  x = (LU)^-1 b
+   with the factor of the last ComputeNumericalILU on this GEOMETRY; d_b and
+   d_x are the caller's device arrays of 4*nnodes doubles (16-byte aligned,
+   distinct).  Runs the sync-free sweep, whose per-row completion flags live
+   in a fixed device array of the library (8 MiB, held by every GPU that loads
+   the library until exit), so the call allocates nothing; at most 2,097,152
+   rows, larger matrices are rejected (KFUN3D_ERR_ARG).  The first call on a
+   device looks up that array's device address (cudaGetSymbolAddress), so make
+   it before any stream capture.  Calls share the array: calls that overlap on
+   the GPU race.  Returns KFUN3D_OK or an error code (also recorded). */
+int kfun3d_sptrsv_device_noalloc(const GEOMETRY *g, const double *d_b, double *d_x);
+
 /* Release the device mirror of g (also done by CXX_Matrix_Delete). */
 void kfun3d_device_release(GEOMETRY *g);
 

@@ -1466,6 +1466,40 @@ void sptrsv(DevMesh &m, const double *b, double *x, int precision)
   }
 }
 
+// The sync-free sweep with caller-supplied completion flags (N words, cleared
+// here), for the allocation-free entry point in noalloc.cu.
+void sptrsv_flags(DevMesh &m, const double *b, double *x, int precision, uint32_t *flags)
+{
+  cudaMemsetAsync(flags, 0, (size_t)m.N * sizeof(uint32_t), m.stream);
+  const double *bb = b;
+  uint32_t N = m.N, eL = 1, eU = 2;
+  int *err = m.status + 1;
+  auto launch = [&](const void *fn, const uint4 *desc, uint32_t *e) {
+    const void *Ap = precision == 0 ? (const void *)m.A : (const void *)m.Af;
+    void *args[] = {&N, (void *)&desc, (void *)&m.ja, (void *)&Ap, (void *)&bb, (void *)&x, (void *)&flags,
+                    e, (void *)&err};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(m.trsv_grid);
+    cfg.blockDim = dim3(256);
+    cfg.stream = m.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e2 = cudaLaunchKernelExC(&cfg, fn, args);
+    if (e2 != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e2));
+  };
+  if (precision == 0) {
+    launch((const void *)k_trsv_syncfree<double, false>, m.desc_l, &eL);
+    launch((const void *)k_trsv_syncfree<double, true>, m.desc_u, &eU);
+  } else {
+    launch((const void *)k_trsv_syncfree<float, false>, m.desc_l, &eL);
+    launch((const void *)k_trsv_syncfree<float, true>, m.desc_u, &eU);
+  }
+  kf_count_launch(2);
+}
+
 void jv_combine(DevMesh &m, double *y, const double *r, const double *w, const double *q, const double *scal, int ia)
 {
   k_jv_combine<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, y, r, w, q, m.cdt, scal, ia);
