@@ -245,7 +245,7 @@ static void release_device(MatrixHandle *h)
                   m->wf_n, m->s_n, m->f_n, m->bnd_of, m->bnd_node, m->bnd_ptr, m->bnd_ent, m->ia, m->ja,
                   m->diag, m->tblk, m->lpos, m->last_lower, m->lev_l, m->lev_u, m->A, m->lslot, m->dinv,
                   m->Af, m->dinvf, m->q, m->r, m->gx, m->gy, m->gz, m->cdt, m->w, m->t, m->x, m->rhs, m->V,
-                  m->red, m->scal, m->forces, m->dscr, m->status, m->flags, m->ticket, m->part, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->s0, m->pair_ptr, m->pairs};
+                  m->red, m->scal, m->forces, m->dscr, m->status, m->flags, m->ticket, m->part, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->s0, m->pair_ptr, m->pairs, m->lev_ptr_d, m->bar};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (m->h_scal) cudaFreeHost(m->h_scal);
@@ -480,12 +480,19 @@ DevMesh *kf_device(const GEOMETRY *g)
     KF_CUDA(upload(&m->desc_l, dl.data(), N));
     KF_CUDA(upload(&m->desc_u, du.data(), N));
     // triangular-solve schedule: "levels16" (default: one launch per level,
-    // 16 lanes per row), "syncfree" (per-row flags, no level barriers) or
-    // "levels" (one launch per level, 4 lanes per row)
+    // 16 lanes per row), "persistent" (one cooperative launch, bounded grid
+    // barrier between levels), "syncfree" (per-row flags, no level barriers)
+    // or "levels" (one launch per level, 4 lanes per row)
     const char *env = getenv("KFUN3D_SPTRSV");
     m->trsv_mode = 2;
+    if (env && strcmp(env, "persistent") == 0) m->trsv_mode = 3;
     if (env && strcmp(env, "syncfree") == 0) m->trsv_mode = 1;
     if (env && strcmp(env, "levels") == 0) m->trsv_mode = 0;
+    std::vector<uint32_t> lp(p.lev_l_ptr);
+    lp.insert(lp.end(), p.lev_u_ptr.begin(), p.lev_u_ptr.end());
+    KF_CUDA(upload(&m->lev_ptr_d, lp.data(), lp.size()));
+    KF_CUDA(cudaMalloc(&m->bar, 4 * sizeof(unsigned)));
+    KF_CUDA(cudaMemset(m->bar, 0, 4 * sizeof(unsigned)));
     m->syncfree = m->trsv_mode == 1;
     const char *genv = getenv("KFUN3D_GRAPHS");
     m->use_graphs = !(genv && strcmp(genv, "0") == 0);

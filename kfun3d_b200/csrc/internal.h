@@ -54,6 +54,39 @@ MatrixHandle *kf_handle(const GEOMETRY *g);
 
 constexpr int KF_NBASIS = 31;
 
+// Grid-wide barrier for cooperative launches, with a bounded wait.  bar[0]
+// counts arrivals, bar[1] is the generation; both start at zero.  Returns
+// false (and sets *err) if the wait gave up, after which every caller skips
+// the rest of its work.
+constexpr uint32_t KF_BARRIER_LIMIT = 1u << 22;
+__device__ __forceinline__ bool kf_grid_barrier(unsigned *bar, int *err)
+{
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    volatile unsigned *gen = bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x * gridDim.y * gridDim.z - 1) {
+      bar[0] = 0;
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      unsigned spins = 0;
+      while (*gen == g) {
+        if (++spins > KF_BARRIER_LIMIT) { atomicExch(err, 1); ok = 0; break; }
+        if ((spins & 255) == 0 && *(volatile int *)err) { ok = 0; break; }
+      }
+    }
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
 // Device mirror of one GEOMETRY.  Node-indexed arrays follow the reference's
 // numbering; edge-indexed arrays its (sorted) edge order.
 struct DevMesh {
@@ -110,7 +143,8 @@ struct DevMesh {
   int *status = nullptr;          // device status words: [0] pivot failure, [1] wait timeout
   // sync-free triangular solves
   bool syncfree = true;
-  int trsv_mode = 1;               // 0 levels (4 lanes/row), 1 sync-free, 2 levels (16 lanes/row)
+  int trsv_mode = 2;               // 0 levels (4 lanes/row), 1 sync-free, 2 levels (16 lanes/row),
+                                   // 3 one persistent launch, grid barrier between levels
   unsigned trsv_grid = 0;          // persistent grid (whole blocks resident on every SM)
   uint32_t *flags = nullptr;       // [N] per-row completion epoch
   unsigned long long *ticket = nullptr;   // unused (kept zero)
@@ -123,6 +157,9 @@ struct DevMesh {
   bool use_graphs = true;
   unsigned mgs_grid = 0;          // cooperative grid for the Gram-Schmidt kernel
   double *part = nullptr;         // [2][mgs_grid] block partial sums
+  unsigned *bar = nullptr;        // grid-barrier words (see kf_grid_barrier), [0..3]
+  uint32_t *lev_ptr_d = nullptr;  // [nlev_l+1 + nlev_u+1] level offsets on the device
+  unsigned trsv_pgrid = 0;        // persistent sweep grid
   double *h_scal = nullptr;       // pinned host mirror of scal
   bool factored = false;
   bool a_valid = false;

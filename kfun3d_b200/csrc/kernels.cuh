@@ -1146,6 +1146,89 @@ __global__ void __launch_bounds__(256) k_trsv_level16(uint32_t s0, uint32_t s1, 
   if (l16 < 4) x[4 * (size_t)i + r] = xi;
 }
 
+// One row of a triangular sweep (the body of k_trsv_level16) for a 16-lane
+// group.
+template <typename T, bool UPPER>
+__device__ __forceinline__ void trsv_row16(const uint4 d, const uint32_t *__restrict__ ja, const T *__restrict__ A,
+                                           const double *__restrict__ b, double *x, int half, int jj, int r,
+                                           int l16, unsigned hmask)
+{
+  const uint32_t i = d.x, jb = d.y, je = d.z;
+  double xi = UPPER ? __ldcg(x + 4 * (size_t)i + r) : b[4 * (size_t)i + r];
+  for (uint32_t c0 = jb; c0 < je; c0 += 16) {
+    double t[4];
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const uint32_t j = c0 + 4 * p + jj;
+      t[p] = 0.0;
+      if (j < je) {
+        const uint32_t col = ja[j];
+        const T *blk = A + 16 * (size_t)j + 4 * r;
+        const double2 x01 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)col);
+        const double2 x23 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)col + 1);
+        double s = 0.0;
+        s += (double)blk[0] * x01.x;
+        s += (double)blk[1] * x01.y;
+        s += (double)blk[2] * x23.x;
+        s += (double)blk[3] * x23.y;
+        t[p] = s;
+      }
+    }
+    const uint32_t cnt = (je - c0) < 16u ? (je - c0) : 16u;
+#pragma unroll
+    for (int p = 0; p < 4; p++)
+      for (uint32_t q = 0; q < 4; q++) {
+        if (4 * p + q >= cnt) break;
+        xi = -1.0 * __shfl_sync(hmask, t[p], 16 * half + 4 * q + r) + xi;
+      }
+  }
+  if (UPPER) {
+    const int b4 = 16 * half;
+    const double x0 = __shfl_sync(hmask, xi, b4 + 0), x1 = __shfl_sync(hmask, xi, b4 + 1);
+    const double x2 = __shfl_sync(hmask, xi, b4 + 2), x3 = __shfl_sync(hmask, xi, b4 + 3);
+    const T *dg = A + 16 * (size_t)(jb - 1) + 4 * r;
+    double y = 0.0;
+    y += (double)dg[0] * x0;
+    y += (double)dg[1] * x1;
+    y += (double)dg[2] * x2;
+    y += (double)dg[3] * x3;
+    xi = y;
+  }
+  if (l16 < 4) __stcg(x + 4 * (size_t)i + r, xi);
+}
+
+// Both sweeps in one cooperative launch: the rows of each level are spread
+// over every half-warp of the grid, and a grid barrier (kf_grid_barrier,
+// bounded) separates consecutive levels.  Arithmetic as in k_trsv_level16.
+template <typename T>
+__global__ void __launch_bounds__(256, 4) k_trsv_persistent(const uint32_t *__restrict__ lev_l, uint32_t nl,
+                                                            const uint32_t *__restrict__ lev_u, uint32_t nu,
+                                                            const uint4 *__restrict__ desc_l,
+                                                            const uint4 *__restrict__ desc_u,
+                                                            const uint32_t *__restrict__ ja, const T *__restrict__ A,
+                                                            const double *__restrict__ b, double *x, unsigned *bar,
+                                                            int *err)
+{
+  const int lane = threadIdx.x & 31, half = lane >> 4, l16 = lane & 15, jj = l16 >> 2, r = l16 & 3;
+  const unsigned hmask = 0xffffu << (16 * half);
+  const uint32_t H = gridDim.x * (blockDim.x >> 4);
+  const uint32_t h = blockIdx.x * (blockDim.x >> 4) + (threadIdx.x >> 4);
+  for (uint32_t l = 0; l < nl; l++) {
+    const uint32_t s1 = lev_l[l + 1];
+    for (uint32_t s = lev_l[l] + h; s < s1; s += H)
+      trsv_row16<T, false>(desc_l[s], ja, A, b, x, half, jj, r, l16, hmask);
+    __threadfence();
+    if (!kf_grid_barrier(bar, err)) return;
+  }
+  for (uint32_t l = 0; l < nu; l++) {
+    const uint32_t s1 = lev_u[l + 1];
+    for (uint32_t s = lev_u[l] + h; s < s1; s += H)
+      trsv_row16<T, true>(desc_u[s], ja, A, b, x, half, jj, r, l16, hmask);
+    __threadfence();
+    if (l + 1 < nu && !kf_grid_barrier(bar, err)) return;
+  }
+}
+
 // ------------------------------------------------------------------ sync-free SpTRSV
 
 // Bounded wait for a row's completion flag (device scope, acquire).
@@ -1392,6 +1475,30 @@ void ilu(DevMesh &m, int precision)
 
 void sptrsv(DevMesh &m, const double *b, double *x, int precision)
 {
+  if (m.trsv_mode == 3) {
+    const uint32_t *levl = m.lev_ptr_d, *levu = m.lev_ptr_d + m.nlev_l + 1;
+    uint32_t nl = m.nlev_l, nu = m.nlev_u;
+    const double *bb = b;
+    unsigned *bar = m.bar;
+    int *err = m.status + 1;
+    const void *Ap = precision == 0 ? (const void *)m.A : (const void *)m.Af;
+    void *args[] = {(void *)&levl, &nl, (void *)&levu, &nu, (void *)&m.desc_l, (void *)&m.desc_u,
+                    (void *)&m.ja, (void *)&Ap, (void *)&bb, (void *)&x, (void *)&bar, (void *)&err};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(m.trsv_grid);
+    cfg.blockDim = dim3(256);
+    cfg.stream = m.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const void *fn = precision == 0 ? (const void *)k_trsv_persistent<double> : (const void *)k_trsv_persistent<float>;
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
+    if (e != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e));
+    kf_count_launch();
+    return;
+  }
   if (m.trsv_mode == 2) {
     for (int pass = 0; pass < 2; pass++) {
       const std::vector<uint32_t> &ptr = pass == 0 ? m.lev_l_ptr : m.lev_u_ptr;

@@ -13,11 +13,7 @@
 #include <string>
 #include <vector>
 
-#include <cooperative_groups.h>
-
 #include "internal.h"
-
-namespace cg = cooperative_groups;
 
 extern int g_kf_verbose;
 
@@ -124,7 +120,7 @@ __device__ __forceinline__ double block_sum(double v, double *sm)
 __device__ __forceinline__ double grid_total(const double *part, int np, double *sm)
 {
   double v = 0.0;
-  for (int i = threadIdx.x; i < np; i += blockDim.x) v += part[i];
+  for (int i = threadIdx.x; i < np; i += blockDim.x) v += __ldcg(part + i);   // written by other blocks
   v = block_sum(v, sm);
   if (threadIdx.x == 0) sm[32] = v;
   __syncthreads();
@@ -134,9 +130,9 @@ __device__ __forceinline__ double grid_total(const double *part, int np, double 
 }
 
 __global__ void __launch_bounds__(256) k_mgs_coop(size_t n, double *__restrict__ V, int k,
-                                                  double *__restrict__ h, double *__restrict__ part)
+                                                  double *__restrict__ h, double *__restrict__ part,
+                                                  unsigned *bar, int *err)
 {
-  cg::grid_group grid = cg::this_grid();
   __shared__ double sm[40];
   const int G = gridDim.x;
   const size_t n2 = n / 2;
@@ -168,7 +164,8 @@ __global__ void __launch_bounds__(256) k_mgs_coop(size_t n, double *__restrict__
     double *pb = part + (v & 1) * G;
     const double bs = block_sum(s, sm);
     if (threadIdx.x == 0) pb[blockIdx.x] = bs;
-    grid.sync();
+    __threadfence();
+    if (!kf_grid_barrier(bar, err)) return;
     const double tot = grid_total(pb, G, sm);
     if (v <= k) {
       hprev = tot;
@@ -431,7 +428,9 @@ void mgs_coop(DevMesh &m, int k)
   mgs_coop_prepare(m);
   size_t n = 4 * (size_t)m.N;
   double *V = m.V, *h = m.scal, *part = m.part;
-  void *args[] = {&n, &V, &k, &h, &part};
+  unsigned *bar = m.bar + 2;
+  int *err = m.status + 1;
+  void *args[] = {&n, &V, &k, &h, &part, &bar, &err};
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(m.mgs_grid);
   cfg.blockDim = dim3(256);
@@ -517,6 +516,8 @@ int device_status(DevMesh &m)
   CK(cudaStreamSynchronize(m.stream));
   if (st[0] || st[1]) {
     CK(cudaMemsetAsync(m.status, 0, 2 * sizeof(int), m.stream));
+    // a wait that gave up may leave a grid barrier half-counted
+    if (st[1] && m.bar) CK(cudaMemsetAsync(m.bar, 0, 4 * sizeof(unsigned), m.stream));
   }
   if (st[1]) return KFUN3D_ERR_TIMEOUT;
   return st[0];
