@@ -321,8 +321,10 @@ DevMesh *kf_device(const GEOMETRY *g)
     for (uint32_t e = 0; e < E; e++) { ptr[n0[e] + 1]++; ptr[n1[e] + 1]++; }
     for (uint32_t i = 0; i < N; i++) ptr[i + 1] += ptr[i];
     const size_t ninc = 2 * (size_t)E;
-    std::vector<uint32_t> oth(ninc), edg(ninc), blk(ninc), pos(ptr.begin(), ptr.end() - 1);
-    std::vector<double> w(3 * ninc);
+    const size_t wst = (ninc + 3) & ~(size_t)3;   // rows of inc_w start on 16 bytes
+    m->wstride = (uint32_t)wst;
+    std::vector<uint32_t> oth(wst + 4, 0), edg(ninc), blk(ninc), pos(ptr.begin(), ptr.end() - 1);
+    std::vector<double> w(3 * wst + 4, 0.0);
     const double *w0[3] = {g->e->w->w0->x0, g->e->w->w0->x1, g->e->w->w0->x2};
     const double *w1[3] = {g->e->w->w1->x0, g->e->w->w1->x1, g->e->w->w1->x2};
     auto find = [&](uint32_t row, uint32_t col) -> uint32_t {
@@ -333,16 +335,26 @@ DevMesh *kf_device(const GEOMETRY *g)
       const uint32_t a = n0[e], b = n1[e];
       uint32_t k = pos[a]++;
       oth[k] = b; edg[k] = e; blk[k] = find(a, b);
-      for (int c = 0; c < 3; c++) w[c * ninc + k] = w0[c][e];
+      for (int c = 0; c < 3; c++) w[c * wst + k] = w0[c][e];
       k = pos[b]++;
       oth[k] = a; edg[k] = e | 0x80000000u; blk[k] = find(b, a);
-      for (int c = 0; c < 3; c++) w[c * ninc + k] = w1[c][e];
+      for (int c = 0; c < 3; c++) w[c * wst + k] = w1[c][e];
     }
     KF_CUDA(upload(&m->inc_ptr, ptr.data(), N + 1));
-    KF_CUDA(upload(&m->inc_oth, oth.data(), ninc));
+    KF_CUDA(upload(&m->inc_oth, oth.data(), oth.size()));
     KF_CUDA(upload(&m->inc_edge, edg.data(), ninc));
     KF_CUDA(upload(&m->inc_blk, blk.data(), ninc));
-    KF_CUDA(upload(&m->inc_w, w.data(), 3 * ninc));
+    KF_CUDA(upload(&m->inc_w, w.data(), w.size()));
+    // shared memory of the staged gradient: the widest 128-node block range
+    size_t maxcnt = 0;
+    for (uint32_t nb = 0; nb < N; nb += 128) {
+      const uint32_t ne = std::min<uint32_t>(nb + 128, N);
+      const size_t ka = ptr[nb] & ~3u, kb = (ptr[ne] + 3u) & ~3u;
+      maxcnt = std::max(maxcnt, kb - ka);
+    }
+    const size_t smem = 4 * ((maxcnt + 3) & ~(size_t)3) + 24 * maxcnt;
+    const char *genv = getenv("KFUN3D_GRADIENT");
+    m->grad_smem = (smem <= 200 * 1024 && !(genv && strcmp(genv, "plain") == 0)) ? (unsigned)smem : 0;
   }
   // two-pass residual structure: edges sorted by n0 with n0 < n1 everywhere
   {
@@ -479,12 +491,14 @@ DevMesh *kf_device(const GEOMETRY *g)
     }
     KF_CUDA(upload(&m->desc_l, dl.data(), N));
     KF_CUDA(upload(&m->desc_u, du.data(), N));
-    // triangular-solve schedule: "levels16" (default: one launch per level,
-    // 16 lanes per row), "persistent" (one cooperative launch, bounded grid
+    // triangular-solve schedule: "pdl" (default: one launch per level with
+    // programmatic dependent launch), "levels16" (one launch per level, 16
+    // lanes per row), "persistent" (one cooperative launch, bounded grid
     // barrier between levels), "syncfree" (per-row flags, no level barriers)
     // or "levels" (one launch per level, 4 lanes per row)
     const char *env = getenv("KFUN3D_SPTRSV");
-    m->trsv_mode = 2;
+    m->trsv_mode = 4;
+    if (env && strcmp(env, "levels16") == 0) m->trsv_mode = 2;
     if (env && strcmp(env, "persistent") == 0) m->trsv_mode = 3;
     if (env && strcmp(env, "syncfree") == 0) m->trsv_mode = 1;
     if (env && strcmp(env, "levels") == 0) m->trsv_mode = 0;

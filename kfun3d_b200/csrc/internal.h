@@ -100,7 +100,9 @@ struct DevMesh {
   uint32_t *inc_oth = nullptr;    // [2E] the other end point
   uint32_t *inc_edge = nullptr;   // [2E] edge index | (1u<<31 when the node is n1)
   uint32_t *inc_blk = nullptr;    // [2E] block index of (node, other)
-  double *inc_w = nullptr;        // [3][2E] least-squares terms seen from the node
+  double *inc_w = nullptr;        // [3][wstride] least-squares terms seen from the node
+  uint32_t wstride = 0;           // 2E rounded up to a multiple of 4 (16-byte aligned rows)
+  unsigned grad_smem = 0;         // dynamic shared memory of k_gradient_tma (0: not used)
   // two-pass residual (every edge has n0 < n1)
   bool two_pass = false;
   uint32_t *eoff = nullptr;       // [N+1] edges with n0 = node (contiguous: edges are sorted by n0)
@@ -143,8 +145,9 @@ struct DevMesh {
   int *status = nullptr;          // device status words: [0] pivot failure, [1] wait timeout
   // sync-free triangular solves
   bool syncfree = true;
-  int trsv_mode = 2;               // 0 levels (4 lanes/row), 1 sync-free, 2 levels (16 lanes/row),
-                                   // 3 one persistent launch, grid barrier between levels
+  int trsv_mode = 4;               // 0 levels (4 lanes/row), 1 sync-free, 2 levels (16 lanes/row),
+                                   // 3 one persistent launch, grid barrier between levels,
+                                   // 4 levels with programmatic dependent launch
   unsigned trsv_grid = 0;          // persistent grid (whole blocks resident on every SM)
   uint32_t *flags = nullptr;       // [N] per-row completion epoch
   unsigned long long *ticket = nullptr;   // unused (kept zero)

@@ -236,7 +236,108 @@ __device__ __forceinline__ double4 farfield_flux(double U, double V, double fx, 
   return o;
 }
 
+// ------------------------------------------------------------------ TMA bulk staging
+
+// 1-D bulk copies (cp.async.bulk, the TMA engine's untiled path) into shared
+// memory, completed on an mbarrier.  Source and destination addresses and the
+// size must be multiples of 16 bytes; callers guarantee it.
+__device__ __forceinline__ unsigned smem_addr(const void *p)
+{
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *mbar, unsigned count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(mbar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *mbar, unsigned bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *mbar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(mbar))
+               : "memory");
+}
+
+constexpr uint32_t KF_MBAR_LIMIT = 1u << 24;
+
+// Bounded wait for phase `phase` of the mbarrier; false (and *err set) if it
+// gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, unsigned phase, int *err)
+{
+  const unsigned a = smem_addr(mbar);
+  for (uint32_t spins = 0; spins < KF_MBAR_LIMIT; spins++) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  atomicExch(err, 1);
+  return false;
+}
+
 // ------------------------------------------------------------------ gradient
+
+// Same sum as k_gradient, with the block's contiguous incidence range (other
+// end points and least-squares terms) staged into shared memory by four bulk
+// copies.  The range is widened to 4-entry boundaries so every copy starts and
+// ends on 16 bytes (the arrays are padded to a multiple of 4 entries).
+__global__ void __launch_bounds__(128) k_gradient_tma(uint32_t N, const uint32_t *__restrict__ inc_ptr,
+                                                      const uint32_t *__restrict__ inc_oth,
+                                                      const double *__restrict__ inc_w, uint32_t wstride,
+                                                      const double4 *__restrict__ q, double4 *__restrict__ gx,
+                                                      double4 *__restrict__ gy, double4 *__restrict__ gz, int *err)
+{
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t mbar;
+  const uint32_t nb = blockIdx.x * blockDim.x;
+  const uint32_t ne = min(nb + blockDim.x, N);
+  const uint32_t k0 = inc_ptr[nb], k1 = inc_ptr[ne];
+  const uint32_t ka = k0 & ~3u, kb = (k1 + 3u) & ~3u, cnt = kb - ka;
+  uint32_t *s_oth = reinterpret_cast<uint32_t *>(smem);
+  double *s_w = reinterpret_cast<double *>(smem + 4 * (size_t)((cnt + 3u) & ~3u));
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar, 1);
+    mbar_expect_tx(&mbar, cnt * 28u);
+    if (cnt) {
+      bulk_g2s(s_oth, inc_oth + ka, cnt * 4u, &mbar);
+      bulk_g2s(s_w, inc_w + ka, cnt * 8u, &mbar);
+      bulk_g2s(s_w + cnt, inc_w + wstride + ka, cnt * 8u, &mbar);
+      bulk_g2s(s_w + 2 * (size_t)cnt, inc_w + 2 * (size_t)wstride + ka, cnt * 8u, &mbar);
+    }
+  }
+  __syncthreads();
+  if (!mbar_wait(&mbar, 0, err)) return;
+  const uint32_t n = nb + threadIdx.x;
+  if (n >= N) return;
+  const double4 qn = q[n];
+  double4 ax = make_double4(0, 0, 0, 0), ay = ax, az = ax;
+  const uint32_t e1 = inc_ptr[n + 1] - ka;
+  for (uint32_t k = inc_ptr[n] - ka; k < e1; k++) {
+    const double4 qo = q[s_oth[k]];
+    const double wx = s_w[k], wy = s_w[cnt + k], wz = s_w[2 * (size_t)cnt + k];
+    double dq;
+    dq = qo.x - qn.x; ax.x += wx * dq; ay.x += wy * dq; az.x += wz * dq;
+    dq = qo.y - qn.y; ax.y += wx * dq; ay.y += wy * dq; az.y += wz * dq;
+    dq = qo.z - qn.z; ax.z += wx * dq; ay.z += wy * dq; az.z += wz * dq;
+    dq = qo.w - qn.w; ax.w += wx * dq; ay.w += wy * dq; az.w += wz * dq;
+  }
+  gx[n] = ax;
+  gy[n] = ay;
+  gz[n] = az;
+}
+
+
 
 // src/flux.c:60-145 as a gather: node n sums w.(q[other]-q[n]) over its
 // incident edges in edge order.
@@ -1229,6 +1330,93 @@ __global__ void __launch_bounds__(256, 4) k_trsv_persistent(const uint32_t *__re
   }
 }
 
+// Level-synchronous sweep with programmatic dependent launch: each level's
+// kernel lets the next one start at once (griddepcontrol.launch_dependents);
+// the next kernel loads everything that does not depend on earlier levels --
+// its row descriptor, the columns and the factor blocks (final since the
+// factorisation, which completed before this solve began) -- and only then
+// waits for the previous level's grid (griddepcontrol.wait) before reading x.
+// Arithmetic as in k_trsv_level16.  Rows with more than 16 blocks take a second
+// pass after the wait.
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(256) k_trsv_level_pdl(uint32_t s0, uint32_t s1, const uint4 *__restrict__ desc,
+                                                        const uint32_t *__restrict__ ja, const T *__restrict__ A,
+                                                        const double *__restrict__ b, double *x)
+{
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t slot = s0 + (gid >> 4);
+  const int lane = threadIdx.x & 31, half = lane >> 4, l16 = lane & 15, jj = l16 >> 2, r = l16 & 3;
+  const unsigned hmask = 0xffffu << (16 * half);
+  const bool active = slot < s1;
+  uint4 d = make_uint4(0, 0, 0, 0);
+  uint32_t col[4];
+  double a[4][4];
+  if (active) {
+    d = desc[slot];
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const uint32_t j = d.y + 4 * p + jj;
+      col[p] = 0xffffffffu;
+      a[p][0] = a[p][1] = a[p][2] = a[p][3] = 0.0;
+      if (j < d.z) {
+        col[p] = ja[j];
+        const T *blk = A + 16 * (size_t)j + 4 * r;
+        a[p][0] = (double)blk[0]; a[p][1] = (double)blk[1];
+        a[p][2] = (double)blk[2]; a[p][3] = (double)blk[3];
+      }
+    }
+  }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (!active) return;
+  const uint32_t i = d.x, jb = d.y, je = d.z;
+  double xi = UPPER ? x[4 * (size_t)i + r] : b[4 * (size_t)i + r];
+  for (uint32_t c0 = jb; c0 < je; c0 += 16) {
+    double t[4];
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const uint32_t j = c0 + 4 * p + jj;
+      t[p] = 0.0;
+      if (j < je) {
+        uint32_t cc = col[p];
+        double a0 = a[p][0], a1 = a[p][1], a2 = a[p][2], a3 = a[p][3];
+        if (c0 != jb) {   // second pass (rows with more than 16 blocks)
+          cc = ja[j];
+          const T *blk = A + 16 * (size_t)j + 4 * r;
+          a0 = (double)blk[0]; a1 = (double)blk[1]; a2 = (double)blk[2]; a3 = (double)blk[3];
+        }
+        const double4 xc = reinterpret_cast<const double4 *>(x)[cc];
+        double s = 0.0;
+        s += a0 * xc.x;
+        s += a1 * xc.y;
+        s += a2 * xc.z;
+        s += a3 * xc.w;
+        t[p] = s;
+      }
+    }
+    const uint32_t cnt = (je - c0) < 16u ? (je - c0) : 16u;
+#pragma unroll
+    for (int p = 0; p < 4; p++)
+      for (uint32_t q = 0; q < 4; q++) {
+        if (4 * p + q >= cnt) break;
+        xi = -1.0 * __shfl_sync(hmask, t[p], 16 * half + 4 * q + r) + xi;
+      }
+  }
+  if (UPPER) {
+    const int b4 = 16 * half;
+    const double x0 = __shfl_sync(hmask, xi, b4 + 0), x1 = __shfl_sync(hmask, xi, b4 + 1);
+    const double x2 = __shfl_sync(hmask, xi, b4 + 2), x3 = __shfl_sync(hmask, xi, b4 + 3);
+    const T *dg = A + 16 * (size_t)(jb - 1) + 4 * r;
+    double y = 0.0;
+    y += (double)dg[0] * x0;
+    y += (double)dg[1] * x1;
+    y += (double)dg[2] * x2;
+    y += (double)dg[3] * x3;
+    xi = y;
+  }
+  if (l16 < 4) x[4 * (size_t)i + r] = xi;
+}
+
 // ------------------------------------------------------------------ sync-free SpTRSV
 
 // Bounded wait for a row's completion flag (device scope, acquire).
@@ -1374,9 +1562,20 @@ inline unsigned blocks(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t
 
 void gradient(DevMesh &m, const double *q)
 {
-  k_gradient<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_w, 2 * m.E,
-                                                      (const double4 *)q, (double4 *)m.gx,
-                                                      (double4 *)m.gy, (double4 *)m.gz);
+  if (m.grad_smem) {
+    static bool attr_set = false;
+    if (!attr_set) {
+      cudaFuncSetAttribute(k_gradient_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      attr_set = true;
+    }
+    k_gradient_tma<<<blocks(m.N, 128), 128, m.grad_smem, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_w, m.wstride,
+                                                                    (const double4 *)q, (double4 *)m.gx,
+                                                                    (double4 *)m.gy, (double4 *)m.gz, m.status + 1);
+  } else {
+    k_gradient<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_w, m.wstride,
+                                                        (const double4 *)q, (double4 *)m.gx,
+                                                        (double4 *)m.gy, (double4 *)m.gz);
+  }
   kf_count_launch();
 }
 
@@ -1475,6 +1674,38 @@ void ilu(DevMesh &m, int precision)
 
 void sptrsv(DevMesh &m, const double *b, double *x, int precision)
 {
+  if (m.trsv_mode == 4) {
+    for (int pass = 0; pass < 2; pass++) {
+      const std::vector<uint32_t> &ptr = pass == 0 ? m.lev_l_ptr : m.lev_u_ptr;
+      const uint4 *desc = pass == 0 ? m.desc_l : m.desc_u;
+      const void *Ap = precision == 0 ? (const void *)m.A : (const void *)m.Af;
+      const void *fn;
+      if (precision == 0)
+        fn = pass == 0 ? (const void *)k_trsv_level_pdl<double, false> : (const void *)k_trsv_level_pdl<double, true>;
+      else
+        fn = pass == 0 ? (const void *)k_trsv_level_pdl<float, false> : (const void *)k_trsv_level_pdl<float, true>;
+      for (size_t l = 0; l + 1 < ptr.size(); l++) {
+        uint32_t s0 = ptr[l], s1 = ptr[l + 1];
+        const double *bb = b;
+        double *xx = x;
+        void *args[] = {&s0, &s1, (void *)&desc, (void *)&m.ja, (void *)&Ap, (void *)&bb, (void *)&xx};
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(blocks((size_t)(s1 - s0) * 16, 256));
+        cfg.blockDim = dim3(256);
+        cfg.stream = m.stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        // the first level of the lower sweep waits normally for its right-hand side
+        cfg.numAttrs = (pass == 0 && l == 0) ? 0 : 1;
+        const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
+        if (e != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e));
+        kf_count_launch();
+      }
+    }
+    return;
+  }
   if (m.trsv_mode == 3) {
     const uint32_t *levl = m.lev_ptr_d, *levu = m.lev_ptr_d + m.nlev_l + 1;
     uint32_t nl = m.nlev_l, nu = m.nlev_u;

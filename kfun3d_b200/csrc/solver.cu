@@ -129,9 +129,11 @@ __device__ __forceinline__ double grid_total(const double *part, int np, double 
   return t;
 }
 
-__global__ void __launch_bounds__(256) k_mgs_coop(size_t n, double *__restrict__ V, int k,
-                                                  double *__restrict__ h, double *__restrict__ part,
-                                                  unsigned *bar, int *err)
+constexpr int KF_MGS_ELEMS = 8;   // double2 elements per thread kept in registers
+
+__global__ void __launch_bounds__(256, 3) k_mgs_coop(size_t n, double *__restrict__ V, int k,
+                                                     double *__restrict__ h, double *__restrict__ part,
+                                                     unsigned *bar, int *err)
 {
   __shared__ double sm[40];
   const int G = gridDim.x;
@@ -139,12 +141,35 @@ __global__ void __launch_bounds__(256) k_mgs_coop(size_t n, double *__restrict__
   double2 *w = reinterpret_cast<double2 *>(V + (size_t)(k + 1) * n);
   const size_t stride = (size_t)G * blockDim.x;
   const size_t i0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t iend_reg = i0 + KF_MGS_ELEMS * stride;   // elements beyond are re-read from memory
+  double2 pv[KF_MGS_ELEMS];   // this thread's elements of the previous basis vector
   double hprev = 0.0;
   for (int v = 0; v <= k + 1; v++) {
     const double2 *prev = v > 0 ? reinterpret_cast<const double2 *>(V + (size_t)(v - 1) * n) : nullptr;
     const double2 *cur = v <= k ? reinterpret_cast<const double2 *>(V + (size_t)v * n) : nullptr;
     double s = 0.0;
-    for (size_t i = i0; i < n2; i += stride) {
+#pragma unroll
+    for (int t = 0; t < KF_MGS_ELEMS; t++) {
+      const size_t i = i0 + (size_t)t * stride;
+      if (i < n2) {
+        double2 a = w[i];
+        if (v > 0) {
+          a.x = fma(-hprev, pv[t].x, a.x);
+          a.y = fma(-hprev, pv[t].y, a.y);
+          w[i] = a;
+        }
+        if (cur) {
+          const double2 c = __ldcs(cur + i);
+          s = fma(a.x, c.x, s);
+          s = fma(a.y, c.y, s);
+          pv[t] = c;
+        } else {
+          s = fma(a.x, a.x, s);
+          s = fma(a.y, a.y, s);
+        }
+      }
+    }
+    for (size_t i = iend_reg; i < n2; i += stride) {
       double2 a = w[i];
       if (prev) {
         const double2 p = prev[i];
@@ -153,7 +178,7 @@ __global__ void __launch_bounds__(256) k_mgs_coop(size_t n, double *__restrict__
         w[i] = a;
       }
       if (cur) {
-        const double2 c = __ldcs(cur + i);
+        const double2 c = cur[i];
         s = fma(a.x, c.x, s);
         s = fma(a.y, c.y, s);
       } else {
@@ -418,7 +443,7 @@ void mgs_coop_prepare(DevMesh &m)
     int nsm = 0, per = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m.device));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mgs_coop, 256, 0));
-    m.mgs_grid = (unsigned)nsm * (unsigned)std::min(std::max(per, 1), 2);
+    m.mgs_grid = (unsigned)nsm * (unsigned)std::min(std::max(per, 1), 3);
     CK(cudaMalloc(&m.part, 2 * m.mgs_grid * sizeof(double)));
   }
 }
@@ -955,6 +980,10 @@ extern "C" double kfun3d_time_kernel(GEOMETRY *g, int which, int reps)
       case 4: o.sptrsv(*m, m->r, m->t, prec); break;
       case 5: arnoldi_step(*m, o, 15, prec); break;
       case 6:
+        if (o.fast) {
+          mgs_coop(*m, 15);
+          break;
+        }
         for (int vv = 0; vv <= 15; vv++) {
           dev_reduce(*m, Vb(*m, 16), Vb(*m, vv), m->scal + vv, 0, o.fast);
           k_axpy_dev<<<nblk(n, 256), 256, 0, m->stream>>>(n, m->scal + vv, -1.0, Vb(*m, vv), Vb(*m, 16), o.fast);
