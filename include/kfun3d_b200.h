@@ -229,6 +229,55 @@ int kfun3d_sptrsv_device_noalloc(const GEOMETRY *g, const double *d_b, double *d
 /* Release the device mirror of g (also done by CXX_Matrix_Delete). */
 void kfun3d_device_release(GEOMETRY *g);
 
+/* ---------------------------------------------------------------------
+ * Part 3: the learned right preconditioner (no reference counterpart).
+ *
+ * An edge-based message-passing network, hidden width 32: an encoder MLP on
+ * node features [y/s, q], three message-passing layers (edge MLP on
+ * [h_i, h_j, n_ij, a_ij], sum over a node's edges, residual node MLP on
+ * [h_i, sum]), and a decoder MLP to 4 outputs.  Every MLP has two linear
+ * layers with a ReLU between; layer L maps kin inputs (its bias is the column
+ * at the ones feature, index nreal) to out outputs, weights W~[out x kin] in
+ * one FP32 parameter vector at `offset`.  Forward, backward and Adam run on
+ * the GPU with BF16 tensor-core operands and FP32 accumulation.
+ *
+ * All d_* arguments are device pointers.  x0 is [nodes x 8] BF16
+ * ([y/s (4), q (4)]); targets and outputs are [nodes x 4] FP32.
+ * --------------------------------------------------------------------- */
+typedef struct kfun3d_mpnn kfun3d_mpnn;
+typedef struct kfun3d_mpnn_graph kfun3d_mpnn_graph;
+
+size_t kfun3d_mpnn_param_count(void);
+int kfun3d_mpnn_layer_shape(int layer, int *out, int *kin, int *nreal, int *offset);
+/* Seeded initialisation on the current device; NULL on failure. */
+kfun3d_mpnn *kfun3d_mpnn_create(unsigned long long seed);
+void kfun3d_mpnn_free(kfun3d_mpnn *net);
+/* Host FP32 parameters in and out; set_params also resets the Adam state. */
+int kfun3d_mpnn_set_params(kfun3d_mpnn *net, const float *host, size_t n);
+int kfun3d_mpnn_get_params(const kfun3d_mpnn *net, float *host, size_t n);
+int kfun3d_mpnn_get_grad(const kfun3d_mpnn *net, float *host, size_t n);
+int kfun3d_mpnn_zero_grad(kfun3d_mpnn *net);
+/* The directed-edge graph of a mesh (node-incidence rows, edge features). */
+kfun3d_mpnn_graph *kfun3d_mpnn_graph_create(const GEOMETRY *g);
+void kfun3d_mpnn_graph_free(kfun3d_mpnn_graph *G);
+/* d_out = N(x0). */
+int kfun3d_mpnn_forward(kfun3d_mpnn *net, kfun3d_mpnn_graph *G, const void *d_x0, float *d_out);
+/* Adds the gradient of weight * sum (N(x0) - target)^2 to the network's
+ * gradient; *loss (optional) receives weight * sum (...)^2. */
+int kfun3d_mpnn_accumulate(kfun3d_mpnn *net, kfun3d_mpnn_graph *G, const void *d_x0, const float *d_target,
+                           double weight, double *loss);
+/* One Adam step on the accumulated gradient, which it then clears. */
+int kfun3d_mpnn_adam_step(kfun3d_mpnn *net, double lr, double beta1, double beta2, double eps);
+/* Features and target of a training pair from FP64 device vectors of
+ * 4 * nnodes: x0 = BF16([y/s, q]), target = (x - y)/s, s = RMS(y). */
+int kfun3d_mpnn_make_pair(size_t nnodes, const double *d_y, const double *d_q, const double *d_x, void *d_x0,
+                          float *d_target);
+/* z = y + s N([y/s, q]): the network's correction of an ILU(0)-preconditioned
+ * vector y. */
+int kfun3d_mpnn_apply(kfun3d_mpnn *net, kfun3d_mpnn_graph *G, const double *d_y, const double *d_q, double *d_z);
+/* Test hook: Y = X Wt^T, one BF16 tensor-core tile per 128 rows. */
+int kfun3d_umma_selftest(const void *X, const void *Wt, float *Y, int rows, int K, int N);
+
 #ifdef __cplusplus
 }
 #endif

@@ -91,6 +91,25 @@ def lib():
         "kfun3d_device_release": (None, [G]),
         "kfun3d_matrix_read": (C.c_long, [G, P(C.c_uint), P(C.c_uint), D]),
         "kfun3d_time_solve": (C.c_double, [G, P(SolverParams), C.c_int, P(Step), C.c_int, P(C.c_int)]),
+        # learned preconditioner (include/kfun3d_b200.h, part 3)
+        "kfun3d_mpnn_param_count": (C.c_size_t, []),
+        "kfun3d_mpnn_layer_shape": (C.c_int, [C.c_int, P(C.c_int), P(C.c_int), P(C.c_int), P(C.c_int)]),
+        "kfun3d_mpnn_create": (C.c_void_p, [C.c_ulonglong]),
+        "kfun3d_mpnn_free": (None, [C.c_void_p]),
+        "kfun3d_mpnn_set_params": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
+        "kfun3d_mpnn_get_params": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
+        "kfun3d_mpnn_get_grad": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
+        "kfun3d_mpnn_zero_grad": (C.c_int, [C.c_void_p]),
+        "kfun3d_mpnn_graph_create": (C.c_void_p, [G]),
+        "kfun3d_mpnn_graph_free": (None, [C.c_void_p]),
+        "kfun3d_mpnn_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "kfun3d_mpnn_accumulate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                             P(C.c_double)]),
+        "kfun3d_mpnn_adam_step": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double]),
+        "kfun3d_mpnn_make_pair": (C.c_int, [C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.c_void_p]),
+        "kfun3d_mpnn_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "kfun3d_umma_selftest": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -189,4 +189,15 @@ void kfun3d_reset_launch_count_by(unsigned long long n);   // undo counts taken 
 KF_DECLARE_KERNELS(kf_exact)
 KF_DECLARE_KERNELS(kf_fast)
 
+// Learned preconditioner (mpnn.cu), for the solver: workspace for a graph
+// (allocates; call before any capture), the correction z = y + s N([y/s, q])
+// enqueued on a stream, the completion status of its bounded waits, and the
+// features/target of a training pair (scr: 264 doubles of device scratch).
+int kf_mpnn_prepare(kfun3d_mpnn *net, kfun3d_mpnn_graph *G);
+int kf_mpnn_apply_async(kfun3d_mpnn *net, kfun3d_mpnn_graph *G, const double *y, const double *q, double *z,
+                        cudaStream_t st);
+int kf_mpnn_status(kfun3d_mpnn *net, cudaStream_t st);
+int kf_mpnn_pair_async(size_t nnodes, const double *y, const double *q, const double *x, void *x0, float *tgt,
+                       double *scr, cudaStream_t st);
+
 #endif

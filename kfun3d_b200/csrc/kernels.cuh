@@ -1109,6 +1109,71 @@ __global__ void __launch_bounds__(128) k_ilu_level_f32(uint32_t nrows, const uin
   }
 }
 
+// FP32 sweep on the precomputed pair lists: the products of m < min(i,k) are
+// the list without its last entry (which is m = min(i,k)); the L factor lives in
+// place in the lower blocks, so the L operand of a pair is block
+// ia[i] + (slot - lpos[i]).
+__global__ void __launch_bounds__(128) k_ilu_level_pairs_f32(uint32_t nrows, const uint32_t *__restrict__ rows,
+                                                             const uint32_t *__restrict__ ia,
+                                                             const uint32_t *__restrict__ ja,
+                                                             const uint32_t *__restrict__ pair_ptr,
+                                                             const uint2 *__restrict__ pairs,
+                                                             const uint32_t *__restrict__ lpos, float *__restrict__ A,
+                                                             float *__restrict__ dinv, int *__restrict__ status)
+{
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t grp = gid >> 4;
+  const int lane = threadIdx.x & 31, l16 = lane & 15, base = lane & 16;
+  const unsigned mask = 0xffffu << base;
+  if (grp >= nrows) return;
+  const uint32_t i = rows[grp];
+  const uint32_t j0 = ia[i], j1 = ia[i + 1], lp = lpos[i];
+  for (uint32_t j = j0; j < j1; j++) {
+    const uint32_t k = ja[j];
+    float a = A[16 * (size_t)j + l16];
+    const uint32_t p0 = pair_ptr[j], p1 = pair_ptr[j + 1] - 1;   // without the last product
+    for (uint32_t pb = p0; pb < p1; pb += 8) {
+      float lv[8], uv[8];
+      const uint32_t cnt = (p1 - pb) < 8 ? (p1 - pb) : 8;
+#pragma unroll
+      for (int t = 0; t < 8; t++) {
+        lv[t] = 0.0f;
+        uv[t] = 0.0f;
+        if ((uint32_t)t < cnt) {
+          const uint2 pr = pairs[pb + t];
+          lv[t] = A[16 * (size_t)(j0 + (pr.x - lp)) + l16];
+          uv[t] = A[16 * (size_t)pr.y + l16];
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < 8; t++) {
+        if ((uint32_t)t >= cnt) break;
+        a -= gemm_lane_f(lv[t], uv[t], l16, mask, base);
+      }
+    }
+    if (k < i) {
+      A[16 * (size_t)j + l16] = gemm_lane_f(a, dinv[16 * (size_t)k + l16], l16, mask, base);
+    } else {
+      A[16 * (size_t)j + l16] = a;
+      if (k == i) {
+        __syncwarp(mask);
+        if (l16 == 0) {
+          double sd[16], o[16];
+          for (int t = 0; t < 16; t++) sd[t] = A[16 * (size_t)j + t];
+          inv4(sd, o);
+          bool bad = false;
+          for (int t = 0; t < 16; t++) {
+            dinv[16 * (size_t)i + t] = (float)o[t];
+            bad |= !isfinite(o[t]);
+          }
+          if (bad) atomicExch(status, KFUN3D_ERR_PIVOT);
+        }
+        __syncwarp(mask);
+      }
+    }
+  }
+}
+
 __global__ void k_ilu_finish_f32(uint32_t N, const uint32_t *__restrict__ diag, const float *__restrict__ dinv,
                                  float *__restrict__ A)
 {
@@ -1660,6 +1725,10 @@ void ilu(DevMesh &m, int precision)
     else if (precision == 0)
       k_ilu_level<<<blocks((size_t)nr * 16, 128), 128, 0, m.stream>>>(nr, m.lev_l + r0, m.ia, m.ja, m.diag, m.tblk,
                                                                       m.lpos, m.A, m.lslot, m.dinv, status);
+    else if (m.pairs)
+      k_ilu_level_pairs_f32<<<blocks((size_t)nr * 16, 128), 128, 0, m.stream>>>(nr, m.lev_l + r0, m.ia, m.ja,
+                                                                                m.pair_ptr, m.pairs, m.lpos, m.Af,
+                                                                                m.dinvf, status);
     else
       k_ilu_level_f32<<<blocks((size_t)nr * 16, 128), 128, 0, m.stream>>>(nr, m.lev_l + r0, m.ia, m.ja, m.diag,
                                                                           m.tblk, m.Af, m.dinvf, status);
