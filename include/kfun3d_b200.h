@@ -275,6 +275,40 @@ int kfun3d_mpnn_make_pair(size_t nnodes, const double *d_y, const double *d_q, c
 /* z = y + s N([y/s, q]): the network's correction of an ILU(0)-preconditioned
  * vector y. */
 int kfun3d_mpnn_apply(kfun3d_mpnn *net, kfun3d_mpnn_graph *G, const double *d_y, const double *d_q, double *d_z);
+/* Statistics of a flexible solve. */
+typedef struct {
+  int newton_steps;     /* Newton steps taken */
+  int gmres_its;        /* FGMRES iterations over the solve */
+  int learned_its;      /* iterations preconditioned by the network */
+  int fallback_solves;  /* linear solves that went on with ILU(0) alone part-way */
+  int rejected_steps;   /* updates undone because the nonlinear residual grew tenfold */
+  int disabled;         /* 1: the network was switched off for the rest of the solve */
+  int pairs;            /* training pairs written (kfun3d_collect_pairs) */
+  double seconds;       /* device time of the whole solve */
+} kfun3d_flex_stats;
+
+/* The pseudo-transient solve of Kernel() with FGMRES(restart) in place of
+ * left-preconditioned GMRES: right preconditioning z = ILU(0)^-1 v, or with
+ * net != NULL the network's correction of it, chosen per iteration.  The
+ * network runs from Newton step 1 on and falls back to ILU(0) alone: within a
+ * linear solve whose residual falls at less than half ILU(0)'s rate, for good
+ * after two steps that need more iterations than the last ILU(0)-only solve,
+ * and for an update after which the FP64 nonlinear residual grows tenfold
+ * (the update is undone).  Solves from g->q->q and updates it; returns the
+ * number of history entries or -1. */
+int kfun3d_solve_flexible(GEOMETRY *g, const kfun3d_solver_params *p, kfun3d_mpnn *net, kfun3d_step *hist,
+                          int max_hist, kfun3d_flex_stats *stats);
+/* The ILU(0)-FGMRES solve writing training pairs: for the iterate after every
+ * `stride` iterations of each Newton step's first cycle, and for the step's
+ * final correction x, v = J x, y = ILU(0)^-1 v and the pair
+ * (BF16([y/s, q]), (x - y)/s) into slot i of d_x0 ([cap][N x 8] BF16) and
+ * d_target ([cap][N x 4] FP32).  Returns the number of pairs or -1. */
+int kfun3d_collect_pairs(GEOMETRY *g, const kfun3d_solver_params *p, int stride, void *d_x0, float *d_target,
+                         int cap, kfun3d_flex_stats *stats);
+/* Mean device seconds of `reps` flexible solves from g->q->q (not updated). */
+double kfun3d_time_solve_flexible(GEOMETRY *g, const kfun3d_solver_params *p, kfun3d_mpnn *net, int reps,
+                                  kfun3d_step *hist, int max_hist, int *nsteps, kfun3d_flex_stats *stats);
+
 /* Test hook: Y = X Wt^T, one BF16 tensor-core tile per 128 rows. */
 int kfun3d_umma_selftest(const void *X, const void *Wt, float *Y, int rows, int K, int N);
 

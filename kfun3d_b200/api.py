@@ -31,6 +31,15 @@ class Step(C.Structure):
                 ("momn", C.c_double), ("seconds", C.c_double)]
 
 
+class FlexStats(C.Structure):
+    _fields_ = [("newton_steps", C.c_int), ("gmres_its", C.c_int), ("learned_its", C.c_int),
+                ("fallback_solves", C.c_int), ("rejected_steps", C.c_int), ("disabled", C.c_int),
+                ("pairs", C.c_int), ("seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class MeshSpec(C.Structure):
     _fields_ = [("n", C.c_uint), ("bump_height", C.c_double), ("bump_sigma", C.c_double),
                 ("jitter", C.c_double), ("seed", C.c_ulonglong), ("permute", C.c_int)]
@@ -110,6 +119,11 @@ def lib():
                                             C.c_void_p]),
         "kfun3d_mpnn_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "kfun3d_umma_selftest": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
+        "kfun3d_solve_flexible": (C.c_int, [G, P(SolverParams), C.c_void_p, P(Step), C.c_int, P(FlexStats)]),
+        "kfun3d_collect_pairs": (C.c_int, [G, P(SolverParams), C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                           P(FlexStats)]),
+        "kfun3d_time_solve_flexible": (C.c_double, [G, P(SolverParams), C.c_void_p, C.c_int, P(Step), C.c_int,
+                                                    P(C.c_int), P(FlexStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -326,8 +340,53 @@ class Mesh:
                       drag=h.drag, momn=h.momn, seconds=h.seconds) for h in hist[:ns.value]]
         return t, steps
 
+    def solve_flexible(self, net=None, **params):
+        """FGMRES solve (ILU(0), or with `net` the learned preconditioner); updates q.
+        Returns (history, stats)."""
+        p = default_params(**params)
+        hist = (Step * 64)()
+        st = FlexStats()
+        n = lib().kfun3d_solve_flexible(self.g, C.byref(p), net.h if net is not None else None, hist, 64,
+                                        C.byref(st))
+        if n < 0:
+            raise RuntimeError(f"kfun3d_solve_flexible failed: {last_error()}")
+        return _hist(hist, n), st.as_dict()
+
+    def time_solve_flexible(self, net=None, reps=1, **params):
+        """Mean device seconds per flexible solve from the current state (not updated)."""
+        p = default_params(**params)
+        hist = (Step * 64)()
+        st = FlexStats()
+        ns = C.c_int(0)
+        t = lib().kfun3d_time_solve_flexible(self.g, C.byref(p), net.h if net is not None else None, int(reps),
+                                             hist, 64, C.byref(ns), C.byref(st))
+        if t < 0:
+            raise RuntimeError(f"kfun3d_time_solve_flexible failed: {last_error()}")
+        return t, _hist(hist, ns.value), st.as_dict()
+
+    def collect_pairs(self, stride=5, cap=64, **params):
+        """Training pairs of the ILU(0)-FGMRES solve from the current state
+        (q updated): (x0 BF16 [n, N, 8], target FP32 [n, N, 4], stats) on the GPU."""
+        import torch
+        N = self.view.nnodes
+        x0 = torch.empty((cap, N, 8), dtype=torch.bfloat16, device="cuda")
+        tgt = torch.empty((cap, N, 4), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        p = default_params(**params)
+        st = FlexStats()
+        n = lib().kfun3d_collect_pairs(self.g, C.byref(p), int(stride), x0.data_ptr(), tgt.data_ptr(), int(cap),
+                                       C.byref(st))
+        if n < 0:
+            raise RuntimeError(f"kfun3d_collect_pairs failed: {last_error()}")
+        return x0[:n], tgt[:n], st.as_dict()
+
     def release_device(self):
         lib().kfun3d_device_release(self.g)
+
+
+def _hist(hist, n):
+    return [dict(step=h.step, gmres_its=h.gmres_its, cfl=h.cfl, fnorm=h.fnorm, lift=h.lift, drag=h.drag,
+                 momn=h.momn, seconds=h.seconds) for h in hist[:n]]
 
 
 def norm2(v):

@@ -245,10 +245,11 @@ static void release_device(MatrixHandle *h)
                   m->wf_n, m->s_n, m->f_n, m->bnd_of, m->bnd_node, m->bnd_ptr, m->bnd_ent, m->ia, m->ja,
                   m->diag, m->tblk, m->lpos, m->last_lower, m->lev_l, m->lev_u, m->A, m->lslot, m->dinv,
                   m->Af, m->dinvf, m->q, m->r, m->gx, m->gy, m->gz, m->cdt, m->w, m->t, m->x, m->rhs, m->V,
-                  m->red, m->scal, m->forces, m->dscr, m->status, m->flags, m->ticket, m->part, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->s0, m->pair_ptr, m->pairs, m->lev_ptr_d, m->bar};
+                  m->red, m->scal, m->forces, m->dscr, m->status, m->flags, m->ticket, m->part, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->s0, m->pair_ptr, m->pairs, m->lev_ptr_d, m->bar, m->Z, m->qold, m->fy, m->fx, m->pscr};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (m->h_scal) cudaFreeHost(m->h_scal);
+  if (m->mgraph) kfun3d_mpnn_graph_free(m->mgraph);
   for (auto &a : m->arnoldi)
     for (auto &b : a)
       for (auto &g : b)

@@ -164,6 +164,13 @@ struct DevMesh {
   uint32_t *lev_ptr_d = nullptr;  // [nlev_l+1 + nlev_u+1] level offsets on the device
   unsigned trsv_pgrid = 0;        // persistent sweep grid
   double *h_scal = nullptr;       // pinned host mirror of scal
+  // flexible GMRES (right preconditioning) and the learned preconditioner
+  double *Z = nullptr;            // [30][4N] preconditioned basis vectors
+  double *qold = nullptr;         // [4N] state before the last update
+  double *fy = nullptr;           // [4N] ILU(0)-preconditioned vector
+  double *fx = nullptr;           // [4N] iterate of a training pair
+  double *pscr = nullptr;         // [264] scratch of the pair features
+  kfun3d_mpnn_graph *mgraph = nullptr;   // the network's graph of this mesh
   bool factored = false;
   bool a_valid = false;
 };

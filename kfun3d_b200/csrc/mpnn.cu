@@ -653,13 +653,14 @@ __global__ void k_adam(int n, float *__restrict__ theta, float *__restrict__ m, 
 {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
+  // every operation rounded on its own (no contraction), in this order
   const float gi = g[idx];
-  const float mi = b1 * m[idx] + (1.f - b1) * gi;
-  const float vi = b2 * v[idx] + (1.f - b2) * gi * gi;
+  const float mi = __fadd_rn(__fmul_rn(b1, m[idx]), __fmul_rn(__fsub_rn(1.f, b1), gi));
+  const float vi = __fadd_rn(__fmul_rn(b2, v[idx]), __fmul_rn(__fmul_rn(__fsub_rn(1.f, b2), gi), gi));
   m[idx] = mi;
   v[idx] = vi;
-  const float mh = mi / c1, vh = vi / c2;
-  const float th = theta[idx] - lr * mh / (sqrtf(vh) + eps);
+  const float mh = __fdiv_rn(mi, c1), vh = __fdiv_rn(vi, c2);
+  const float th = __fsub_rn(theta[idx], __fdiv_rn(__fmul_rn(lr, mh), __fadd_rn(__fsqrt_rn(vh), eps)));
   theta[idx] = th;
   int L = 0;
   while (idx >= c_off[L + 1]) L++;

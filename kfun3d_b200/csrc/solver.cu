@@ -471,6 +471,22 @@ void mgs_coop(DevMesh &m, int k)
 
 // One Arnoldi step k (src/kernel.c:123-141): V[k+1] = M^-1 J V[k],
 // modified Gram-Schmidt against V[0..k], normalised; h in scal[0..k+1].
+// Modified Gram-Schmidt of V[k+1] against V[0..k], normalised; h in scal[0..k+1].
+void orthogonalize(DevMesh &m, const Ops &o, int k)
+{
+  const size_t n = 4 * (size_t)m.N;
+  if (o.fast && (n % 2) == 0) {
+    mgs_coop(m, k);
+    return;
+  }
+  for (int v = 0; v <= k; v++) {
+    dev_reduce(m, Vb(m, k + 1), Vb(m, v), m.scal + v, 0, o.fast);
+    k_axpy_dev<<<nblk(n, 256), 256, 0, m.stream>>>(n, m.scal + v, -1.0, Vb(m, v), Vb(m, k + 1), o.fast);
+    kf_count_launch();
+  }
+  dev_normalize(m, Vb(m, k + 1), m.scal + k + 1, o.fast);
+}
+
 void arnoldi_step(DevMesh &m, const Ops &o, int k, int prec)
 {
   const size_t n = 4 * (size_t)m.N;
@@ -710,6 +726,281 @@ static int solve_device(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_param
   }
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
+  return steps < 0 ? -1 : nrec;
+}
+
+// ------------------------------------------------------------------ flexible GMRES
+
+namespace {
+
+// Training pairs written by the ILU(0)-FGMRES solve: slot i holds x0 at
+// x0 + i * 16N bytes (BF16 [N x 8]) and the target at tgt + i * 4N floats.
+struct PairSink {
+  int stride = 0;
+  unsigned char *x0 = nullptr;
+  float *tgt = nullptr;
+  int cap = 0;
+  int count = 0;
+};
+
+// Givens update of Hessenberg column k (host, src/kernel.c:143-160 arithmetic);
+// returns |rs[k+1]|.
+double givens(double *hh, double *cs, double *sn, double *rs, int k)
+{
+  for (int i = 0; i < k; i++) {
+    const double tt = hh[i];
+    hh[i] = cs[i] * hh[i] + sn[i] * hh[i + 1];
+    hh[i + 1] = cs[i] * hh[i + 1] - sn[i] * tt;
+  }
+  const double tt = sqrt(hh[k] * hh[k] + hh[k + 1] * hh[k + 1]);
+  const double c = hh[k] / tt, s = hh[k + 1] / tt;
+  cs[k] = c;
+  sn[k] = s;
+  rs[k + 1] = -(s * rs[k]);
+  rs[k] = c * rs[k];
+  hh[k] = c * hh[k] + s * hh[k + 1];
+  return fabs(rs[k + 1]);
+}
+
+// y[0..k-1] from the rotated Hessenberg columns and right-hand side
+void back_substitute(const double *ghh, const double *rs, int k, double *y)
+{
+  for (int i = 0; i < k; i++) y[i] = rs[i];
+  y[k - 1] /= ghh[(k - 1) * (KF_NBASIS + 1) + (k - 1)];
+  for (int i = 1; i <= k - 1; i++) {
+    const int mm = (k - 1) - i;
+    double tt = y[mm];
+    for (int j = mm + 1; j <= k - 1; j++) tt -= ghh[j * (KF_NBASIS + 1) + mm] * y[j];
+    y[mm] = tt / ghh[mm * (KF_NBASIS + 1) + mm];
+  }
+}
+
+double *Zb(DevMesh &m, int k) { return m.Z + (size_t)k * 4 * m.N; }
+
+bool ensure_flex(DevMesh &m)
+{
+  const size_t n = 4 * (size_t)m.N;
+  if (!m.Z && cudaMalloc(&m.Z, 30 * n * sizeof(double)) != cudaSuccess) return false;
+  if (!m.qold && cudaMalloc(&m.qold, n * sizeof(double)) != cudaSuccess) return false;
+  if (!m.fy && cudaMalloc(&m.fy, n * sizeof(double)) != cudaSuccess) return false;
+  if (!m.fx && cudaMalloc(&m.fx, n * sizeof(double)) != cudaSuccess) return false;
+  if (!m.pscr && cudaMalloc(&m.pscr, 264 * sizeof(double)) != cudaSuccess) return false;
+  return true;
+}
+
+// Pair of the correction x (device, 4N): v = J x, y = ILU(0)^-1 v,
+// x0 = BF16([y/s, q]), target = (x - y)/s.
+void write_pair(DevMesh &m, const Ops &o, int prec, const double *x, PairSink &ps)
+{
+  if (ps.count >= ps.cap) return;
+  dev_jacvec(m, o, x, m.t);
+  o.sptrsv(m, m.t, m.fy, prec);
+  kf_mpnn_pair_async(m.N, m.fy, m.q, x, ps.x0 + (size_t)ps.count * 16 * m.N,
+                     ps.tgt + (size_t)ps.count * 4 * m.N, m.pscr, m.stream);
+  ps.count++;
+}
+
+}  // namespace
+
+// The pseudo-transient Newton loop of src/kernel.c:47-232 with its linear
+// solves done by FGMRES(restart) -- right preconditioning, a preconditioner
+// allowed to change from one iteration to the next:
+//   z_k = M_k(v_k),  w = J z_k orthogonalised against v_0..v_k,
+//   x = Z y after each cycle, the true residual b - J x at a restart.
+// M_k is ILU(0)^-1, or with a network the network's correction of it.  The
+// network is a guest: Newton step 0 runs on ILU(0) alone to measure its
+// convergence rate; a linear solve whose residual falls at less than half
+// that rate after 4 iterations continues on ILU(0) alone; two steps in a row
+// that need more iterations than the last ILU(0)-only solve switch the
+// network off for good; and an update after which the FP64 nonlinear
+// residual is non-finite or grows tenfold is undone and redone on ILU(0).
+static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_params *p, kfun3d_mpnn *net,
+                          PairSink *ps, kfun3d_step *hist, int max_hist, kfun3d_flex_stats *st)
+{
+  const Ops o = ops();
+  const int prec = kf_precision();
+  const size_t n = 4 * (size_t)m.N;
+  const int restart = std::min(std::max(p->gmres_restart, 1), 30);
+  double u, v;
+  kfun3d_get_freestream(&u, &v);
+  kfun3d_flex_stats S{};
+  if (!ensure_flex(m)) {
+    kf_set_error(KFUN3D_ERR_CUDA, "flexible solve: out of device memory");
+    return -1;
+  }
+  if (net) {
+    if (!m.mgraph) m.mgraph = kfun3d_mpnn_graph_create(g);
+    if (!m.mgraph || kf_mpnn_prepare(net, m.mgraph) != KFUN3D_OK) return -1;
+  }
+  double ghh[KF_NBASIS * (KF_NBASIS + 1)] = {0};
+  double cs[KF_NBASIS], sn[KF_NBASIS], rs[KF_NBASIS], yk[KF_NBASIS];
+  double fnorm0 = 0.0, fnorm_prev = 0.0, cfl = p->cfl_init, rate_ilu = 0.0;
+  bool use_net = net != nullptr, last_used_net = false;
+  int strikes = 0, plain_its_last = -1;
+  int nrec = 0, steps = 0;
+  cudaEvent_t ev0, ev1, es0, es1;
+  CK(cudaEventCreate(&ev0));
+  CK(cudaEventCreate(&ev1));
+  CK(cudaEventCreate(&es0));
+  CK(cudaEventCreate(&es1));
+  CK(cudaEventRecord(es0, m.stream));
+  for (int its = 0; its < p->ts_max; its++) {
+    CK(cudaEventRecord(ev0, m.stream));
+    dev_residual(m, o, m.q, m.r);
+    dev_reduce(m, m.r, m.r, m.scal + S_FN, 1, o.fast);
+    fetch(m, S_FN, 1);
+    double fnorm = m.h_scal[S_FN];
+    if (last_used_net && (!std::isfinite(fnorm) || fnorm > 10.0 * fnorm_prev)) {
+      // the nonlinear residual rejects the learned update: undo it, go on without the network
+      CK(cudaMemcpyAsync(m.q, m.qold, n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+      dev_residual(m, o, m.q, m.r);
+      dev_reduce(m, m.r, m.r, m.scal + S_FN, 1, o.fast);
+      fetch(m, S_FN, 1);
+      fnorm = m.h_scal[S_FN];
+      use_net = false;
+      S.disabled = 1;
+      S.rejected_steps++;
+    }
+    if (!std::isfinite(fnorm)) {
+      kf_set_error(KFUN3D_ERR_NONFINITE, "residual norm is not finite");
+      steps = -1;
+      break;
+    }
+    if (its == 0) fnorm0 = fnorm;
+    else {
+      double cfl0 = 1.1 * p->cfl_init * fnorm0;   // src/kernel.c:86-88
+      cfl0 /= fnorm;
+      cfl = (cfl0 < p->cfl_max) ? cfl0 : p->cfl_max;
+    }
+    fnorm_prev = fnorm;
+    o.timestep(m, m.q, cfl);
+    o.fill(m, m.q, u, v, prec);
+    dev_reduce(m, m.q, m.q, m.scal + S_QN, 2, o.fast);
+    CK(cudaMemsetAsync(m.x, 0, n * sizeof(double), m.stream));
+    o.ilu(m, prec);
+    CK(cudaMemcpyAsync(Vb(m, 0), m.r, n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+    {
+      const int sd = device_status(m);
+      if (sd == KFUN3D_ERR_PIVOT) {
+        kf_set_error(KFUN3D_ERR_PIVOT, "singular or non-finite pivot block in ILU(0)");
+        steps = -1;
+        break;
+      }
+    }
+    bool step_net = use_net && its > 0;
+    const bool step_net0 = step_net;
+    double tol = 0.0, beta0 = 0.0, res = 0.0;
+    unsigned int total = 0;
+    bool done = false, failed = false;
+    for (int cycle = 0; total <= (unsigned)p->gmres_max_it; cycle++) {
+      if (total > 0) {   // true residual of the current iterate
+        dev_jacvec(m, o, m.x, m.t);
+        k_waxpy<<<nblk(n, 256), 256, 0, m.stream>>>(n, -1.0, m.t, m.r, Vb(m, 0), o.fast);
+        kf_count_launch();
+      }
+      dev_normalize(m, Vb(m, 0), m.scal + S_T0, o.fast);
+      fetch(m, S_T0, 1);
+      rs[0] = m.h_scal[S_T0];
+      if (!std::isfinite(rs[0])) { failed = true; break; }
+      if (total == 0) {
+        beta0 = rs[0];
+        tol = p->gmres_rtol * beta0;
+        res = beta0;
+        if (beta0 == 0.0) { done = true; break; }
+      }
+      const double beta_c = rs[0];
+      int k = 0;
+      while (k < restart) {
+        if (step_net) {
+          o.sptrsv(m, Vb(m, k), m.fy, prec);
+          if (kf_mpnn_apply_async(net, m.mgraph, m.fy, m.q, Zb(m, k), m.stream) != KFUN3D_OK) { failed = true; break; }
+          S.learned_its++;
+        } else {
+          o.sptrsv(m, Vb(m, k), Zb(m, k), prec);
+        }
+        dev_jacvec(m, o, Zb(m, k), Vb(m, k + 1));
+        orthogonalize(m, o, k);
+        fetch(m, 0, k + 2);
+        double *hh = ghh + k * (KF_NBASIS + 1);
+        for (int i = 0; i <= k + 1; i++) hh[i] = m.h_scal[i];
+        res = givens(hh, cs, sn, rs, k);
+        k++;
+        if (res <= tol) { done = true; break; }
+        if (!std::isfinite(res)) { failed = true; break; }
+        if (step_net && k >= 4 && rate_ilu < 0.0 && log(res / beta_c) > 0.5 * k * rate_ilu) {
+          step_net = false;   // the network is not pulling its weight in this solve
+          S.fallback_solves++;
+        }
+        if (ps && ps->stride > 0 && cycle == 0 && k < restart && !done && (k % ps->stride) == 0 &&
+            ps->count < ps->cap) {
+          back_substitute(ghh, rs, k, yk);
+          CK(cudaMemsetAsync(m.fx, 0, n * sizeof(double), m.stream));
+          for (int vv = 0; vv < k; vv++) dev_axpy(m, yk[vv], Zb(m, vv), m.fx, o.fast);
+          write_pair(m, o, prec, m.fx, *ps);
+        }
+      }
+      if (failed || k == 0) break;
+      total += k;
+      back_substitute(ghh, rs, k, yk);
+      for (int vv = 0; vv < k; vv++) dev_axpy(m, yk[vv], Zb(m, vv), m.x, o.fast);
+      if (done) break;
+    }
+    if (failed || !done) {
+      if (!failed && total > (unsigned)p->gmres_max_it) {
+        // iteration limit: keep the iterate, as the reference does
+      } else {
+        kf_set_error(KFUN3D_ERR_NONFINITE, "flexible GMRES: non-finite residual");
+        steps = -1;
+        break;
+      }
+    }
+    if (net && kf_mpnn_status(net, m.stream) != KFUN3D_OK) { steps = -1; break; }
+    S.gmres_its += (int)total;
+    if (!step_net0) {
+      plain_its_last = (int)total;
+      if (total > 0 && res > 0.0 && beta0 > 0.0) rate_ilu = log(res / beta0) / total;
+    } else if (plain_its_last >= 0 && (int)total > plain_its_last) {
+      if (++strikes >= 2) {
+        use_net = false;
+        S.disabled = 1;
+      }
+    } else {
+      strikes = 0;
+    }
+    if (ps && ps->count < ps->cap) write_pair(m, o, prec, m.x, *ps);
+    if (step_net0) CK(cudaMemcpyAsync(m.qold, m.q, n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+    last_used_net = step_net0;
+    dev_axpy(m, -1.0, m.x, m.q, o.fast);                           // src/kernel.c:200
+    k_forces<<<1, forces_threads(m.ncol), 0, m.stream>>>(m.ncol, m.col, m.wf_nodes, m.xyz, (const double4 *)m.q, u, v,
+                                                         m.forces);
+    kf_count_launch();
+    CK(cudaEventRecord(ev1, m.stream));
+    CK(cudaMemcpyAsync(m.h_scal + 48, m.forces, 3 * sizeof(double), cudaMemcpyDeviceToHost, m.stream));
+    CK(cudaStreamSynchronize(m.stream));
+    if (!check_cuda("flexible solve")) { steps = -1; break; }
+    if (device_status(m) == KFUN3D_ERR_TIMEOUT) {
+      kf_set_error(KFUN3D_ERR_TIMEOUT, "a triangular-solve wait exceeded its bound");
+      steps = -1;
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    if (hist && nrec < max_hist) {
+      hist[nrec] = kfun3d_step{its, (int)total, cfl, fnorm, m.h_scal[48], m.h_scal[49], m.h_scal[50], ms * 1e-3};
+      nrec++;
+    }
+    steps = its + 1;
+    if (round(fnorm0 / fnorm) >= p->stop_ratio) break;   // src/kernel.c:214
+  }
+  CK(cudaEventRecord(es1, m.stream));
+  CK(cudaEventSynchronize(es1));
+  float tot = 0.f;
+  cudaEventElapsedTime(&tot, es0, es1);
+  S.newton_steps = steps < 0 ? 0 : steps;
+  S.seconds = tot * 1e-3;
+  S.pairs = ps ? ps->count : 0;
+  if (st) *st = S;
+  for (cudaEvent_t e : {ev0, ev1, es0, es1}) cudaEventDestroy(e);
   return steps < 0 ? -1 : nrec;
 }
 
@@ -1074,5 +1365,76 @@ extern "C" double kfun3d_time_solve(GEOMETRY *g, const kfun3d_solver_params *p, 
   cudaFree(q0);
   if (nsteps) *nsteps = ns;
   if (!finish(*m, "kfun3d_time_solve") || ns < 0) return -1.0;
+  return total / reps;
+}
+
+// ---- flexible GMRES and the learned preconditioner
+
+extern "C" int kfun3d_solve_flexible(GEOMETRY *g, const kfun3d_solver_params *p, kfun3d_mpnn *net,
+                                     kfun3d_step *hist, int max_hist, kfun3d_flex_stats *stats)
+{
+  DevMesh *m = dev_or_fail(g);
+  if (!m) return -1;
+  kfun3d_solver_params def;
+  if (!p) { kfun3d_default_params(&def); p = &def; }
+  h2d(*m, m->q, g->q->q, 4 * (size_t)m->N);
+  const int n = solve_flexible(*m, g, p, net, nullptr, hist, max_hist, stats);
+  d2h(*m, g->q->q, m->q, 4 * (size_t)m->N);
+  d2h(*m, g->n->cdt, m->cdt, m->N);
+  if (!finish(*m, "kfun3d_solve_flexible")) return -1;
+  return n;
+}
+
+extern "C" int kfun3d_collect_pairs(GEOMETRY *g, const kfun3d_solver_params *p, int stride, void *d_x0,
+                                    float *d_target, int cap, kfun3d_flex_stats *stats)
+{
+  if (!d_x0 || !d_target || cap < 0) {
+    kf_set_error(KFUN3D_ERR_ARG, "kfun3d_collect_pairs: bad arguments");
+    return -1;
+  }
+  DevMesh *m = dev_or_fail(g);
+  if (!m) return -1;
+  kfun3d_solver_params def;
+  if (!p) { kfun3d_default_params(&def); p = &def; }
+  PairSink ps;
+  ps.stride = stride;
+  ps.x0 = (unsigned char *)d_x0;
+  ps.tgt = d_target;
+  ps.cap = cap;
+  h2d(*m, m->q, g->q->q, 4 * (size_t)m->N);
+  const int n = solve_flexible(*m, g, p, nullptr, &ps, nullptr, 0, stats);
+  d2h(*m, g->q->q, m->q, 4 * (size_t)m->N);
+  d2h(*m, g->n->cdt, m->cdt, m->N);
+  if (!finish(*m, "kfun3d_collect_pairs")) return -1;
+  return n < 0 ? -1 : ps.count;
+}
+
+extern "C" double kfun3d_time_solve_flexible(GEOMETRY *g, const kfun3d_solver_params *p, kfun3d_mpnn *net,
+                                             int reps, kfun3d_step *hist, int max_hist, int *nsteps,
+                                             kfun3d_flex_stats *stats)
+{
+  DevMesh *m = dev_or_fail(g);
+  if (!m || reps < 1) return -1.0;
+  kfun3d_solver_params def;
+  if (!p) { kfun3d_default_params(&def); p = &def; }
+  const size_t n = 4 * (size_t)m->N;
+  double *q0 = nullptr;
+  CK(cudaMalloc(&q0, n * sizeof(double)));
+  if (!q0) return -1.0;
+  h2d(*m, q0, g->q->q, n);
+  double total = 0.0;
+  int ns = 0;
+  for (int r = 0; r < reps; r++) {
+    CK(cudaMemcpyAsync(m->q, q0, n * sizeof(double), cudaMemcpyDeviceToDevice, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    kfun3d_flex_stats st{};
+    ns = solve_flexible(*m, g, p, net, nullptr, hist, max_hist, &st);
+    total += st.seconds;
+    if (stats) *stats = st;
+    if (ns < 0) break;
+  }
+  cudaFree(q0);
+  if (nsteps) *nsteps = ns;
+  if (!finish(*m, "kfun3d_time_solve_flexible") || ns < 0) return -1.0;
   return total / reps;
 }

@@ -128,18 +128,19 @@ def loss_and_grad(theta, g, x0, target, weight):
     t = torch.as_tensor(target, dtype=torch.float64)
     loss = weight * ((out - t) ** 2).sum()
     loss.backward()
-    return float(loss), th.grad.numpy().copy()
+    return float(loss.detach()), th.grad.numpy().copy()
 
 
 def adam(theta, m, v, grad, step, lr, b1=0.9, b2=0.999, eps=1e-8):
     """One Adam step in FP32 (the kernel's arithmetic), returns new (theta, m, v)."""
     f = np.float32
     theta, m, v, grad = (np.asarray(a, np.float32) for a in (theta, m, v, grad))
-    c1 = f(1.0 - b1 ** step)
+    b1f, b2f = f(b1), f(b2)
+    c1 = f(1.0 - b1 ** step)          # formed in double, rounded once
     c2 = f(1.0 - b2 ** step)
-    m2 = f(b1) * m + f(1.0 - b1) * grad
-    v2 = f(b2) * v + f(1.0 - b2) * grad * grad
-    th2 = theta - f(lr) * (m2 / c1) / (np.sqrt(v2 / c2) + f(eps))
+    m2 = b1f * m + (f(1.0) - b1f) * grad
+    v2 = b2f * v + ((f(1.0) - b2f) * grad) * grad
+    th2 = theta - (f(lr) * (m2 / c1)) / (np.sqrt(v2 / c2) + f(eps))
     return th2.astype(np.float32), m2.astype(np.float32), v2.astype(np.float32)
 
 

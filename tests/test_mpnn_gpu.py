@@ -108,7 +108,9 @@ def test_adam_step_matches_oracle(box_mesh):
     net.adam_step(lr=1e-3)
     th1 = net.params()
     ref, _, _ = mpnn_ref.adam(th, np.zeros_like(th), np.zeros_like(th), g, 1, 1e-3)
-    assert np.allclose(th1, ref, rtol=1e-6, atol=1e-9)
+    # the same FP32 operations in the same order, each rounded on its own
+    bad = np.flatnonzero(th1 != ref)
+    assert bad.size == 0, (bad[:5], th1[bad[:5]], ref[bad[:5]], g[bad[:5]])
     assert np.all(net.grad() == 0.0)   # cleared by the step
 
 
