@@ -47,10 +47,13 @@ CONFIGS = {
     2: dict(workload="config2: 70^3 Kuhn box, FP32 Jacobian/ILU(0)/SpTRSV, FP64 residual and GMRES, to 1e-8 drop",
             n=70, seed=1, bump=0.1, aoa=3.06, precision=1, mode="fast", first_order=False,
             ts_max=20, stop_ratio=1e8),
-    4: dict(workload="config4: 120^3 Kuhn box (bump 0.12, AoA 4.5), FP32 preconditioner, to 1e-8 drop",
+    4: dict(workload="config4: 120^3 Kuhn box (bump 0.12, AoA 4.5, held out of training), mixed precision + "
+                     "learned FGMRES against plain FP64, to 1e-8 drop",
             n=120, seed=4, bump=0.12, aoa=4.5, precision=1, mode="fast", first_order=False,
-            ts_max=20, stop_ratio=1e8),
+            ts_max=20, stop_ratio=1e8, learned=True, ref_ts=1),
 }
+WEIGHTS = os.path.join(ROOT, "kfun3d_b200", "weights", "mpnn_box40.npy")
+DEFAULT_CONFIG = 1
 
 
 def log(*a):
@@ -207,7 +210,7 @@ def host_cores():
 
 def reference_sample(path, cfg, total_its, threads):
     """Time the reference (oracle/_ref) on a bounded sample of the solve: its
-    first two Newton steps on the same mesh and settings, at `threads` OpenMP
+    first Newton steps (two, one at 120^3) on the same mesh and settings, at `threads` OpenMP
     threads.  Seconds to the 1e-8 drop are extrapolated by GMRES iterations:
     sample_time * total_its / sample_its (the per-iteration work of this solver
     is the same at every step)."""
@@ -222,7 +225,7 @@ def reference_sample(path, cfg, total_its, threads):
         m.flux(q0)
     t_flux = (time.perf_counter() - t0) / nflux
     t0 = time.perf_counter()
-    hist = m.solve(ts_max=2, stop_ratio=cfg["stop_ratio"])
+    hist = m.solve(ts_max=cfg.get("ref_ts", 2), stop_ratio=cfg["stop_ratio"])
     t_sample = time.perf_counter() - t0
     its = sum(h["gmres_its"] for h in hist)
     m.close()
@@ -257,7 +260,7 @@ def run_reference_arm(args, cfg):
             vals.append(reference_sample(path, cfg, total_its, threads))
     wall = time.perf_counter() - t_all
     value = statistics.mean(v["seconds"] for v in vals)
-    sample = (f"first 2 Newton steps ({vals[-1]['sample_its']} GMRES iterations, "
+    sample = (f"first {cfg.get('ref_ts', 2)} Newton step(s) ({vals[-1]['sample_its']} GMRES iterations, "
               f"{vals[-1]['sample_seconds']:.2f} s) of the workload, extrapolated to {total_its} iterations")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3,
@@ -302,9 +305,22 @@ def run_gpu_arm(args, cfg):
     v = m.view
     N, E = v.nnodes, v.nedges
     params = dict(ts_max=cfg["ts_max"], stop_ratio=cfg["stop_ratio"])
+    net = None
+    if cfg.get("learned"):
+        from kfun3d_b200 import learned
+        if not os.path.exists(WEIGHTS):
+            raise SystemExit(f"trained network missing: {WEIGHTS} (python -m kfun3d_b200.train_mpnn)")
+        net = learned.Network.load(WEIGHTS)
+
+    def timed(reps):
+        """Mean device seconds of `reps` solves of the workload's form from free stream."""
+        if net is not None:
+            return m.time_solve_flexible(net=net, reps=reps, **params)
+        t, h = m.time_solve(reps=reps, **params)
+        return t, h, None
 
     # warm-up (uploads the mesh, builds the device mirror)
-    m.time_solve(reps=args.warmup, **params)
+    timed(args.warmup)
     cuda_sync()
     dist.barrier()
     cuda_sync()
@@ -313,7 +329,7 @@ def run_gpu_arm(args, cfg):
         sampler.start()
     kf.reset_launch_count()
     t_wall = time.perf_counter()
-    t_solve, hist = m.time_solve(reps=args.steps, **params)
+    t_solve, hist, fstats = timed(args.steps)
     cuda_sync()
     launches = kf.launch_count()
     dist.barrier()
@@ -330,10 +346,32 @@ def run_gpu_arm(args, cfg):
     for _ in range(max(1, min(args.steps, 3))):
         v.q[:] = q0
         t0 = time.perf_counter()
-        m.solve(**params)
+        if net is not None:
+            m.solve_flexible(net=net, **params)
+        else:
+            m.solve(**params)
         e2e.append(time.perf_counter() - t0)
     v.q[:] = q0
     e2e_value = dist.max(statistics.mean(e2e))
+
+    # the learned form against plain FP64 (the reference's method) and against
+    # the same mixed-precision FGMRES without the network, one solve each
+    comparison = None
+    if net is not None:
+        f_ours = [hist[-1][k] for k in ("lift", "drag", "momn")]
+        t_ilu, h_ilu, st_ilu = m.time_solve_flexible(net=None, reps=1, **params)
+        kf.set_precision(0)
+        t_plain, h_plain = m.time_solve(reps=1, **params)
+        kf.set_precision(cfg["precision"])
+        f_plain = [h_plain[-1][k] for k in ("lift", "drag", "momn")]
+        comparison = {
+            "plain_fp64_s": t_plain, "plain_fp64_gmres_its": sum(h["gmres_its"] for h in h_plain),
+            "plain_fp64_newton_steps": len(h_plain),
+            "speedup_vs_plain_fp64": t_plain / value,
+            "mixed_ilu_fgmres_s": t_ilu, "mixed_ilu_fgmres_gmres_its": st_ilu["gmres_its"],
+            "learned_stats": fstats,
+            "forces_rel_err_vs_fp64": max(abs(a - b) / abs(b) for a, b in zip(f_ours, f_plain)),
+        }
 
     # per-kernel live timing (CUDA events on the solver's stream)
     peak, peak_kind = peaks()
@@ -365,7 +403,7 @@ def run_gpu_arm(args, cfg):
             with CStdoutToStderr():
                 s = reference_sample(path, cfg, gmres_its, threads)
             cpu = {"value": s["seconds"], "unit": "s", "cores": threads, "kind": "reference",
-                   "sample": (f"reference (oracle/_ref) first 2 Newton steps of this workload: "
+                   "sample": (f"reference (oracle/_ref) first {cfg.get('ref_ts', 2)} Newton step(s) of this workload: "
                               f"{s['sample_its']} GMRES iterations in {s['sample_seconds']:.2f} s at "
                               f"{threads} threads, extrapolated to this solve's {gmres_its} iterations"),
                    "flux_edges_per_s": s["flux_edges_per_s"]}
@@ -388,6 +426,7 @@ def run_gpu_arm(args, cfg):
             "fill_edges_per_s": E / (t["fill"] * 1e-3),
             "gmres_iterations_per_s": gmres_its / value,
             "gpu_launches": int(launches),
+            "comparison": comparison,
             "clocks": clocks,
             "cpu_baseline": cpu,
             "wall_s": wall,
@@ -403,7 +442,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=1, choices=sorted(CONFIGS))
+    ap.add_argument("--config", type=int, default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-total-its", type=int, default=741,
                     help="GMRES iterations of the full solve used to extrapolate the reference sample")

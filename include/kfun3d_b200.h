@@ -298,11 +298,13 @@ typedef struct {
  * number of history entries or -1. */
 int kfun3d_solve_flexible(GEOMETRY *g, const kfun3d_solver_params *p, kfun3d_mpnn *net, kfun3d_step *hist,
                           int max_hist, kfun3d_flex_stats *stats);
-/* The ILU(0)-FGMRES solve writing training pairs: for the iterate after every
- * `stride` iterations of each Newton step's first cycle, and for the step's
- * final correction x, v = J x, y = ILU(0)^-1 v and the pair
- * (BF16([y/s, q]), (x - y)/s) into slot i of d_x0 ([cap][N x 8] BF16) and
- * d_target ([cap][N x 4] FP32).  Returns the number of pairs or -1. */
+/* The ILU(0)-FGMRES solve writing training pairs (x, v = J x): the pair
+ * (BF16([y/s, q]), (x - y)/s) with y = ILU(0)^-1 v, s = RMS(y), goes to slot i
+ * of d_x0 ([cap][N x 8] BF16) and d_target ([cap][N x 4] FP32).  x is each
+ * Newton step's final correction and, for stride > 0, the iterate after every
+ * `stride` iterations of the step's first cycle; for stride < 0, the
+ * preconditioned basis vector z_k of every -stride-th iteration (v = J z_k,
+ * the product the iteration forms anyway).  Returns the number of pairs or -1. */
 int kfun3d_collect_pairs(GEOMETRY *g, const kfun3d_solver_params *p, int stride, void *d_x0, float *d_target,
                          int cap, kfun3d_flex_stats *stats);
 /* Mean device seconds of `reps` flexible solves from g->q->q (not updated). */

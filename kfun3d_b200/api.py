@@ -378,7 +378,9 @@ class Mesh:
                                        C.byref(st))
         if n < 0:
             raise RuntimeError(f"kfun3d_collect_pairs failed: {last_error()}")
-        return x0[:n], tgt[:n], st.as_dict()
+        if n < cap:
+            x0, tgt = x0[:n].clone(), tgt[:n].clone()
+        return x0, tgt, st.as_dict()
 
     def release_device(self):
         lib().kfun3d_device_release(self.g)

@@ -483,6 +483,8 @@ DevMesh *kf_device(const GEOMETRY *g)
     // cooperative grid: 4 blocks of 256 threads per SM (the kernel's launch
     // bounds guarantee they fit); the runtime refuses the launch otherwise
     m->trsv_grid = (unsigned)nsm * 4;
+    // one 512-thread CTA per SM (launch bounds (512, 1))
+    m->trsv_mgrid = (unsigned)nsm;
     std::vector<uint4> dl(N), du(N);
     for (uint32_t s = 0; s < N; s++) {
       const uint32_t i = p.lev_l[s];
@@ -503,11 +505,12 @@ DevMesh *kf_device(const GEOMETRY *g)
     if (env && strcmp(env, "persistent") == 0) m->trsv_mode = 3;
     if (env && strcmp(env, "syncfree") == 0) m->trsv_mode = 1;
     if (env && strcmp(env, "levels") == 0) m->trsv_mode = 0;
+    if (env && strcmp(env, "mono") == 0) m->trsv_mode = 5;
     std::vector<uint32_t> lp(p.lev_l_ptr);
     lp.insert(lp.end(), p.lev_u_ptr.begin(), p.lev_u_ptr.end());
     KF_CUDA(upload(&m->lev_ptr_d, lp.data(), lp.size()));
-    KF_CUDA(cudaMalloc(&m->bar, 4 * sizeof(unsigned)));
-    KF_CUDA(cudaMemset(m->bar, 0, 4 * sizeof(unsigned)));
+    KF_CUDA(cudaMalloc(&m->bar, 8 * sizeof(unsigned)));
+    KF_CUDA(cudaMemset(m->bar, 0, 8 * sizeof(unsigned)));
     m->syncfree = m->trsv_mode == 1;
     const char *genv = getenv("KFUN3D_GRAPHS");
     m->use_graphs = !(genv && strcmp(genv, "0") == 0);

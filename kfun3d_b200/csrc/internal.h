@@ -147,7 +147,8 @@ struct DevMesh {
   bool syncfree = true;
   int trsv_mode = 4;               // 0 levels (4 lanes/row), 1 sync-free, 2 levels (16 lanes/row),
                                    // 3 one persistent launch, grid barrier between levels,
-                                   // 4 levels with programmatic dependent launch
+                                   // 4 levels with programmatic dependent launch,
+                                   // 5 one persistent launch, one CTA per SM, counter barrier
   unsigned trsv_grid = 0;          // persistent grid (whole blocks resident on every SM)
   uint32_t *flags = nullptr;       // [N] per-row completion epoch
   unsigned long long *ticket = nullptr;   // unused (kept zero)
@@ -160,9 +161,11 @@ struct DevMesh {
   bool use_graphs = true;
   unsigned mgs_grid = 0;          // cooperative grid for the Gram-Schmidt kernel
   double *part = nullptr;         // [2][mgs_grid] block partial sums
-  unsigned *bar = nullptr;        // grid-barrier words (see kf_grid_barrier), [0..3]
+  unsigned *bar = nullptr;        // grid-barrier words: [0..1] persistent sweep, [2..3] Gram-Schmidt,
+                                  // [4] counter of the one-CTA-per-SM sweep
   uint32_t *lev_ptr_d = nullptr;  // [nlev_l+1 + nlev_u+1] level offsets on the device
   unsigned trsv_pgrid = 0;        // persistent sweep grid
+  unsigned trsv_mgrid = 0;        // one-CTA-per-SM persistent sweep grid (mode 5)
   double *h_scal = nullptr;       // pinned host mirror of scal
   // flexible GMRES (right preconditioning) and the learned preconditioner
   double *Z = nullptr;            // [30][4N] preconditioned basis vectors

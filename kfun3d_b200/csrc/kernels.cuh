@@ -1395,6 +1395,65 @@ __global__ void __launch_bounds__(256, 4) k_trsv_persistent(const uint32_t *__re
   }
 }
 
+// Grid barrier on a counter that only grows within one launch (cleared before
+// it): every CTA adds one on arrival and waits, bounded, until the counter
+// reaches target = (barriers passed so far) x (CTAs).  One atomic per CTA, no
+// generation word to flip.
+__device__ __forceinline__ bool kf_mono_barrier(unsigned *cnt, unsigned target, int *err)
+{
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    atomicAdd(cnt, 1u);
+    unsigned spins = 0, v = 0;
+    while (true) {
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(cnt) : "memory");
+      if (v >= target) break;
+      if (++spins > KF_BARRIER_LIMIT) { atomicExch(err, 1); ok = 0; break; }
+      if ((spins & 255) == 0 && *(volatile int *)err) { ok = 0; break; }
+    }
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+// Both sweeps in one cooperative launch of one 512-thread CTA per SM; levels
+// separated by kf_mono_barrier.  Arithmetic as in k_trsv_level16.
+template <typename T>
+__global__ void __launch_bounds__(512, 1) k_trsv_persistent_mono(const uint32_t *__restrict__ lev_l, uint32_t nl,
+                                                                 const uint32_t *__restrict__ lev_u, uint32_t nu,
+                                                                 const uint4 *__restrict__ desc_l,
+                                                                 const uint4 *__restrict__ desc_u,
+                                                                 const uint32_t *__restrict__ ja,
+                                                                 const T *__restrict__ A,
+                                                                 const double *__restrict__ b, double *x,
+                                                                 unsigned *cnt, int *err)
+{
+  const int lane = threadIdx.x & 31, half = lane >> 4, l16 = lane & 15, jj = l16 >> 2, r = l16 & 3;
+  const unsigned hmask = 0xffffu << (16 * half);
+  const uint32_t H = gridDim.x * (blockDim.x >> 4);
+  const uint32_t h = blockIdx.x * (blockDim.x >> 4) + (threadIdx.x >> 4);
+  unsigned passed = 0;
+  for (uint32_t l = 0; l < nl; l++) {
+    const uint32_t s1 = lev_l[l + 1];
+    for (uint32_t s = lev_l[l] + h; s < s1; s += H)
+      trsv_row16<T, false>(desc_l[s], ja, A, b, x, half, jj, r, l16, hmask);
+    __threadfence();
+    if (!kf_mono_barrier(cnt, ++passed * gridDim.x, err)) return;
+  }
+  for (uint32_t l = 0; l < nu; l++) {
+    const uint32_t s1 = lev_u[l + 1];
+    for (uint32_t s = lev_u[l] + h; s < s1; s += H)
+      trsv_row16<T, true>(desc_u[s], ja, A, b, x, half, jj, r, l16, hmask);
+    __threadfence();
+    if (l + 1 < nu && !kf_mono_barrier(cnt, ++passed * gridDim.x, err)) return;
+  }
+}
+
 // Level-synchronous sweep with programmatic dependent launch: each level's
 // kernel lets the next one start at once (griddepcontrol.launch_dependents);
 // the next kernel loads everything that does not depend on earlier levels --
@@ -1773,6 +1832,32 @@ void sptrsv(DevMesh &m, const double *b, double *x, int precision)
         kf_count_launch();
       }
     }
+    return;
+  }
+  if (m.trsv_mode == 5) {
+    const uint32_t *levl = m.lev_ptr_d, *levu = m.lev_ptr_d + m.nlev_l + 1;
+    uint32_t nl = m.nlev_l, nu = m.nlev_u;
+    const double *bb = b;
+    unsigned *cnt = m.bar + 4;
+    int *err = m.status + 1;
+    cudaMemsetAsync(cnt, 0, sizeof(unsigned), m.stream);
+    const void *Ap = precision == 0 ? (const void *)m.A : (const void *)m.Af;
+    void *args[] = {(void *)&levl, &nl, (void *)&levu, &nu, (void *)&m.desc_l, (void *)&m.desc_u,
+                    (void *)&m.ja, (void *)&Ap, (void *)&bb, (void *)&x, (void *)&cnt, (void *)&err};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(m.trsv_mgrid);
+    cfg.blockDim = dim3(512);
+    cfg.stream = m.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const void *fn = precision == 0 ? (const void *)k_trsv_persistent_mono<double>
+                                    : (const void *)k_trsv_persistent_mono<float>;
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
+    if (e != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e));
+    kf_count_launch();
     return;
   }
   if (m.trsv_mode == 3) {

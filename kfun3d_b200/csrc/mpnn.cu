@@ -857,8 +857,10 @@ uint64_t splitmix(uint64_t &s)
   return z ^ (z >> 31);
 }
 
-// He-uniform for layers followed by a ReLU, Glorot-uniform for the others,
-// a tenth of that for the output layer; biases and padding zero.
+// He-uniform for layers followed by a ReLU, Glorot-uniform for the others;
+// messages scaled by 1/4 (a node sums about 14 of them) and the output layer
+// by 1/100 (the untrained network starts close to plain ILU(0)); biases and
+// padding zero.
 void init_params(std::vector<float> &th, unsigned long long seed)
 {
   th.assign(NPARAM, 0.f);
@@ -867,7 +869,8 @@ void init_params(std::vector<float> &th, unsigned long long seed)
     const LayerShape sh = kShape[L];
     const bool relu_after = (L % 2) == 0;   // first layer of every MLP
     double bound = relu_after ? std::sqrt(6.0 / sh.nreal) : std::sqrt(6.0 / (sh.nreal + sh.out));
-    if (L == L_DEC2) bound *= 0.1;
+    if (L == L_DEC2) bound *= 0.01;
+    if (L >= 2 && L < 14 && (L - 2) % 4 == 1) bound *= 0.25;   // edge2 of each layer
     const int nout = (L == L_DEC2) ? 4 : sh.out;
     for (int o = 0; o < nout; o++)
       for (int f = 0; f < sh.nreal; f++) {

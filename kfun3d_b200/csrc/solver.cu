@@ -558,7 +558,7 @@ int device_status(DevMesh &m)
   if (st[0] || st[1]) {
     CK(cudaMemsetAsync(m.status, 0, 2 * sizeof(int), m.stream));
     // a wait that gave up may leave a grid barrier half-counted
-    if (st[1] && m.bar) CK(cudaMemsetAsync(m.bar, 0, 4 * sizeof(unsigned), m.stream));
+    if (st[1] && m.bar) CK(cudaMemsetAsync(m.bar, 0, 8 * sizeof(unsigned), m.stream));
   }
   if (st[1]) return KFUN3D_ERR_TIMEOUT;
   return st[0];
@@ -807,7 +807,12 @@ void write_pair(DevMesh &m, const Ops &o, int prec, const double *x, PairSink &p
 // allowed to change from one iteration to the next:
 //   z_k = M_k(v_k),  w = J z_k orthogonalised against v_0..v_k,
 //   x = Z y after each cycle, the true residual b - J x at a restart.
-// M_k is ILU(0)^-1, or with a network the network's correction of it.  The
+// M_k is ILU(0)^-1, or with a network the network's correction of it.  A
+// linear solve stops once the true residual |b - J x| has fallen by
+// gmres_rtol (within a cycle), or -- checked at every restart -- the
+// ILU(0)-preconditioned residual has, which is the reference's own measure
+// (right preconditioning alone can stall on the true residual where the
+// reference's left-preconditioned GMRES converges).  The
 // network is a guest: Newton step 0 runs on ILU(0) alone to measure its
 // convergence rate; a linear solve whose residual falls at less than half
 // that rate after 4 iterations continues on ILU(0) alone; two steps in a row
@@ -889,14 +894,23 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
     }
     bool step_net = use_net && its > 0;
     const bool step_net0 = step_net;
-    double tol = 0.0, beta0 = 0.0, res = 0.0;
+    double tol = 0.0, beta0 = 0.0, res = 0.0, pres0 = 0.0;
     unsigned int total = 0;
     bool done = false, failed = false;
+    // the reference's own measure, |ILU(0)^-1 (b - J x)|, at every restart
+    o.sptrsv(m, m.r, m.fy, prec);
+    dev_reduce(m, m.fy, m.fy, m.scal + S_T0 + 1, 1, o.fast);
+    fetch(m, S_T0 + 1, 1);
+    pres0 = m.h_scal[S_T0 + 1];
     for (int cycle = 0; total <= (unsigned)p->gmres_max_it; cycle++) {
       if (total > 0) {   // true residual of the current iterate
         dev_jacvec(m, o, m.x, m.t);
         k_waxpy<<<nblk(n, 256), 256, 0, m.stream>>>(n, -1.0, m.t, m.r, Vb(m, 0), o.fast);
         kf_count_launch();
+        o.sptrsv(m, Vb(m, 0), m.fy, prec);
+        dev_reduce(m, m.fy, m.fy, m.scal + S_T0 + 1, 1, o.fast);
+        fetch(m, S_T0 + 1, 1);
+        if (m.h_scal[S_T0 + 1] <= p->gmres_rtol * pres0) { done = true; break; }
       }
       dev_normalize(m, Vb(m, 0), m.scal + S_T0, o.fast);
       fetch(m, S_T0, 1);
@@ -919,6 +933,13 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
           o.sptrsv(m, Vb(m, k), Zb(m, k), prec);
         }
         dev_jacvec(m, o, Zb(m, k), Vb(m, k + 1));
+        if (ps && ps->stride < 0 && (k % -ps->stride) == 0 && ps->count < ps->cap) {
+          // basis pair: w = J z_k (not yet orthogonalised), y = ILU(0)^-1 w, target from z_k
+          o.sptrsv(m, Vb(m, k + 1), m.fy, prec);
+          kf_mpnn_pair_async(m.N, m.fy, m.q, Zb(m, k), ps->x0 + (size_t)ps->count * 16 * m.N,
+                             ps->tgt + (size_t)ps->count * 4 * m.N, m.pscr, m.stream);
+          ps->count++;
+        }
         orthogonalize(m, o, k);
         fetch(m, 0, k + 2);
         double *hh = ghh + k * (KF_NBASIS + 1);

@@ -143,3 +143,85 @@ def make_pair(y, q, x=None):
     _check(lib().kfun3d_mpnn_make_pair(n, y.data_ptr(), q.data_ptr(), x.data_ptr() if x is not None else None,
                                        x0.data_ptr(), tgt.data_ptr() if tgt is not None else None), "make_pair")
     return x0, tgt
+
+
+# ---------------------------------------------------------------- training
+
+class Sample:
+    """Pairs of one mesh kept on the device, with its graph."""
+
+    def __init__(self, mesh, graph, x0, target, aoa, bump, stats):
+        self.mesh, self.graph, self.x0, self.target = mesh, graph, x0, target
+        self.aoa, self.bump, self.stats = aoa, bump, stats
+
+    def __len__(self):
+        return int(self.x0.shape[0])
+
+
+def training_set(workdir, n_meshes=128, n=40, seed=0, stride=-3, cap=160, bump=(0.05, 0.15), aoa=(0.0, 6.0),
+                 log=None, **params):
+    """Seeded Kuhn-box meshes (n^3 nodes, bump height and angle of attack drawn
+    uniformly from the given ranges), each solved from free stream by the
+    ILU(0)-FGMRES solve writing training pairs on the GPU
+    (kfun3d_collect_pairs).  The solver's device mirror of each mesh is
+    released afterwards; its graph and pairs stay on the device."""
+    import os
+    from .api import Mesh, generate_mesh, set_aoa, get_aoa
+    os.makedirs(workdir, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    p = dict(ts_max=20, stop_ratio=1e8)
+    p.update(params)
+    keep_aoa = get_aoa()
+    out = []
+    try:
+        for i in range(n_meshes):
+            b = float(rng.uniform(*bump))
+            a = float(rng.uniform(*aoa))
+            path = os.path.join(workdir, f"train_{n}_{seed}_{i}.msh")
+            generate_mesh(path, n, bump_height=b, seed=int(rng.integers(1 << 31)))
+            m = Mesh(path)
+            os.remove(path)
+            set_aoa(a)
+            x0, tgt, st = m.collect_pairs(stride=stride, cap=cap, **p)
+            g = Graph(m)
+            m.release_device()
+            out.append(Sample(m, g, x0, tgt, a, b, st))
+            if log:
+                log(f"mesh {i}: aoa {a:.2f} bump {b:.3f} pairs {len(x0)} its {st['gmres_its']}")
+    finally:
+        set_aoa(keep_aoa)
+    return out
+
+
+def train(net, data, steps, batch=8, lr=1e-3, seed=0, log=None, log_every=100):
+    """Adam on the mean squared error over pairs: each step draws `batch`
+    pairs at random (the kernels accumulate their gradients), then one Adam
+    step.  Returns the per-step loss."""
+    rng = np.random.default_rng(seed)
+    index = [(k, j) for k, s in enumerate(data) for j in range(len(s))]
+    if not index:
+        raise ValueError("no training pairs")
+    losses = []
+    for it in range(steps):
+        pick = rng.choice(len(index), size=min(batch, len(index)), replace=False)
+        loss = 0.0
+        for q in pick:
+            k, j = index[q]
+            s = data[k]
+            loss += net.accumulate(s.graph, s.x0[j], s.target[j], 1.0 / (len(pick) * 4 * s.graph.nnodes))
+        net.adam_step(lr=lr)
+        losses.append(loss)
+        if log and (it % log_every == 0 or it == steps - 1):
+            log(f"step {it}: loss {np.mean(losses[-log_every:]):.4e}")
+    return losses
+
+
+def zero_loss(data):
+    """Loss of the zero correction (plain ILU(0)) over all pairs: the scale
+    against which a trained loss is read."""
+    tot, cnt = 0.0, 0
+    for s in data:
+        for j in range(len(s)):
+            tot += float((s.target[j].double() ** 2).sum()) / (4 * s.graph.nnodes)
+            cnt += 1
+    return tot / max(cnt, 1)

@@ -198,3 +198,31 @@ def test_blas_entry_points():
     nrm = kf.api.normalize(z)
     assert nrm == np.sqrt(s)
     assert np.array_equal(z, x * (1.0 / nrm))
+
+
+@pytest.mark.parametrize("schedule", ["levels", "syncfree", "levels16", "persistent", "pdl", "mono"])
+def test_exact_sptrsv_every_schedule(box_mesh, schedule, monkeypatch):
+    """Every triangular-solve schedule (chosen when the device mirror is built)
+    gives the oracle's solve bit for bit in exact mode, FP64 and FP32."""
+    monkeypatch.setenv("KFUN3D_SPTRSV", schedule)
+    kf.set_mode("exact")
+    kf.set_aoa(3.06)
+    m = kf.Mesh(box_mesh(12, seed=31))
+    v = m.view
+    q = seeded_state(v.q.copy(), 31)
+    cdt = port.timestep(m.g, v.nnodes, 40.0, q)
+    M = port.Matrix(m.g)
+    b = np.random.default_rng(31).standard_normal(v.dofs)
+    for prec in (0, 1):
+        kf.set_precision(prec)
+        m.fill(q, cdt)
+        M.fill(3.06, q, cdt)
+        m.ilu()
+        if prec == 0:
+            M.ilu()
+            assert np.array_equal(m.sptrsv(b), M.sptrsv(b)), schedule
+        else:
+            M.ilu_f32()
+            assert rel(m.sptrsv(b), M.sptrsv_f32(b)) < 1e-5, schedule
+    kf.set_precision(0)
+    assert kf.last_status() == 0
