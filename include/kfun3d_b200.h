@@ -280,36 +280,44 @@ typedef struct {
   int newton_steps;     /* Newton steps taken */
   int gmres_its;        /* FGMRES iterations over the solve */
   int learned_its;      /* iterations preconditioned by the network */
-  int fallback_solves;  /* linear solves that went on with ILU(0) alone part-way */
+  int fallback_solves;  /* linear solves run without the network: it lost the first direction */
   int rejected_steps;   /* updates undone because the nonlinear residual grew tenfold */
   int disabled;         /* 1: the network was switched off for the rest of the solve */
   int pairs;            /* training pairs written (kfun3d_collect_pairs) */
   double seconds;       /* device time of the whole solve */
 } kfun3d_flex_stats;
 
-/* The pseudo-transient solve of Kernel() with FGMRES(restart) in place of
- * left-preconditioned GMRES: right preconditioning z = ILU(0)^-1 v, or with
- * net != NULL the network's correction of it, chosen per iteration.  The
- * network runs from Newton step 1 on and falls back to ILU(0) alone: within a
- * linear solve whose residual falls at less than half ILU(0)'s rate, for good
- * after two steps that need more iterations than the last ILU(0)-only solve,
+/* The pseudo-transient solve of Kernel() with flexible GMRES(restart) on the
+ * reference's left-preconditioned system (Arnoldi on ILU(0)^-1 J, the
+ * reference's residual measure and stopping test) and a right preconditioner
+ * that may change per iteration: the identity (net == NULL: the reference's
+ * GMRES, iteration for iteration) or the network's correction
+ * v + s N([v/s, q]).  The network falls back to the identity: for a linear
+ * solve whose first direction it does not improve (its image under
+ * ILU(0)^-1 J farther from v0), for good after three such solves in a row,
  * and for an update after which the FP64 nonlinear residual grows tenfold
  * (the update is undone).  Solves from g->q->q and updates it; returns the
  * number of history entries or -1. */
 int kfun3d_solve_flexible(GEOMETRY *g, const kfun3d_solver_params *p, kfun3d_mpnn *net, kfun3d_step *hist,
                           int max_hist, kfun3d_flex_stats *stats);
-/* The ILU(0)-FGMRES solve writing training pairs (x, v = J x): the pair
- * (BF16([y/s, q]), (x - y)/s) with y = ILU(0)^-1 v, s = RMS(y), goes to slot i
- * of d_x0 ([cap][N x 8] BF16) and d_target ([cap][N x 4] FP32).  x is each
- * Newton step's final correction and, for stride > 0, the iterate after every
- * `stride` iterations of the step's first cycle; for stride < 0, the
- * preconditioned basis vector z_k of every -stride-th iteration (v = J z_k,
- * the product the iteration forms anyway).  Returns the number of pairs or -1. */
+/* The flexible solve without a network, writing training pairs (x, y) with
+ * ILU(0)^-1 J x = y: the pair (BF16([y/s, q]), (x - y)/s), s = RMS(y), goes
+ * to slot i of d_x0 ([cap][N x 8] BF16) and d_target ([cap][N x 4] FP32).  x
+ * is each Newton step's final correction (y = ILU(0)^-1 J x formed for it)
+ * and, for stride > 0, the iterate after every `stride` iterations of the
+ * step's first cycle; for stride < 0, the Krylov vector v_k of every
+ * -stride-th iteration with y = ILU(0)^-1 J v_k, the product the iteration
+ * forms anyway.  Returns the number of pairs or -1. */
 int kfun3d_collect_pairs(GEOMETRY *g, const kfun3d_solver_params *p, int stride, void *d_x0, float *d_target,
                          int cap, kfun3d_flex_stats *stats);
 /* Mean device seconds of `reps` flexible solves from g->q->q (not updated). */
 double kfun3d_time_solve_flexible(GEOMETRY *g, const kfun3d_solver_params *p, kfun3d_mpnn *net, int reps,
                                   kfun3d_step *hist, int max_hist, int *nsteps, kfun3d_flex_stats *stats);
+
+/* Milliseconds of one application of the learned preconditioner's network
+ * (features, encoder, three message-passing layers, decoder) on g's device
+ * mirror, averaged over reps. */
+double kfun3d_time_learned_apply(GEOMETRY *g, kfun3d_mpnn *net, int reps);
 
 /* Test hook: Y = X Wt^T, one BF16 tensor-core tile per 128 rows. */
 int kfun3d_umma_selftest(const void *X, const void *Wt, float *Y, int rows, int K, int N);

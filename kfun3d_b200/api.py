@@ -119,6 +119,7 @@ def lib():
                                             C.c_void_p]),
         "kfun3d_mpnn_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "kfun3d_umma_selftest": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
+        "kfun3d_time_learned_apply": (C.c_double, [G, C.c_void_p, C.c_int]),
         "kfun3d_solve_flexible": (C.c_int, [G, P(SolverParams), C.c_void_p, P(Step), C.c_int, P(FlexStats)]),
         "kfun3d_collect_pairs": (C.c_int, [G, P(SolverParams), C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                            P(FlexStats)]),
@@ -363,6 +364,13 @@ class Mesh:
         if t < 0:
             raise RuntimeError(f"kfun3d_time_solve_flexible failed: {last_error()}")
         return t, _hist(hist, ns.value), st.as_dict()
+
+    def time_learned_apply(self, net, reps=10):
+        """Milliseconds of one application of the network on this mesh."""
+        ms = lib().kfun3d_time_learned_apply(self.g, net.h, int(reps))
+        if ms < 0:
+            raise RuntimeError(f"kfun3d_time_learned_apply failed: {last_error()}")
+        return ms
 
     def collect_pairs(self, stride=5, cap=64, **params):
         """Training pairs of the ILU(0)-FGMRES solve from the current state

@@ -21,7 +21,7 @@ namespace {
 
 constexpr double JV_EPS = 1.490116119384766e-08;   // src/kernel.c:12
 constexpr int RED_BLOCKS = 296;                    // 2 x 148 SMs
-constexpr int S_XN = 40, S_H = 41, S_QN = 42, S_FN = 43, S_T0 = 44;
+constexpr int S_XN = 40, S_H = 41, S_QN = 42, S_FN = 43, S_T0 = 44, S_CMP = 52;
 
 inline unsigned nblk(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
@@ -803,22 +803,21 @@ void write_pair(DevMesh &m, const Ops &o, int prec, const double *x, PairSink &p
 }  // namespace
 
 // The pseudo-transient Newton loop of src/kernel.c:47-232 with its linear
-// solves done by FGMRES(restart) -- right preconditioning, a preconditioner
-// allowed to change from one iteration to the next:
-//   z_k = M_k(v_k),  w = J z_k orthogonalised against v_0..v_k,
-//   x = Z y after each cycle, the true residual b - J x at a restart.
-// M_k is ILU(0)^-1, or with a network the network's correction of it.  A
-// linear solve stops once the true residual |b - J x| has fallen by
-// gmres_rtol (within a cycle), or -- checked at every restart -- the
-// ILU(0)-preconditioned residual has, which is the reference's own measure
-// (right preconditioning alone can stall on the true residual where the
-// reference's left-preconditioned GMRES converges).  The
-// network is a guest: Newton step 0 runs on ILU(0) alone to measure its
-// convergence rate; a linear solve whose residual falls at less than half
-// that rate after 4 iterations continues on ILU(0) alone; two steps in a row
-// that need more iterations than the last ILU(0)-only solve switch the
-// network off for good; and an update after which the FP64 nonlinear
-// residual is non-finite or grows tenfold is undone and redone on ILU(0).
+// solves done by flexible GMRES on the reference's left-preconditioned
+// system: Arnoldi on ILU(0)^-1 J, residual measured as |ILU(0)^-1 (b - J x)|
+// exactly as the reference does, and a right preconditioner allowed to
+// change from one iteration to the next,
+//   z_k = N_k(v_k),  w = ILU(0)^-1 J z_k orthogonalised against v_0..v_k,
+//   x = Z y after each cycle.
+// N_k is the identity -- the reference's GMRES, iteration for iteration -- or
+// the network's correction v + s N([v/s, q]), which maps an ILU(0)-
+// preconditioned residual to an approximation of the correction x with
+// ILU(0)^-1 J x = v.  The network is a guest: each linear solve starts with
+// both candidate first directions and keeps the network only if its image
+// under ILU(0)^-1 J lies closer to v0 (one extra product per Newton step);
+// three refusals in a row switch it off for good; and an update after which
+// the FP64 nonlinear residual is non-finite or grows tenfold is undone and
+// redone without it.
 static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_params *p, kfun3d_mpnn *net,
                           PairSink *ps, kfun3d_step *hist, int max_hist, kfun3d_flex_stats *st)
 {
@@ -839,9 +838,9 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
   }
   double ghh[KF_NBASIS * (KF_NBASIS + 1)] = {0};
   double cs[KF_NBASIS], sn[KF_NBASIS], rs[KF_NBASIS], yk[KF_NBASIS];
-  double fnorm0 = 0.0, fnorm_prev = 0.0, cfl = p->cfl_init, rate_ilu = 0.0;
+  double fnorm0 = 0.0, fnorm_prev = 0.0, cfl = p->cfl_init;
   bool use_net = net != nullptr, last_used_net = false;
-  int strikes = 0, plain_its_last = -1;
+  int misses = 0;
   int nrec = 0, steps = 0;
   cudaEvent_t ev0, ev1, es0, es1;
   CK(cudaEventCreate(&ev0));
@@ -883,7 +882,7 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
     dev_reduce(m, m.q, m.q, m.scal + S_QN, 2, o.fast);
     CK(cudaMemsetAsync(m.x, 0, n * sizeof(double), m.stream));
     o.ilu(m, prec);
-    CK(cudaMemcpyAsync(Vb(m, 0), m.r, n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+    o.sptrsv(m, m.r, Vb(m, 0), prec);                            // src/kernel.c:103
     {
       const int sd = device_status(m);
       if (sd == KFUN3D_ERR_PIVOT) {
@@ -892,78 +891,101 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
         break;
       }
     }
-    bool step_net = use_net && its > 0;
-    const bool step_net0 = step_net;
-    double tol = 0.0, beta0 = 0.0, res = 0.0, pres0 = 0.0;
+    bool step_net = use_net;
+    bool usez[KF_NBASIS] = {false};
+    double tol = 0.0;
     unsigned int total = 0;
     bool done = false, failed = false;
-    // the reference's own measure, |ILU(0)^-1 (b - J x)|, at every restart
-    o.sptrsv(m, m.r, m.fy, prec);
-    dev_reduce(m, m.fy, m.fy, m.scal + S_T0 + 1, 1, o.fast);
-    fetch(m, S_T0 + 1, 1);
-    pres0 = m.h_scal[S_T0 + 1];
-    for (int cycle = 0; total <= (unsigned)p->gmres_max_it; cycle++) {
-      if (total > 0) {   // true residual of the current iterate
+    for (int cycle = 0; total <= (unsigned)p->gmres_max_it; cycle++) {   // src/kernel.c:107-196
+      if (total > 0) {
         dev_jacvec(m, o, m.x, m.t);
-        k_waxpy<<<nblk(n, 256), 256, 0, m.stream>>>(n, -1.0, m.t, m.r, Vb(m, 0), o.fast);
+        k_waxpy<<<nblk(n, 256), 256, 0, m.stream>>>(n, -1.0, m.t, m.r, m.w, o.fast);
         kf_count_launch();
-        o.sptrsv(m, Vb(m, 0), m.fy, prec);
-        dev_reduce(m, m.fy, m.fy, m.scal + S_T0 + 1, 1, o.fast);
-        fetch(m, S_T0 + 1, 1);
-        if (m.h_scal[S_T0 + 1] <= p->gmres_rtol * pres0) { done = true; break; }
+        o.sptrsv(m, m.w, Vb(m, 0), prec);
       }
       dev_normalize(m, Vb(m, 0), m.scal + S_T0, o.fast);
       fetch(m, S_T0, 1);
       rs[0] = m.h_scal[S_T0];
       if (!std::isfinite(rs[0])) { failed = true; break; }
       if (total == 0) {
-        beta0 = rs[0];
-        tol = p->gmres_rtol * beta0;
-        res = beta0;
-        if (beta0 == 0.0) { done = true; break; }
+        tol = p->gmres_rtol * rs[0];
+        if (rs[0] == 0.0) { done = true; break; }
       }
-      const double beta_c = rs[0];
       int k = 0;
       while (k < restart) {
-        if (step_net) {
-          o.sptrsv(m, Vb(m, k), m.fy, prec);
-          if (kf_mpnn_apply_async(net, m.mgraph, m.fy, m.q, Zb(m, k), m.stream) != KFUN3D_OK) { failed = true; break; }
+        if (step_net && cycle == 0 && k == 0) {
+          // the network earns this solve on its first direction: both
+          // candidates, z = v0 and the network's z, are mapped by
+          // ILU(0)^-1 J; the one whose image comes closer to v0
+          // (1 - (v0.w)^2 / w.w, the least-squares residual along w) is kept
+          if (kf_mpnn_apply_async(net, m.mgraph, Vb(m, 0), m.q, Zb(m, 0), m.stream) != KFUN3D_OK) {
+            failed = true;
+            break;
+          }
+          dev_jacvec(m, o, Zb(m, 0), m.t);
+          o.sptrsv(m, m.t, Vb(m, 1), prec);
+          dev_jacvec(m, o, Vb(m, 0), m.t);
+          o.sptrsv(m, m.t, m.fy, prec);
+          dev_reduce(m, Vb(m, 0), Vb(m, 1), m.scal + S_CMP, 0, o.fast);
+          dev_reduce(m, Vb(m, 1), Vb(m, 1), m.scal + S_CMP + 1, 0, o.fast);
+          dev_reduce(m, Vb(m, 0), m.fy, m.scal + S_CMP + 2, 0, o.fast);
+          dev_reduce(m, m.fy, m.fy, m.scal + S_CMP + 3, 0, o.fast);
+          fetch(m, S_CMP, 4);
+          const double *c = m.h_scal + S_CMP;
+          const double rho_net = 1.0 - c[0] * c[0] / c[1], rho_plain = 1.0 - c[2] * c[2] / c[3];
+          if (!(rho_net < rho_plain)) {
+            CK(cudaMemcpyAsync(Vb(m, 1), m.fy, n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+            step_net = false;
+            usez[0] = false;
+            S.fallback_solves++;
+            if (++misses >= 3) {   // three solves in a row: off for the rest of the solve
+              use_net = false;
+              S.disabled = 1;
+            }
+          } else {
+            misses = 0;
+            usez[0] = true;
+            S.learned_its++;
+          }
+        } else if (step_net) {
+          if (kf_mpnn_apply_async(net, m.mgraph, Vb(m, k), m.q, Zb(m, k), m.stream) != KFUN3D_OK) {
+            failed = true;
+            break;
+          }
+          dev_jacvec(m, o, Zb(m, k), m.t);
+          o.sptrsv(m, m.t, Vb(m, k + 1), prec);
+          usez[k] = true;
           S.learned_its++;
         } else {
-          o.sptrsv(m, Vb(m, k), Zb(m, k), prec);
-        }
-        dev_jacvec(m, o, Zb(m, k), Vb(m, k + 1));
-        if (ps && ps->stride < 0 && (k % -ps->stride) == 0 && ps->count < ps->cap) {
-          // basis pair: w = J z_k (not yet orthogonalised), y = ILU(0)^-1 w, target from z_k
-          o.sptrsv(m, Vb(m, k + 1), m.fy, prec);
-          kf_mpnn_pair_async(m.N, m.fy, m.q, Zb(m, k), ps->x0 + (size_t)ps->count * 16 * m.N,
-                             ps->tgt + (size_t)ps->count * 4 * m.N, m.pscr, m.stream);
-          ps->count++;
+          dev_jacvec(m, o, Vb(m, k), m.t);                             // src/kernel.c:123-130
+          o.sptrsv(m, m.t, Vb(m, k + 1), prec);
+          usez[k] = false;
+          if (ps && ps->stride < 0 && (k % -ps->stride) == 0 && ps->count < ps->cap) {
+            // basis pair: x = v_k, y = ILU(0)^-1 J v_k (before Gram-Schmidt)
+            kf_mpnn_pair_async(m.N, Vb(m, k + 1), m.q, Vb(m, k), ps->x0 + (size_t)ps->count * 16 * m.N,
+                               ps->tgt + (size_t)ps->count * 4 * m.N, m.pscr, m.stream);
+            ps->count++;
+          }
         }
         orthogonalize(m, o, k);
         fetch(m, 0, k + 2);
         double *hh = ghh + k * (KF_NBASIS + 1);
         for (int i = 0; i <= k + 1; i++) hh[i] = m.h_scal[i];
-        res = givens(hh, cs, sn, rs, k);
+        const double res = givens(hh, cs, sn, rs, k);
         k++;
         if (res <= tol) { done = true; break; }
         if (!std::isfinite(res)) { failed = true; break; }
-        if (step_net && k >= 4 && rate_ilu < 0.0 && log(res / beta_c) > 0.5 * k * rate_ilu) {
-          step_net = false;   // the network is not pulling its weight in this solve
-          S.fallback_solves++;
-        }
-        if (ps && ps->stride > 0 && cycle == 0 && k < restart && !done && (k % ps->stride) == 0 &&
-            ps->count < ps->cap) {
+        if (ps && ps->stride > 0 && cycle == 0 && k < restart && (k % ps->stride) == 0 && ps->count < ps->cap) {
           back_substitute(ghh, rs, k, yk);
           CK(cudaMemsetAsync(m.fx, 0, n * sizeof(double), m.stream));
-          for (int vv = 0; vv < k; vv++) dev_axpy(m, yk[vv], Zb(m, vv), m.fx, o.fast);
+          for (int vv = 0; vv < k; vv++) dev_axpy(m, yk[vv], Vb(m, vv), m.fx, o.fast);
           write_pair(m, o, prec, m.fx, *ps);
         }
       }
       if (failed || k == 0) break;
       total += k;
-      back_substitute(ghh, rs, k, yk);
-      for (int vv = 0; vv < k; vv++) dev_axpy(m, yk[vv], Zb(m, vv), m.x, o.fast);
+      back_substitute(ghh, rs, k, yk);                                  // src/kernel.c:178-190
+      for (int vv = 0; vv < k; vv++) dev_axpy(m, yk[vv], usez[vv] ? Zb(m, vv) : Vb(m, vv), m.x, o.fast);
       if (done) break;
     }
     if (failed || !done) {
@@ -977,20 +999,9 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
     }
     if (net && kf_mpnn_status(net, m.stream) != KFUN3D_OK) { steps = -1; break; }
     S.gmres_its += (int)total;
-    if (!step_net0) {
-      plain_its_last = (int)total;
-      if (total > 0 && res > 0.0 && beta0 > 0.0) rate_ilu = log(res / beta0) / total;
-    } else if (plain_its_last >= 0 && (int)total > plain_its_last) {
-      if (++strikes >= 2) {
-        use_net = false;
-        S.disabled = 1;
-      }
-    } else {
-      strikes = 0;
-    }
     if (ps && ps->count < ps->cap) write_pair(m, o, prec, m.x, *ps);
-    if (step_net0) CK(cudaMemcpyAsync(m.qold, m.q, n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
-    last_used_net = step_net0;
+    if (step_net) CK(cudaMemcpyAsync(m.qold, m.q, n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
+    last_used_net = step_net;
     dev_axpy(m, -1.0, m.x, m.q, o.fast);                           // src/kernel.c:200
     k_forces<<<1, forces_threads(m.ncol), 0, m.stream>>>(m.ncol, m.col, m.wf_nodes, m.xyz, (const double4 *)m.q, u, v,
                                                          m.forces);
@@ -1458,4 +1469,31 @@ extern "C" double kfun3d_time_solve_flexible(GEOMETRY *g, const kfun3d_solver_pa
   if (nsteps) *nsteps = ns;
   if (!finish(*m, "kfun3d_time_solve_flexible") || ns < 0) return -1.0;
   return total / reps;
+}
+
+extern "C" double kfun3d_time_learned_apply(GEOMETRY *g, kfun3d_mpnn *net, int reps)
+{
+  DevMesh *m = dev_or_fail(g);
+  if (!m || !net || reps < 1) return -1.0;
+  if (!ensure_flex(*m)) return -1.0;
+  if (!m->mgraph) m->mgraph = kfun3d_mpnn_graph_create(g);
+  if (!m->mgraph || kf_mpnn_prepare(net, m->mgraph) != KFUN3D_OK) return -1.0;
+  const Ops o = ops();
+  const size_t n = 4 * (size_t)m->N;
+  h2d(*m, m->q, g->q->q, n);
+  dev_residual(*m, o, m->q, m->fy);   // a residual-like input
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  kf_mpnn_apply_async(net, m->mgraph, m->fy, m->q, m->t, m->stream);   // warm-up
+  CK(cudaEventRecord(e0, m->stream));
+  for (int r = 0; r < reps; r++) kf_mpnn_apply_async(net, m->mgraph, m->fy, m->q, m->t, m->stream);
+  CK(cudaEventRecord(e1, m->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (kf_mpnn_status(net, m->stream) != KFUN3D_OK || !finish(*m, "kfun3d_time_learned_apply")) return -1.0;
+  return ms / reps;
 }

@@ -1,7 +1,7 @@
 """Flexible GMRES and the learned right preconditioner on the GPU.
 
-* ILU(0)-FGMRES reaches the same converged state as the reference's
-  left-preconditioned GMRES (wall forces at a 1e-8 residual drop);
+* without a network the flexible solve repeats the reference's
+  left-preconditioned GMRES step for step;
 * a network that makes things worse is caught by the fallback and the solve
   still converges to the same state (the FP64 nonlinear residual is the judge);
 * the pair writer fills the requested slots with finite data;
@@ -31,7 +31,7 @@ def _fast():
     kf.set_aoa(3.06)
 
 
-def test_ilu_fgmres_reaches_the_plain_solution(box_mesh):
+def test_flexible_without_network_is_the_plain_solve(box_mesh):
     m = kf.Mesh(box_mesh(14, seed=21))
     q0 = m.view.q.copy()
     h = m.solve(**P)
@@ -39,8 +39,9 @@ def test_ilu_fgmres_reaches_the_plain_solution(box_mesh):
     hf, st = m.solve_flexible(**P)
     assert h[0]["fnorm"] / h[-1]["fnorm"] >= 1e7 and hf[0]["fnorm"] / hf[-1]["fnorm"] >= 1e7
     assert st["learned_its"] == 0 and st["gmres_its"] == sum(s["gmres_its"] for s in hf)
-    # both stop at a 1e-8 drop: the states agree to that level
-    assert np.allclose(_forces(hf), _forces(h), rtol=1e-6, atol=0)
+    # without a network the flexible solve is the reference's GMRES, step for step
+    assert [s["gmres_its"] for s in hf] == [s["gmres_its"] for s in h]
+    assert np.allclose(_forces(hf), _forces(h), rtol=1e-12, atol=0)
 
 
 def test_bad_network_falls_back_to_ilu(box_mesh):
@@ -55,8 +56,8 @@ def test_bad_network_falls_back_to_ilu(box_mesh):
     net.set_params(th)
     m.view.q[:] = q0
     h, st = m.solve_flexible(net=net, **P)
-    assert st["learned_its"] > 0
-    assert st["fallback_solves"] + st["rejected_steps"] + st["disabled"] > 0, st
+    # the network loses the first direction of every solve: ILU(0) alone, then switched off
+    assert st["fallback_solves"] >= 3 and st["disabled"] == 1, st
     assert h[0]["fnorm"] / h[-1]["fnorm"] >= 1e7
     assert np.allclose(_forces(h), _forces(h_ilu), rtol=1e-6, atol=0)
 
