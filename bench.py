@@ -1,18 +1,25 @@
 #!/usr/bin/env python
 """One-line benchmark of the kfun3d_b200 hot path (pseudo-transient Newton-Krylov).
 
-Workload (N = 1): the config-1 solve — the 70^3 seeded Kuhn-box mesh (343,000
-nodes, 2,342,619 edges, bump 0.1, jitter 0.2h, random numbering), AoA 3.06,
-second-order residual, FP64 ILU(0)-GMRES(30), SER CFL from 50, at most 20
-Newton steps, stopped at a 1e-8 drop of the residual norm.  A step is one such
-solve from the free-stream state.  The metric is BASELINE.json's: seconds to
-the 1e-8 drop (lower is better), with flux edges/s and the other kernel
-throughputs reported beside it.
+Workload (N = 1): the config-4 comparison -- the 120^3 seeded Kuhn-box mesh
+(1,728,000 nodes, 11,923,919 edges, bump 0.12, angle of attack 4.5, both
+held out of the network's training set, jitter 0.2h, random numbering),
+second-order residual, SER CFL from 50, at most 20 Newton steps, stopped at a
+1e-8 drop of the residual norm.  A step is one solve from the free-stream
+state in the mixed-precision + learned form (FP32 Jacobian blocks, ILU(0) and
+triangular solves; FP64 residual, norms, CFL, Gram-Schmidt and Givens;
+flexible GMRES(30) with the trained network as right preconditioner and its
+fallback).  `comparison` holds, on the same mesh, the plain FP64 solve (the
+reference's method), the same mixed solve without the network, and the wall
+forces' relative error against FP64.  The metric is seconds to the 1e-8 drop
+(lower is better), with flux edges/s and the other kernel throughputs beside
+it.  --config 1 runs the 70^3 plain FP64 solve instead.
 
 value    device-resident: state and mesh already in HBM, CUDA events on the
          solver's stream around each solve, max over ranks.
-e2e      the same solve through the C ABI with host buffers (kfun3d_solve:
-         state uploaded, solved, state and time step downloaded), wall clock.
+e2e      the same solve through the C ABI with host buffers
+         (kfun3d_solve_flexible / kfun3d_solve: state uploaded, solved, state
+         and time step downloaded), wall clock.
 roofline the kernel family with the largest share of one GMRES iteration,
          algorithmic bytes (per-kernel formulas below) / its CUDA-event time,
          against MEASURED_PEAKS.json's HBM copy bandwidth.
@@ -43,17 +50,17 @@ CONFIGS = {
             ts_max=20, stop_ratio=1e30),
     1: dict(workload="config1: 70^3 Kuhn box, second-order flux, plain FP64, solve to 1e-8 drop",
             n=70, seed=1, bump=0.1, aoa=3.06, precision=0, mode="fast", first_order=False,
-            ts_max=20, stop_ratio=1e8),
+            ts_max=20, stop_ratio=1e8, ref_total_its=741),
     2: dict(workload="config2: 70^3 Kuhn box, FP32 Jacobian/ILU(0)/SpTRSV, FP64 residual and GMRES, to 1e-8 drop",
             n=70, seed=1, bump=0.1, aoa=3.06, precision=1, mode="fast", first_order=False,
             ts_max=20, stop_ratio=1e8),
     4: dict(workload="config4: 120^3 Kuhn box (bump 0.12, AoA 4.5, held out of training), mixed precision + "
                      "learned FGMRES against plain FP64, to 1e-8 drop",
             n=120, seed=4, bump=0.12, aoa=4.5, precision=1, mode="fast", first_order=False,
-            ts_max=20, stop_ratio=1e8, learned=True, ref_ts=1),
+            ts_max=20, stop_ratio=1e8, learned=True, ref_ts=1, ref_total_its=1556),
 }
 WEIGHTS = os.path.join(ROOT, "kfun3d_b200", "weights", "mpnn_box40.npy")
-DEFAULT_CONFIG = 1
+DEFAULT_CONFIG = 4
 
 
 def log(*a):
@@ -244,7 +251,7 @@ def run_reference_arm(args, cfg):
     import kfun3d_b200 as kf
     path = mesh_path(cfg)
     threads = host_cores()
-    total_its = args.ref_total_its
+    total_its = args.ref_total_its or cfg.get("ref_total_its", 741)
     # Warm-up: one untimed ComputeFlux pass per requested warm-up step (page-in
     # of the mesh and OpenMP thread start); each timed step is a full sample.
     if args.warmup:
@@ -444,8 +451,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-total-its", type=int, default=741,
-                    help="GMRES iterations of the full solve used to extrapolate the reference sample")
+    ap.add_argument("--ref-total-its", type=int, default=None,
+                    help="GMRES iterations of the full solve used to extrapolate the reference sample "
+                         "(default: the plain FP64 solve's count for the workload)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     if args.impl == "reference":

@@ -280,7 +280,7 @@ typedef struct {
   int newton_steps;     /* Newton steps taken */
   int gmres_its;        /* FGMRES iterations over the solve */
   int learned_its;      /* iterations preconditioned by the network */
-  int fallback_solves;  /* linear solves run without the network: it lost the first direction */
+  int fallback_solves;  /* linear solves run (or finished) without the network */
   int rejected_steps;   /* updates undone because the nonlinear residual grew tenfold */
   int disabled;         /* 1: the network was switched off for the rest of the solve */
   int pairs;            /* training pairs written (kfun3d_collect_pairs) */
@@ -294,7 +294,9 @@ typedef struct {
  * GMRES, iteration for iteration) or the network's correction
  * v + s N([v/s, q]).  The network falls back to the identity: for a linear
  * solve whose first direction it does not improve (its image under
- * ILU(0)^-1 J farther from v0), for good after three such solves in a row,
+ * ILU(0)^-1 J farther from v0), for the rest of a solve that has used 1.5x
+ * the previous Newton step's iterations, for good after three such
+ * fallbacks in a row,
  * and for an update after which the FP64 nonlinear residual grows tenfold
  * (the update is undone).  Solves from g->q->q and updates it; returns the
  * number of history entries or -1. */

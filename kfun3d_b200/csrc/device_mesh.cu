@@ -245,7 +245,7 @@ static void release_device(MatrixHandle *h)
                   m->wf_n, m->s_n, m->f_n, m->bnd_of, m->bnd_node, m->bnd_ptr, m->bnd_ent, m->ia, m->ja,
                   m->diag, m->tblk, m->lpos, m->last_lower, m->lev_l, m->lev_u, m->A, m->lslot, m->dinv,
                   m->Af, m->dinvf, m->q, m->r, m->gx, m->gy, m->gz, m->cdt, m->w, m->t, m->x, m->rhs, m->V,
-                  m->red, m->scal, m->forces, m->dscr, m->status, m->flags, m->ticket, m->part, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->s0, m->pair_ptr, m->pairs, m->lev_ptr_d, m->bar, m->Z, m->qold, m->fy, m->fx, m->pscr};
+                  m->red, m->scal, m->forces, m->dscr, m->status, m->flags, m->ticket, m->part, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->s0, m->pair_ptr, m->pairs, m->lev_ptr_d, m->bar, m->Z, m->qold, m->fy, m->fx, m->pscr, m->ord, m->rowof, m->egeo_s};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (m->h_scal) cudaFreeHost(m->h_scal);
@@ -315,16 +315,67 @@ DevMesh *kf_device(const GEOMETRY *g)
     KF_CUDA(upload(&m->egeo, eg.data(), E));
     KF_CUDA(upload(&m->xyz, xyz.data(), N));
   }
-  // node incidence in edge order, with the least-squares terms seen from the
-  // node (w0 at n0, w1 at n1) and the block of (node, other)
+  // Order in which the node-centric kernels visit nodes: on meshes whose node
+  // data (state, gradients, coordinates: 160 B a node) outgrows what L2 keeps
+  // (from 500,000 nodes), Morton (Z-order) of the coordinates, so that a
+  // warp's nodes and their neighbours are close in space and the gathers hit
+  // in L2 even when the mesh's own numbering is random; below, the mesh's own
+  // order.  A node's sums still run over its edges in edge order, so results
+  // do not depend on this order.  KFUN3D_NODE_ORDER=natural|morton overrides.
+  std::vector<uint32_t> ord(N);
+  for (uint32_t i = 0; i < N; i++) ord[i] = i;
   {
-    std::vector<uint32_t> ptr(N + 1, 0);
-    for (uint32_t e = 0; e < E; e++) { ptr[n0[e] + 1]++; ptr[n1[e] + 1]++; }
-    for (uint32_t i = 0; i < N; i++) ptr[i + 1] += ptr[i];
+    const char *env = getenv("KFUN3D_NODE_ORDER");
+    bool morton = N >= 500000u;
+    if (env && strcmp(env, "natural") == 0) morton = false;
+    if (env && strcmp(env, "morton") == 0) morton = true;
+    if (morton && N > 0) {
+      const double *X = g->n->xyz->x0, *Y = g->n->xyz->x1, *Z = g->n->xyz->x2;
+      double lo[3] = {X[0], Y[0], Z[0]}, hi[3] = {X[0], Y[0], Z[0]};
+      for (uint32_t i = 0; i < N; i++) {
+        const double c[3] = {X[i], Y[i], Z[i]};
+        for (int d = 0; d < 3; d++) { lo[d] = std::min(lo[d], c[d]); hi[d] = std::max(hi[d], c[d]); }
+      }
+      auto spread = [](uint64_t v) {   // 21 bits -> every third bit
+        v &= 0x1fffffull;
+        v = (v | v << 32) & 0x1f00000000ffffull;
+        v = (v | v << 16) & 0x1f0000ff0000ffull;
+        v = (v | v << 8) & 0x100f00f00f00f00full;
+        v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+        v = (v | v << 2) & 0x1249249249249249ull;
+        return v;
+      };
+      std::vector<uint64_t> key(N);
+      for (uint32_t i = 0; i < N; i++) {
+        const double c[3] = {X[i], Y[i], Z[i]};
+        uint64_t k = 0;
+        for (int d = 0; d < 3; d++) {
+          const double span = hi[d] > lo[d] ? hi[d] - lo[d] : 1.0;
+          const uint64_t b = (uint64_t)std::min(2097151.0, std::max(0.0, (c[d] - lo[d]) / span * 2097151.0));
+          k |= spread(b) << d;
+        }
+        key[i] = k;
+      }
+      std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+    }
+    KF_CUDA(upload(&m->ord, ord.data(), N));
+  }
+  // node incidence in edge order, with the least-squares terms seen from the
+  // node (w0 at n0, w1 at n1) and the block of (node, other); row p of the
+  // CSR belongs to node ord[p]
+  {
+    std::vector<uint32_t> deg(N, 0), ptr(N + 1, 0), rowof(N);
+    for (uint32_t e = 0; e < E; e++) { deg[n0[e]]++; deg[n1[e]]++; }
+    for (uint32_t p2 = 0; p2 < N; p2++) {
+      ptr[p2 + 1] = ptr[p2] + deg[ord[p2]];
+      rowof[ord[p2]] = p2;
+    }
+    KF_CUDA(upload(&m->rowof, rowof.data(), N));
     const size_t ninc = 2 * (size_t)E;
     const size_t wst = (ninc + 3) & ~(size_t)3;   // rows of inc_w start on 16 bytes
     m->wstride = (uint32_t)wst;
-    std::vector<uint32_t> oth(wst + 4, 0), edg(ninc), blk(ninc), pos(ptr.begin(), ptr.end() - 1);
+    std::vector<uint32_t> oth(wst + 4, 0), edg(ninc), blk(ninc), pos(N);
+    for (uint32_t i = 0; i < N; i++) pos[i] = ptr[rowof[i]];
     std::vector<double> w(3 * wst + 4, 0.0);
     const double *w0[3] = {g->e->w->w0->x0, g->e->w->w0->x1, g->e->w->w0->x2};
     const double *w1[3] = {g->e->w->w1->x0, g->e->w->w1->x1, g->e->w->w1->x2};
@@ -367,13 +418,32 @@ DevMesh *kf_device(const GEOMETRY *g)
     const char *env = getenv("KFUN3D_RESIDUAL");
     m->two_pass = ok && !(env && strcmp(env, "gather") == 0);
     if (m->two_pass) {
-      std::vector<uint32_t> eoff(N + 1, 0), iptr(N + 1, 0), iedge(E);
-      for (uint32_t e = 0; e < E; e++) { eoff[n0[e] + 1]++; iptr[n1[e] + 1]++; }
-      for (uint32_t i = 0; i < N; i++) { eoff[i + 1] += eoff[i]; iptr[i + 1] += iptr[i]; }
-      std::vector<uint32_t> pos(iptr.begin(), iptr.end() - 1);
-      for (uint32_t e = 0; e < E; e++) iedge[pos[n1[e]]++] = e;
+      // reference ranges of the edges with n0 = node (contiguous, edges sorted by n0)
+      std::vector<uint32_t> r0(N + 1, 0), c1(N, 0);
+      for (uint32_t e = 0; e < E; e++) { r0[n0[e] + 1]++; c1[n1[e]]++; }
+      for (uint32_t i = 0; i < N; i++) r0[i + 1] += r0[i];
+      // storage: groups by n0 in visit order, each in edge order
+      std::vector<uint32_t> eoff(N + 1, 0), spos(E), n1s(E), iptr(N + 1, 0), iedge(E);
+      std::vector<double4> egs(E);
+      uint32_t next = 0;
+      for (uint32_t p2 = 0; p2 < N; p2++) {
+        const uint32_t nd = ord[p2];
+        eoff[p2] = next;
+        for (uint32_t e = r0[nd]; e < r0[nd + 1]; e++) {
+          spos[e] = next;
+          n1s[next] = n1[e];
+          egs[next] = make_double4(g->e->xyzn->x0[e], g->e->xyzn->x1[e], g->e->xyzn->x2[e], g->e->xyzn->x3[e]);
+          next++;
+        }
+        iptr[p2 + 1] = iptr[p2] + c1[nd];
+      }
+      eoff[N] = next;
+      std::vector<uint32_t> ipos(N);
+      for (uint32_t p2 = 0; p2 < N; p2++) ipos[ord[p2]] = iptr[p2];
+      for (uint32_t e = 0; e < E; e++) iedge[ipos[n1[e]]++] = spos[e];
       KF_CUDA(upload(&m->eoff, eoff.data(), N + 1));
-      KF_CUDA(upload(&m->n1, n1, E));
+      KF_CUDA(upload(&m->n1, n1s.data(), E));
+      KF_CUDA(upload(&m->egeo_s, egs.data(), E));
       KF_CUDA(upload(&m->in1_ptr, iptr.data(), N + 1));
       KF_CUDA(upload(&m->in1_edge, iedge.data(), E));
       KF_CUDA(cudaMalloc(&m->eres, std::max<size_t>(E, 1) * sizeof(double4)));
@@ -483,8 +553,11 @@ DevMesh *kf_device(const GEOMETRY *g)
     // cooperative grid: 4 blocks of 256 threads per SM (the kernel's launch
     // bounds guarantee they fit); the runtime refuses the launch otherwise
     m->trsv_grid = (unsigned)nsm * 4;
-    // one 512-thread CTA per SM (launch bounds (512, 1))
-    m->trsv_mgrid = (unsigned)nsm;
+    // mode 5: 1-3 CTAs of 512 threads per SM (the kernel's launch bounds
+    // guarantee they fit); KFUN3D_SPTRSV_CTAS picks the count
+    const char *cenv = getenv("KFUN3D_SPTRSV_CTAS");
+    if (cenv && (atoi(cenv) >= 1 && atoi(cenv) <= 3)) m->trsv_mgrid_per = atoi(cenv);
+    m->trsv_mgrid = (unsigned)nsm * (unsigned)m->trsv_mgrid_per;
     std::vector<uint4> dl(N), du(N);
     for (uint32_t s = 0; s < N; s++) {
       const uint32_t i = p.lev_l[s];
@@ -500,7 +573,10 @@ DevMesh *kf_device(const GEOMETRY *g)
     // barrier between levels), "syncfree" (per-row flags, no level barriers)
     // or "levels" (one launch per level, 4 lanes per row)
     const char *env = getenv("KFUN3D_SPTRSV");
-    m->trsv_mode = 4;
+    // default: the persistent sweep (2 CTAs per SM) on large meshes, where
+    // it is the faster one, levels with programmatic dependent launch below
+    m->trsv_mode = N >= 1000000u ? 5 : 4;
+    if (env && strcmp(env, "pdl") == 0) m->trsv_mode = 4;
     if (env && strcmp(env, "levels16") == 0) m->trsv_mode = 2;
     if (env && strcmp(env, "persistent") == 0) m->trsv_mode = 3;
     if (env && strcmp(env, "syncfree") == 0) m->trsv_mode = 1;

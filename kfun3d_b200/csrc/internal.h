@@ -96,21 +96,25 @@ struct DevMesh {
   // static geometry
   double4 *egeo = nullptr;        // [E] unit normal n0->n1, area
   double4 *xyz = nullptr;         // [N] coordinates, w = 0
-  uint32_t *inc_ptr = nullptr;    // [N+1] incident edges of each node, in edge order
+  uint32_t *ord = nullptr;        // [N] node visited at position p by the node-centric gathers
+  uint32_t *rowof = nullptr;      // [N] position (CSR row) of each node
+  uint32_t *inc_ptr = nullptr;    // [N+1] incident edges of node ord[p] (row p), in edge order
   uint32_t *inc_oth = nullptr;    // [2E] the other end point
   uint32_t *inc_edge = nullptr;   // [2E] edge index | (1u<<31 when the node is n1)
   uint32_t *inc_blk = nullptr;    // [2E] block index of (node, other)
   double *inc_w = nullptr;        // [3][wstride] least-squares terms seen from the node
   uint32_t wstride = 0;           // 2E rounded up to a multiple of 4 (16-byte aligned rows)
   unsigned grad_smem = 0;         // dynamic shared memory of k_gradient_tma (0: not used)
-  // two-pass residual (every edge has n0 < n1)
+  // two-pass residual (every edge has n0 < n1); edge arrays in storage
+  // order: grouped by n0 in node-visit order (ord), each group in edge order
   bool two_pass = false;
-  uint32_t *eoff = nullptr;       // [N+1] edges with n0 = node (contiguous: edges are sorted by n0)
-  uint32_t *n1 = nullptr;         // [E]
-  uint32_t *in1_ptr = nullptr;    // [N+1] edges with n1 = node, in edge order
-  uint32_t *in1_edge = nullptr;   // [E]
-  double4 *eres = nullptr;        // [E] edge fluxes
-  double4 *s0 = nullptr;          // [N] n0-side sums (fast build)
+  uint32_t *eoff = nullptr;       // [N+1] storage range of the edges with n0 = ord[p]
+  uint32_t *n1 = nullptr;         // [E] far end (n1) of each stored edge
+  double4 *egeo_s = nullptr;      // [E] edge geometry in storage order
+  uint32_t *in1_ptr = nullptr;    // [N+1] edges with n1 = ord[p], in edge order
+  uint32_t *in1_edge = nullptr;   // [E] their storage positions
+  double4 *eres = nullptr;        // [E] edge fluxes, storage order
+  double4 *s0 = nullptr;          // [N] n0-side sums by position (fast build)
   uint32_t *wf_nodes = nullptr;   // [3F] wall faces in colour order
   double *wf_n = nullptr;         // [3F] wall-face normals -(1/6) a x b
   uint32_t *col = nullptr;        // [ncol+1] wall-face colour offsets
@@ -148,7 +152,7 @@ struct DevMesh {
   int trsv_mode = 4;               // 0 levels (4 lanes/row), 1 sync-free, 2 levels (16 lanes/row),
                                    // 3 one persistent launch, grid barrier between levels,
                                    // 4 levels with programmatic dependent launch,
-                                   // 5 one persistent launch, one CTA per SM, counter barrier
+                                   // 5 one persistent launch, 1-3 CTAs per SM, counter barrier
   unsigned trsv_grid = 0;          // persistent grid (whole blocks resident on every SM)
   uint32_t *flags = nullptr;       // [N] per-row completion epoch
   unsigned long long *ticket = nullptr;   // unused (kept zero)
@@ -165,7 +169,8 @@ struct DevMesh {
                                   // [4] counter of the one-CTA-per-SM sweep
   uint32_t *lev_ptr_d = nullptr;  // [nlev_l+1 + nlev_u+1] level offsets on the device
   unsigned trsv_pgrid = 0;        // persistent sweep grid
-  unsigned trsv_mgrid = 0;        // one-CTA-per-SM persistent sweep grid (mode 5)
+  unsigned trsv_mgrid = 0;        // persistent sweep grid of mode 5 (SMs x trsv_mgrid_per)
+  int trsv_mgrid_per = 2;         // 512-thread CTAs per SM in mode 5 (1, 2 or 3)
   double *h_scal = nullptr;       // pinned host mirror of scal
   // flexible GMRES (right preconditioning) and the learned preconditioner
   double *Z = nullptr;            // [30][4N] preconditioned basis vectors

@@ -292,7 +292,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *mbar, unsigned phase, int *e
 // end points and least-squares terms) staged into shared memory by four bulk
 // copies.  The range is widened to 4-entry boundaries so every copy starts and
 // ends on 16 bytes (the arrays are padded to a multiple of 4 entries).
-__global__ void __launch_bounds__(128) k_gradient_tma(uint32_t N, const uint32_t *__restrict__ inc_ptr,
+__global__ void __launch_bounds__(128) k_gradient_tma(uint32_t N, const uint32_t *__restrict__ ord,
+                                                      const uint32_t *__restrict__ inc_ptr,
                                                       const uint32_t *__restrict__ inc_oth,
                                                       const double *__restrict__ inc_w, uint32_t wstride,
                                                       const double4 *__restrict__ q, double4 *__restrict__ gx,
@@ -318,12 +319,13 @@ __global__ void __launch_bounds__(128) k_gradient_tma(uint32_t N, const uint32_t
   }
   __syncthreads();
   if (!mbar_wait(&mbar, 0, err)) return;
-  const uint32_t n = nb + threadIdx.x;
-  if (n >= N) return;
+  const uint32_t p = nb + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t n = ord[p];
   const double4 qn = q[n];
   double4 ax = make_double4(0, 0, 0, 0), ay = ax, az = ax;
-  const uint32_t e1 = inc_ptr[n + 1] - ka;
-  for (uint32_t k = inc_ptr[n] - ka; k < e1; k++) {
+  const uint32_t e1 = inc_ptr[p + 1] - ka;
+  for (uint32_t k = inc_ptr[p] - ka; k < e1; k++) {
     const double4 qo = q[s_oth[k]];
     const double wx = s_w[k], wy = s_w[cnt + k], wz = s_w[2 * (size_t)cnt + k];
     double dq;
@@ -341,18 +343,20 @@ __global__ void __launch_bounds__(128) k_gradient_tma(uint32_t N, const uint32_t
 
 // src/flux.c:60-145 as a gather: node n sums w.(q[other]-q[n]) over its
 // incident edges in edge order.
-__global__ void __launch_bounds__(256) k_gradient(uint32_t N, const uint32_t *__restrict__ inc_ptr,
+__global__ void __launch_bounds__(256) k_gradient(uint32_t N, const uint32_t *__restrict__ ord,
+                                                  const uint32_t *__restrict__ inc_ptr,
                                                   const uint32_t *__restrict__ inc_oth,
                                                   const double *__restrict__ inc_w, uint32_t ninc,
                                                   const double4 *__restrict__ q, double4 *__restrict__ gx,
                                                   double4 *__restrict__ gy, double4 *__restrict__ gz)
 {
-  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t n = ord[p];
   const double4 qn = q[n];
   double4 ax = make_double4(0, 0, 0, 0), ay = ax, az = ax;
-  const uint32_t k1 = inc_ptr[n + 1];
-  for (uint32_t k = inc_ptr[n]; k < k1; k++) {
+  const uint32_t k1 = inc_ptr[p + 1];
+  for (uint32_t k = inc_ptr[p]; k < k1; k++) {
     const double4 qo = q[inc_oth[k]];
     const double wx = inc_w[k], wy = inc_w[ninc + k], wz = inc_w[2 * (size_t)ninc + k];
     double dq;
@@ -372,7 +376,8 @@ __global__ void __launch_bounds__(256) k_gradient(uint32_t N, const uint32_t *__
 // edge (end points in the reference's n0/n1 roles) and adds it (n = n0) or
 // subtracts it (n = n1) in edge order.
 template <bool FIRST_ORDER>
-__global__ void __launch_bounds__(128) k_residual(uint32_t N, const uint32_t *__restrict__ inc_ptr,
+__global__ void __launch_bounds__(128) k_residual(uint32_t N, const uint32_t *__restrict__ ord,
+                                                  const uint32_t *__restrict__ inc_ptr,
                                                   const uint32_t *__restrict__ inc_oth,
                                                   const uint32_t *__restrict__ inc_edge,
                                                   const double4 *__restrict__ egeo,
@@ -382,14 +387,15 @@ __global__ void __launch_bounds__(128) k_residual(uint32_t N, const uint32_t *__
                                                   const double4 *__restrict__ gy,
                                                   const double4 *__restrict__ gz, double4 *__restrict__ r)
 {
-  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t n = ord[p];
   const double4 qs = q[n], xs = xyz[n];
   double4 gxs, gys, gzs;
   if (!FIRST_ORDER) { gxs = gx[n]; gys = gy[n]; gzs = gz[n]; }
   double4 acc = make_double4(0, 0, 0, 0);
-  const uint32_t k1 = inc_ptr[n + 1];
-  for (uint32_t k = inc_ptr[n]; k < k1; k++) {
+  const uint32_t k1 = inc_ptr[p + 1];
+  for (uint32_t k = inc_ptr[p]; k < k1; k++) {
     const uint32_t o = inc_oth[k], ev = inc_edge[k];
     const bool is_n1 = ev >> 31;
     const double4 geo = egeo[ev & 0x7fffffffu];
@@ -421,8 +427,13 @@ __global__ void __launch_bounds__(128) k_residual(uint32_t N, const uint32_t *__
 // edge order, then add the n0-side fluxes in edge order.  Pass 1 evaluates
 // each edge's flux once (thread per n0 node over its contiguous edges) and
 // stores it; in the fast build it also keeps the n0-side sum.  Pass 2 gathers.
+// Nodes are visited in the order ord (position p -> node ord[p]); the edge
+// arrays (geometry, far end, flux) are stored grouped by n0 in that order,
+// each group in edge order, so eoff, in1_ptr and s0 are indexed by position
+// and in1_edge holds storage positions.
 template <bool FIRST_ORDER, bool FAST>
-__global__ void __launch_bounds__(128) k_flux_edges(uint32_t N, const uint32_t *__restrict__ eoff,
+__global__ void __launch_bounds__(128) k_flux_edges(uint32_t N, const uint32_t *__restrict__ ord,
+                                                    const uint32_t *__restrict__ eoff,
                                                     const uint32_t *__restrict__ n1,
                                                     const double4 *__restrict__ egeo,
                                                     const double4 *__restrict__ xyz,
@@ -432,9 +443,10 @@ __global__ void __launch_bounds__(128) k_flux_edges(uint32_t N, const uint32_t *
                                                     const double4 *__restrict__ gz, double4 *__restrict__ res,
                                                     double4 *__restrict__ s0)
 {
-  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const uint32_t e0 = eoff[n], e1 = eoff[n + 1];
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t n = ord ? ord[p] : p;
+  const uint32_t e0 = eoff[p], e1 = eoff[p + 1];
   double4 acc = make_double4(0, 0, 0, 0);
   if (e0 < e1) {
     const double4 qa = q[n], xa = xyz[n];
@@ -459,26 +471,28 @@ __global__ void __launch_bounds__(128) k_flux_edges(uint32_t N, const uint32_t *
       if (FAST) acc = add4(acc, f);
     }
   }
-  if (FAST) s0[n] = acc;
+  if (FAST) s0[p] = acc;
 }
 
 template <bool FAST>
-__global__ void __launch_bounds__(256) k_flux_nodes(uint32_t N, const uint32_t *__restrict__ in1_ptr,
+__global__ void __launch_bounds__(256) k_flux_nodes(uint32_t N, const uint32_t *__restrict__ ord,
+                                                    const uint32_t *__restrict__ in1_ptr,
                                                     const uint32_t *__restrict__ in1_edge,
                                                     const uint32_t *__restrict__ eoff,
                                                     const double4 *__restrict__ res,
                                                     const double4 *__restrict__ s0, double4 *__restrict__ r)
 {
-  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t n = ord ? ord[p] : p;
   double4 acc = make_double4(0, 0, 0, 0);
-  const uint32_t k1 = in1_ptr[n + 1];
-  for (uint32_t k = in1_ptr[n]; k < k1; k++) acc = sub4(acc, res[in1_edge[k]]);
+  const uint32_t k1 = in1_ptr[p + 1];
+  for (uint32_t k = in1_ptr[p]; k < k1; k++) acc = sub4(acc, res[in1_edge[k]]);
   if (FAST) {
-    acc = add4(s0[n], acc);
+    acc = add4(s0[p], acc);
   } else {
-    const uint32_t e1 = eoff[n + 1];
-    for (uint32_t e = eoff[n]; e < e1; e++) acc = add4(acc, res[e]);
+    const uint32_t e1 = eoff[p + 1];
+    for (uint32_t e = eoff[p]; e < e1; e++) acc = add4(acc, res[e]);
   }
   r[n] = acc;
 }
@@ -524,7 +538,8 @@ __global__ void k_residual_boundary(uint32_t nb, const uint32_t *__restrict__ bn
 
 // src/timestep.c:58-91 as a gather; nodes without boundary terms are divided
 // by the CFL number here, boundary nodes in k_timestep_boundary.
-__global__ void __launch_bounds__(256) k_timestep(uint32_t N, const uint32_t *__restrict__ inc_ptr,
+__global__ void __launch_bounds__(256) k_timestep(uint32_t N, const uint32_t *__restrict__ ord,
+                                                  const uint32_t *__restrict__ inc_ptr,
                                                   const uint32_t *__restrict__ inc_oth,
                                                   const uint32_t *__restrict__ inc_edge,
                                                   const double4 *__restrict__ egeo,
@@ -532,12 +547,13 @@ __global__ void __launch_bounds__(256) k_timestep(uint32_t N, const uint32_t *__
                                                   const uint32_t *__restrict__ bnd_of, double cfl,
                                                   double *__restrict__ cdt)
 {
-  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t n = ord[p];
   const double4 qs = q[n];
   double acc = 0.0;
-  const uint32_t k1 = inc_ptr[n + 1];
-  for (uint32_t k = inc_ptr[n]; k < k1; k++) {
+  const uint32_t k1 = inc_ptr[p + 1];
+  for (uint32_t k = inc_ptr[p]; k < k1; k++) {
     const uint32_t ev = inc_edge[k];
     const bool is_n1 = ev >> 31;
     const double4 geo = egeo[ev & 0x7fffffffu];
@@ -747,7 +763,8 @@ template <> __device__ __forceinline__ void store_block<float>(float *dst, const
 // row n1, is written once.  The row's first persistent L slot receives the
 // last lower block the reference's fill would touch (matrix/matrix.cpp:239).
 template <typename T>
-__global__ void __launch_bounds__(128) k_fill(uint32_t N, const uint32_t *__restrict__ inc_ptr,
+__global__ void __launch_bounds__(128) k_fill(uint32_t N, const uint32_t *__restrict__ rowof,
+                                              const uint32_t *__restrict__ inc_ptr,
                                               const uint32_t *__restrict__ inc_oth,
                                               const uint32_t *__restrict__ inc_edge,
                                               const uint32_t *__restrict__ inc_blk,
@@ -762,6 +779,7 @@ __global__ void __launch_bounds__(128) k_fill(uint32_t N, const uint32_t *__rest
 {
   const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= N) return;
+  const uint32_t p = rowof[n];   // nodes in their own order: the matrix rows are written in sequence
   const double4 qs = q[n];
   double D[16];
 #pragma unroll
@@ -769,8 +787,8 @@ __global__ void __launch_bounds__(128) k_fill(uint32_t N, const uint32_t *__rest
   const double c = cdt[n];
   D[0] += c; D[5] += c; D[10] += c; D[15] += c;
   const uint32_t ll = last_lower[n];
-  const uint32_t k1 = inc_ptr[n + 1];
-  for (uint32_t k = inc_ptr[n]; k < k1; k++) {
+  const uint32_t k1 = inc_ptr[p + 1];
+  for (uint32_t k = inc_ptr[p]; k < k1; k++) {
     const uint32_t ev = inc_edge[k];
     const bool is_n1 = ev >> 31;
     const double4 geo = egeo[ev & 0x7fffffffu];
@@ -1421,10 +1439,10 @@ __device__ __forceinline__ bool kf_mono_barrier(unsigned *cnt, unsigned target, 
   return ok_s != 0;
 }
 
-// Both sweeps in one cooperative launch of one 512-thread CTA per SM; levels
-// separated by kf_mono_barrier.  Arithmetic as in k_trsv_level16.
-template <typename T>
-__global__ void __launch_bounds__(512, 1) k_trsv_persistent_mono(const uint32_t *__restrict__ lev_l, uint32_t nl,
+// Both sweeps in one cooperative launch of MINB 512-thread CTAs per SM;
+// levels separated by kf_mono_barrier.  Arithmetic as in k_trsv_level16.
+template <typename T, int MINB>
+__global__ void __launch_bounds__(512, MINB) k_trsv_persistent_mono(const uint32_t *__restrict__ lev_l, uint32_t nl,
                                                                  const uint32_t *__restrict__ lev_u, uint32_t nu,
                                                                  const uint4 *__restrict__ desc_l,
                                                                  const uint4 *__restrict__ desc_u,
@@ -1692,11 +1710,11 @@ void gradient(DevMesh &m, const double *q)
       cudaFuncSetAttribute(k_gradient_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
       attr_set = true;
     }
-    k_gradient_tma<<<blocks(m.N, 128), 128, m.grad_smem, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_w, m.wstride,
+    k_gradient_tma<<<blocks(m.N, 128), 128, m.grad_smem, m.stream>>>(m.N, m.ord, m.inc_ptr, m.inc_oth, m.inc_w, m.wstride,
                                                                     (const double4 *)q, (double4 *)m.gx,
                                                                     (double4 *)m.gy, (double4 *)m.gz, m.status + 1);
   } else {
-    k_gradient<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_w, m.wstride,
+    k_gradient<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.inc_ptr, m.inc_oth, m.inc_w, m.wstride,
                                                         (const double4 *)q, (double4 *)m.gx,
                                                         (double4 *)m.gy, (double4 *)m.gz);
   }
@@ -1709,19 +1727,19 @@ void residual(DevMesh &m, const double *q, double *r, int first_order, double u,
     const double4 *G[3] = {(const double4 *)m.gx, (const double4 *)m.gy, (const double4 *)m.gz};
     if (first_order)
       k_flux_edges<true, KF_FAST><<<blocks(m.N, 128), 128, 0, m.stream>>>(
-          m.N, m.eoff, m.n1, m.egeo, m.xyz, (const double4 *)q, nullptr, nullptr, nullptr, m.eres, m.s0);
+          m.N, m.ord, m.eoff, m.n1, m.egeo_s, m.xyz, (const double4 *)q, nullptr, nullptr, nullptr, m.eres, m.s0);
     else
       k_flux_edges<false, KF_FAST><<<blocks(m.N, 128), 128, 0, m.stream>>>(
-          m.N, m.eoff, m.n1, m.egeo, m.xyz, (const double4 *)q, G[0], G[1], G[2], m.eres, m.s0);
-    k_flux_nodes<KF_FAST><<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.in1_ptr, m.in1_edge, m.eoff, m.eres, m.s0,
+          m.N, m.ord, m.eoff, m.n1, m.egeo_s, m.xyz, (const double4 *)q, G[0], G[1], G[2], m.eres, m.s0);
+    k_flux_nodes<KF_FAST><<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.in1_ptr, m.in1_edge, m.eoff, m.eres, m.s0,
                                                                   (double4 *)r);
     kf_count_launch(2);
   } else if (first_order)
-    k_residual<true><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo, m.xyz,
+    k_residual<true><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.ord, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo, m.xyz,
                                                             (const double4 *)q, nullptr, nullptr, nullptr,
                                                             (double4 *)r);
   else
-    k_residual<false><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo, m.xyz,
+    k_residual<false><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.ord, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo, m.xyz,
                                                              (const double4 *)q, (const double4 *)m.gx,
                                                              (const double4 *)m.gy, (const double4 *)m.gz,
                                                              (double4 *)r);
@@ -1735,7 +1753,7 @@ void residual(DevMesh &m, const double *q, double *r, int first_order, double u,
 
 void timestep(DevMesh &m, const double *q, double cfl)
 {
-  k_timestep<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo,
+  k_timestep<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo,
                                                       (const double4 *)q, m.bnd_of, cfl, m.cdt);
   kf_count_launch();
   if (m.nb) {
@@ -1748,7 +1766,7 @@ void timestep(DevMesh &m, const double *q, double cfl)
 void fill(DevMesh &m, const double *q, double u, double v, int precision)
 {
   if (precision == 0) {
-    k_fill<double><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_edge, m.inc_blk, m.egeo,
+    k_fill<double><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.rowof, m.inc_ptr, m.inc_oth, m.inc_edge, m.inc_blk, m.egeo,
                                                           (const double4 *)q, m.cdt, m.diag, m.last_lower,
                                                           m.lpos, m.A, m.lslot, m.bnd_of, nullptr);
     kf_count_launch();
@@ -1759,7 +1777,7 @@ void fill(DevMesh &m, const double *q, double u, double v, int precision)
       kf_count_launch();
     }
   } else {
-    k_fill<float><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.inc_ptr, m.inc_oth, m.inc_edge, m.inc_blk, m.egeo,
+    k_fill<float><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.rowof, m.inc_ptr, m.inc_oth, m.inc_edge, m.inc_blk, m.egeo,
                                                          (const double4 *)q, m.cdt, m.diag, m.last_lower, m.lpos,
                                                          m.Af, nullptr, m.bnd_of, m.dscr);
     kf_count_launch();
@@ -1853,8 +1871,15 @@ void sptrsv(DevMesh &m, const double *b, double *x, int precision)
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const void *fn = precision == 0 ? (const void *)k_trsv_persistent_mono<double>
-                                    : (const void *)k_trsv_persistent_mono<float>;
+    const void *fn;
+    switch (m.trsv_mgrid_per) {
+      case 1: fn = precision == 0 ? (const void *)k_trsv_persistent_mono<double, 1>
+                                  : (const void *)k_trsv_persistent_mono<float, 1>; break;
+      case 3: fn = precision == 0 ? (const void *)k_trsv_persistent_mono<double, 3>
+                                  : (const void *)k_trsv_persistent_mono<float, 3>; break;
+      default: fn = precision == 0 ? (const void *)k_trsv_persistent_mono<double, 2>
+                                   : (const void *)k_trsv_persistent_mono<float, 2>; break;
+    }
     const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
     if (e != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e));
     kf_count_launch();

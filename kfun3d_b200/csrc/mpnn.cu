@@ -911,7 +911,7 @@ int launch_fwd(kfun3d_mpnn *net, G g, O o, uint32_t rows, int layer, uint4 *a1_s
   auto kern = k_mlp_fwd<K1, N2, G, O>;
   static unsigned grid_cache[64] = {0};
   unsigned &gc = grid_cache[net->device & 63];
-  if (!gc) gc = persistent_grid(kern, smem, net->nsm, 4);   // 64 TMEM columns per CTA
+  if (!gc) gc = persistent_grid(kern, smem, net->nsm, 8);   // 64 TMEM columns per CTA: 8 fill the SM's 512
   const unsigned ntiles = (rows + 127) / 128;
   const unsigned grid = std::min(gc, ntiles);
   const uint4 *W1 = reinterpret_cast<const uint4 *>(net->W + kOff.off[layer]);

@@ -814,8 +814,10 @@ void write_pair(DevMesh &m, const Ops &o, int prec, const double *x, PairSink &p
 // preconditioned residual to an approximation of the correction x with
 // ILU(0)^-1 J x = v.  The network is a guest: each linear solve starts with
 // both candidate first directions and keeps the network only if its image
-// under ILU(0)^-1 J lies closer to v0 (one extra product per Newton step);
-// three refusals in a row switch it off for good; and an update after which
+// under ILU(0)^-1 J lies closer to v0 (one extra product per Newton step),
+// and only for as many iterations as the previous step's solve needed in all
+// (x 1.5), after which the solve goes on without it; three refusals in a row
+// switch it off for good; and an update after which
 // the FP64 nonlinear residual is non-finite or grows tenfold is undone and
 // redone without it.
 static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_params *p, kfun3d_mpnn *net,
@@ -840,7 +842,7 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
   double cs[KF_NBASIS], sn[KF_NBASIS], rs[KF_NBASIS], yk[KF_NBASIS];
   double fnorm0 = 0.0, fnorm_prev = 0.0, cfl = p->cfl_init;
   bool use_net = net != nullptr, last_used_net = false;
-  int misses = 0;
+  int misses = 0, prev_total = -1;
   int nrec = 0, steps = 0;
   cudaEvent_t ev0, ev1, es0, es1;
   CK(cudaEventCreate(&ev0));
@@ -892,6 +894,9 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
       }
     }
     bool step_net = use_net;
+    // iterations the network may use in this solve: 1.5 x the previous step's
+    // solve (two cycles for the first step)
+    const int budget = prev_total > 0 ? (3 * prev_total + 1) / 2 : 2 * restart;
     bool usez[KF_NBASIS] = {false};
     double tol = 0.0;
     unsigned int total = 0;
@@ -975,6 +980,15 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
         k++;
         if (res <= tol) { done = true; break; }
         if (!std::isfinite(res)) { failed = true; break; }
+        if (step_net && (int)total + k > budget) {
+          // the network has had the iterations the previous solve needed in all: go on without it
+          step_net = false;
+          S.fallback_solves++;
+          if (++misses >= 3) {
+            use_net = false;
+            S.disabled = 1;
+          }
+        }
         if (ps && ps->stride > 0 && cycle == 0 && k < restart && (k % ps->stride) == 0 && ps->count < ps->cap) {
           back_substitute(ghh, rs, k, yk);
           CK(cudaMemsetAsync(m.fx, 0, n * sizeof(double), m.stream));
@@ -999,6 +1013,7 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
     }
     if (net && kf_mpnn_status(net, m.stream) != KFUN3D_OK) { steps = -1; break; }
     S.gmres_its += (int)total;
+    prev_total = (int)total;
     if (ps && ps->count < ps->cap) write_pair(m, o, prec, m.x, *ps);
     if (step_net) CK(cudaMemcpyAsync(m.qold, m.q, n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
     last_used_net = step_net;

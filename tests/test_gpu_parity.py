@@ -226,3 +226,28 @@ def test_exact_sptrsv_every_schedule(box_mesh, schedule, monkeypatch):
             assert rel(m.sptrsv(b), M.sptrsv_f32(b)) < 1e-5, schedule
     kf.set_precision(0)
     assert kf.last_status() == 0
+
+
+@pytest.mark.parametrize("order", ["natural", "morton"])
+def test_exact_kernels_any_node_order(box_mesh, order, monkeypatch):
+    """The order in which node-centric kernels visit nodes (and the storage
+    order of the edge arrays that follows it) leaves every result bit-identical
+    to the oracle: each node's sums still run over its edges in edge order."""
+    monkeypatch.setenv("KFUN3D_NODE_ORDER", order)
+    kf.set_mode("exact")
+    kf.set_precision(0)
+    kf.set_aoa(3.06)
+    for path in (box_mesh(12, seed=41), MESH_A):
+        m = kf.Mesh(path)
+        v = m.view
+        q = seeded_state(v.q.copy(), 41)
+        (g1, r1) = m.flux(q)
+        (g2, r2) = port.flux(m.g, 3.06, q)
+        assert np.array_equal(r1, r2) and all(np.array_equal(a, b) for a, b in zip(g1, g2)), (order, path)
+        c1 = m.timestep(37.5, q)
+        assert np.array_equal(c1, port.timestep(m.g, v.nnodes, 37.5, q))
+        M = port.Matrix(m.g)
+        m.fill(q, c1)
+        M.fill(3.06, q, c1)
+        assert np.array_equal(m.matrix()[2], M.blocks()), (order, path)
+    assert kf.last_status() == 0
