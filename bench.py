@@ -443,6 +443,21 @@ def run_gpu_arm(args, cfg):
     dist.close()
 
 
+def run_kernel_probe(args, cfg):
+    """--kernel NAME: time one kernel family `reps` times on the workload's mesh
+    and print {"kernel", "ms", "gbs"} -- the command the profiles use to
+    capture a single kernel under ncu."""
+    import kfun3d_b200 as kf
+    configure(kf, cfg)
+    m = kf.Mesh(mesh_path(cfg))
+    v = m.view
+    B = alg_bytes(v.nnodes, v.nedges, v.nfaces, v.ns, v.nf, v.nnodes + 2 * v.nedges, cfg["precision"])
+    ms = m.time_kernel(args.kernel, args.reps)
+    print(json.dumps({"kernel": args.kernel, "config": cfg["workload"], "ms": ms,
+                      "gbs": B.get(args.kernel, 0) / (ms * 1e-3) / 1e9 if ms > 0 else None}))
+    m.close()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -454,9 +469,19 @@ def main():
     ap.add_argument("--ref-total-its", type=int, default=None,
                     help="GMRES iterations of the full solve used to extrapolate the reference sample "
                          "(default: the plain FP64 solve's count for the workload)")
+    ap.add_argument("--kernel", default=None,
+                    help="time one kernel family (flux, gradient, edge_flux, timestep, fill, ilu, sptrsv, mgs, "
+                         "gmres_iter) instead of the solve")
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--precision", type=int, default=None, choices=[0, 1],
+                    help="override the workload's preconditioner precision (with --kernel)")
     args = ap.parse_args()
-    cfg = CONFIGS[args.config]
-    if args.impl == "reference":
+    cfg = dict(CONFIGS[args.config])
+    if args.precision is not None:
+        cfg["precision"] = args.precision
+    if args.kernel:
+        run_kernel_probe(args, cfg)
+    elif args.impl == "reference":
         run_reference_arm(args, cfg)
     else:
         run_gpu_arm(args, cfg)

@@ -292,10 +292,11 @@ typedef struct {
  * reference's residual measure and stopping test) and a right preconditioner
  * that may change per iteration: the identity (net == NULL: the reference's
  * GMRES, iteration for iteration) or the network's correction
- * v + s N([v/s, q]).  The network falls back to the identity: for a linear
- * solve whose first direction it does not improve (its image under
- * ILU(0)^-1 J farther from v0), for the rest of a solve that has used 1.5x
- * the previous Newton step's iterations, for good after three such
+ * v + s N([v/s, q]), from Newton step 1 on.  The network falls back to
+ * the identity: for a linear solve whose first direction it does not improve
+ * (its image under ILU(0)^-1 J farther from v0), for the rest of a solve
+ * whose residual falls at less than half the previous solve's rate or that
+ * has used 1.5x the previous solve's iterations, for good after three such
  * fallbacks in a row,
  * and for an update after which the FP64 nonlinear residual grows tenfold
  * (the update is undone).  Solves from g->q->q and updates it; returns the

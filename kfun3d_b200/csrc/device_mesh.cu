@@ -245,7 +245,7 @@ static void release_device(MatrixHandle *h)
                   m->wf_n, m->s_n, m->f_n, m->bnd_of, m->bnd_node, m->bnd_ptr, m->bnd_ent, m->ia, m->ja,
                   m->diag, m->tblk, m->lpos, m->last_lower, m->lev_l, m->lev_u, m->A, m->lslot, m->dinv,
                   m->Af, m->dinvf, m->q, m->r, m->gx, m->gy, m->gz, m->cdt, m->w, m->t, m->x, m->rhs, m->V,
-                  m->red, m->scal, m->forces, m->dscr, m->status, m->flags, m->ticket, m->part, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->s0, m->pair_ptr, m->pairs, m->lev_ptr_d, m->bar, m->Z, m->qold, m->fy, m->fx, m->pscr, m->ord, m->rowof, m->egeo_s};
+                  m->red, m->scal, m->forces, m->dscr, m->status, m->flags, m->ticket, m->part, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->n0s, m->pair_ptr, m->pairs, m->lev_ptr_d, m->bar, m->Z, m->qold, m->fy, m->fx, m->pscr, m->ord, m->rowof, m->egeo_s};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (m->h_scal) cudaFreeHost(m->h_scal);
@@ -423,7 +423,7 @@ DevMesh *kf_device(const GEOMETRY *g)
       for (uint32_t e = 0; e < E; e++) { r0[n0[e] + 1]++; c1[n1[e]]++; }
       for (uint32_t i = 0; i < N; i++) r0[i + 1] += r0[i];
       // storage: groups by n0 in visit order, each in edge order
-      std::vector<uint32_t> eoff(N + 1, 0), spos(E), n1s(E), iptr(N + 1, 0), iedge(E);
+      std::vector<uint32_t> eoff(N + 1, 0), spos(E), n0s(E), n1s(E), iptr(N + 1, 0), iedge(E);
       std::vector<double4> egs(E);
       uint32_t next = 0;
       for (uint32_t p2 = 0; p2 < N; p2++) {
@@ -431,6 +431,7 @@ DevMesh *kf_device(const GEOMETRY *g)
         eoff[p2] = next;
         for (uint32_t e = r0[nd]; e < r0[nd + 1]; e++) {
           spos[e] = next;
+          n0s[next] = nd;
           n1s[next] = n1[e];
           egs[next] = make_double4(g->e->xyzn->x0[e], g->e->xyzn->x1[e], g->e->xyzn->x2[e], g->e->xyzn->x3[e]);
           next++;
@@ -442,12 +443,12 @@ DevMesh *kf_device(const GEOMETRY *g)
       for (uint32_t p2 = 0; p2 < N; p2++) ipos[ord[p2]] = iptr[p2];
       for (uint32_t e = 0; e < E; e++) iedge[ipos[n1[e]]++] = spos[e];
       KF_CUDA(upload(&m->eoff, eoff.data(), N + 1));
+      KF_CUDA(upload(&m->n0s, n0s.data(), E));
       KF_CUDA(upload(&m->n1, n1s.data(), E));
       KF_CUDA(upload(&m->egeo_s, egs.data(), E));
       KF_CUDA(upload(&m->in1_ptr, iptr.data(), N + 1));
       KF_CUDA(upload(&m->in1_edge, iedge.data(), E));
       KF_CUDA(cudaMalloc(&m->eres, std::max<size_t>(E, 1) * sizeof(double4)));
-      KF_CUDA(cudaMalloc(&m->s0, std::max<size_t>(N, 1) * sizeof(double4)));
     }
   }
   // wall faces (colour order) with normals -(1/6) a x b (src/flux.c:485-508)
@@ -558,6 +559,8 @@ DevMesh *kf_device(const GEOMETRY *g)
     const char *cenv = getenv("KFUN3D_SPTRSV_CTAS");
     if (cenv && (atoi(cenv) >= 1 && atoi(cenv) <= 3)) m->trsv_mgrid_per = atoi(cenv);
     m->trsv_mgrid = (unsigned)nsm * (unsigned)m->trsv_mgrid_per;
+    const char *lenv = getenv("KFUN3D_SPTRSV_LANES");
+    if (lenv && atoi(lenv) == 8) m->trsv_lanes = 8;
     std::vector<uint4> dl(N), du(N);
     for (uint32_t s = 0; s < N; s++) {
       const uint32_t i = p.lev_l[s];

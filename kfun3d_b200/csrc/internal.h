@@ -109,12 +109,12 @@ struct DevMesh {
   // order: grouped by n0 in node-visit order (ord), each group in edge order
   bool two_pass = false;
   uint32_t *eoff = nullptr;       // [N+1] storage range of the edges with n0 = ord[p]
-  uint32_t *n1 = nullptr;         // [E] far end (n1) of each stored edge
+  uint32_t *n0s = nullptr;        // [E] n0 of each stored edge
+  uint32_t *n1 = nullptr;         // [E] n1 of each stored edge
   double4 *egeo_s = nullptr;      // [E] edge geometry in storage order
   uint32_t *in1_ptr = nullptr;    // [N+1] edges with n1 = ord[p], in edge order
   uint32_t *in1_edge = nullptr;   // [E] their storage positions
   double4 *eres = nullptr;        // [E] edge fluxes, storage order
-  double4 *s0 = nullptr;          // [N] n0-side sums by position (fast build)
   uint32_t *wf_nodes = nullptr;   // [3F] wall faces in colour order
   double *wf_n = nullptr;         // [3F] wall-face normals -(1/6) a x b
   uint32_t *col = nullptr;        // [ncol+1] wall-face colour offsets
@@ -171,6 +171,7 @@ struct DevMesh {
   unsigned trsv_pgrid = 0;        // persistent sweep grid
   unsigned trsv_mgrid = 0;        // persistent sweep grid of mode 5 (SMs x trsv_mgrid_per)
   int trsv_mgrid_per = 2;         // 512-thread CTAs per SM in mode 5 (1, 2 or 3)
+  int trsv_lanes = 16;            // lanes per row in mode 5 (8 or 16)
   double *h_scal = nullptr;       // pinned host mirror of scal
   // flexible GMRES (right preconditioning) and the learned preconditioner
   double *Z = nullptr;            // [30][4N] preconditioned basis vectors

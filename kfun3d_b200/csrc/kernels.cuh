@@ -425,75 +425,54 @@ __global__ void __launch_bounds__(128) k_residual(uint32_t N, const uint32_t *__
 // Then a node's edges as n1 all precede its edges as n0 in edge order, so the
 // reference's per-node sum in edge order is: subtract the n1-side fluxes in
 // edge order, then add the n0-side fluxes in edge order.  Pass 1 evaluates
-// each edge's flux once (thread per n0 node over its contiguous edges) and
-// stores it; in the fast build it also keeps the n0-side sum.  Pass 2 gathers.
-// Nodes are visited in the order ord (position p -> node ord[p]); the edge
-// arrays (geometry, far end, flux) are stored grouped by n0 in that order,
-// each group in edge order, so eoff, in1_ptr and s0 are indexed by position
-// and in1_edge holds storage positions.
-template <bool FIRST_ORDER, bool FAST>
-__global__ void __launch_bounds__(128) k_flux_edges(uint32_t N, const uint32_t *__restrict__ ord,
-                                                    const uint32_t *__restrict__ eoff,
+// each edge's flux once, one thread per edge, and stores it; pass 2 gathers
+// per node.  The edge arrays (end points, geometry, flux) are stored grouped
+// by n0 in the nodes' visit order ord, each group in edge order: a warp's
+// edges are then close in space (their end points' data is shared in L2 and
+// L1), and eoff / in1_ptr are indexed by visit position, in1_edge holds
+// storage positions.
+template <bool FIRST_ORDER>
+__global__ void __launch_bounds__(128) k_flux_edges(uint32_t E, const uint32_t *__restrict__ n0,
                                                     const uint32_t *__restrict__ n1,
                                                     const double4 *__restrict__ egeo,
                                                     const double4 *__restrict__ xyz,
                                                     const double4 *__restrict__ q,
                                                     const double4 *__restrict__ gx,
                                                     const double4 *__restrict__ gy,
-                                                    const double4 *__restrict__ gz, double4 *__restrict__ res,
-                                                    double4 *__restrict__ s0)
+                                                    const double4 *__restrict__ gz, double4 *__restrict__ res)
 {
-  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= N) return;
-  const uint32_t n = ord ? ord[p] : p;
-  const uint32_t e0 = eoff[p], e1 = eoff[p + 1];
-  double4 acc = make_double4(0, 0, 0, 0);
-  if (e0 < e1) {
-    const double4 qa = q[n], xa = xyz[n];
-    double4 gxa, gya, gza;
-    if (!FIRST_ORDER) { gxa = gx[n]; gya = gy[n]; gza = gz[n]; }
-    for (uint32_t e = e0; e < e1; e++) {
-      const uint32_t o = n1[e];
-      const double4 geo = egeo[e];
-      const double4 qb = q[o], xb = xyz[o];
-      const double xm = 0.5 * (xa.x + xb.x), ym = 0.5 * (xa.y + xb.y), zm = 0.5 * (xa.z + xb.z);
-      double4 sL, sR;
-      if (FIRST_ORDER) {
-        const double4 z = make_double4(0, 0, 0, 0);
-        sL = recon(qa, z, z, z, xm - xa.x, ym - xa.y, zm - xa.z);
-        sR = recon(qb, z, z, z, xm - xb.x, ym - xb.y, zm - xb.z);
-      } else {
-        sL = recon(qa, gxa, gya, gza, xm - xa.x, ym - xa.y, zm - xa.z);
-        sR = recon(qb, gx[o], gy[o], gz[o], xm - xb.x, ym - xb.y, zm - xb.z);
-      }
-      const double4 f = edge_flux(geo, sL, sR);
-      res[e] = f;
-      if (FAST) acc = add4(acc, f);
-    }
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  const uint32_t a = n0[e], o = n1[e];
+  const double4 geo = egeo[e];
+  const double4 qa = q[a], xa = xyz[a], qb = q[o], xb = xyz[o];
+  const double xm = 0.5 * (xa.x + xb.x), ym = 0.5 * (xa.y + xb.y), zm = 0.5 * (xa.z + xb.z);
+  double4 sL, sR;
+  if (FIRST_ORDER) {
+    const double4 z = make_double4(0, 0, 0, 0);
+    sL = recon(qa, z, z, z, xm - xa.x, ym - xa.y, zm - xa.z);
+    sR = recon(qb, z, z, z, xm - xb.x, ym - xb.y, zm - xb.z);
+  } else {
+    sL = recon(qa, gx[a], gy[a], gz[a], xm - xa.x, ym - xa.y, zm - xa.z);
+    sR = recon(qb, gx[o], gy[o], gz[o], xm - xb.x, ym - xb.y, zm - xb.z);
   }
-  if (FAST) s0[p] = acc;
+  res[e] = edge_flux(geo, sL, sR);
 }
 
-template <bool FAST>
 __global__ void __launch_bounds__(256) k_flux_nodes(uint32_t N, const uint32_t *__restrict__ ord,
                                                     const uint32_t *__restrict__ in1_ptr,
                                                     const uint32_t *__restrict__ in1_edge,
                                                     const uint32_t *__restrict__ eoff,
-                                                    const double4 *__restrict__ res,
-                                                    const double4 *__restrict__ s0, double4 *__restrict__ r)
+                                                    const double4 *__restrict__ res, double4 *__restrict__ r)
 {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= N) return;
-  const uint32_t n = ord ? ord[p] : p;
+  const uint32_t n = ord[p];
   double4 acc = make_double4(0, 0, 0, 0);
   const uint32_t k1 = in1_ptr[p + 1];
   for (uint32_t k = in1_ptr[p]; k < k1; k++) acc = sub4(acc, res[in1_edge[k]]);
-  if (FAST) {
-    acc = add4(s0[p], acc);
-  } else {
-    const uint32_t e1 = eoff[p + 1];
-    for (uint32_t e = eoff[p]; e < e1; e++) acc = add4(acc, res[e]);
-  }
+  const uint32_t e1 = eoff[p + 1];
+  for (uint32_t e = eoff[p]; e < e1; e++) acc = add4(acc, res[e]);
   r[n] = acc;
 }
 
@@ -1381,6 +1360,59 @@ __device__ __forceinline__ void trsv_row16(const uint4 d, const uint32_t *__rest
   if (l16 < 4) __stcg(x + 4 * (size_t)i + r, xi);
 }
 
+// One row of a triangular sweep for a group of G lanes (G = 8 or 16): lane
+// (jj, r) takes blocks c0 + (G/4) p + jj, row r of each; the partial products
+// are subtracted in column order, so the arithmetic is k_trsv_level16's.
+template <typename T, bool UPPER, int G>
+__device__ __forceinline__ void trsv_row_g(const uint4 d, const uint32_t *__restrict__ ja, const T *__restrict__ A,
+                                           const double *__restrict__ b, double *x, int base, int gl,
+                                           unsigned gmask)
+{
+  constexpr int S = G / 4;   // block slots per step
+  const int jj = gl >> 2, r = gl & 3;
+  const uint32_t i = d.x, jb = d.y, je = d.z;
+  double xi = UPPER ? __ldcg(x + 4 * (size_t)i + r) : b[4 * (size_t)i + r];
+  for (uint32_t c0 = jb; c0 < je; c0 += 4 * S) {
+    double t[4];
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const uint32_t j = c0 + S * p + jj;
+      t[p] = 0.0;
+      if (j < je) {
+        const uint32_t col = ja[j];
+        const T *blk = A + 16 * (size_t)j + 4 * r;
+        const double2 x01 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)col);
+        const double2 x23 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)col + 1);
+        double s = 0.0;
+        s += (double)blk[0] * x01.x;
+        s += (double)blk[1] * x01.y;
+        s += (double)blk[2] * x23.x;
+        s += (double)blk[3] * x23.y;
+        t[p] = s;
+      }
+    }
+    const uint32_t cnt = (je - c0) < (uint32_t)(4 * S) ? (je - c0) : (uint32_t)(4 * S);
+#pragma unroll
+    for (int p = 0; p < 4; p++)
+      for (int q = 0; q < S; q++) {
+        if ((uint32_t)(S * p + q) >= cnt) break;
+        xi = -1.0 * __shfl_sync(gmask, t[p], base + 4 * q + r) + xi;
+      }
+  }
+  if (UPPER) {
+    const double x0 = __shfl_sync(gmask, xi, base + 0), x1 = __shfl_sync(gmask, xi, base + 1);
+    const double x2 = __shfl_sync(gmask, xi, base + 2), x3 = __shfl_sync(gmask, xi, base + 3);
+    const T *dg = A + 16 * (size_t)(jb - 1) + 4 * r;
+    double y = 0.0;
+    y += (double)dg[0] * x0;
+    y += (double)dg[1] * x1;
+    y += (double)dg[2] * x2;
+    y += (double)dg[3] * x3;
+    xi = y;
+  }
+  if (gl < 4) __stcg(x + 4 * (size_t)i + r, xi);
+}
+
 // Both sweeps in one cooperative launch: the rows of each level are spread
 // over every half-warp of the grid, and a grid barrier (kf_grid_barrier,
 // bounded) separates consecutive levels.  Arithmetic as in k_trsv_level16.
@@ -1441,7 +1473,7 @@ __device__ __forceinline__ bool kf_mono_barrier(unsigned *cnt, unsigned target, 
 
 // Both sweeps in one cooperative launch of MINB 512-thread CTAs per SM;
 // levels separated by kf_mono_barrier.  Arithmetic as in k_trsv_level16.
-template <typename T, int MINB>
+template <typename T, int MINB, int G>
 __global__ void __launch_bounds__(512, MINB) k_trsv_persistent_mono(const uint32_t *__restrict__ lev_l, uint32_t nl,
                                                                  const uint32_t *__restrict__ lev_u, uint32_t nu,
                                                                  const uint4 *__restrict__ desc_l,
@@ -1451,22 +1483,34 @@ __global__ void __launch_bounds__(512, MINB) k_trsv_persistent_mono(const uint32
                                                                  const double *__restrict__ b, double *x,
                                                                  unsigned *cnt, int *err)
 {
-  const int lane = threadIdx.x & 31, half = lane >> 4, l16 = lane & 15, jj = l16 >> 2, r = l16 & 3;
-  const unsigned hmask = 0xffffu << (16 * half);
-  const uint32_t H = gridDim.x * (blockDim.x >> 4);
-  const uint32_t h = blockIdx.x * (blockDim.x >> 4) + (threadIdx.x >> 4);
+  const int lane = threadIdx.x & 31, gl = lane & (G - 1), base = lane - gl;
+  const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << base;
+  const uint32_t H = gridDim.x * (blockDim.x / G);
+  const uint32_t h = blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
   unsigned passed = 0;
+  // each half-warp's next row descriptor is loaded while it solves the
+  // current row (the rows of one level are independent)
   for (uint32_t l = 0; l < nl; l++) {
     const uint32_t s1 = lev_l[l + 1];
-    for (uint32_t s = lev_l[l] + h; s < s1; s += H)
-      trsv_row16<T, false>(desc_l[s], ja, A, b, x, half, jj, r, l16, hmask);
+    uint32_t s = lev_l[l] + h;
+    uint4 d = s < s1 ? desc_l[s] : make_uint4(0, 0, 0, 0);
+    for (; s < s1; s += H) {
+      const uint4 dn = s + H < s1 ? desc_l[s + H] : d;
+      trsv_row_g<T, false, G>(d, ja, A, b, x, base, gl, gmask);
+      d = dn;
+    }
     __threadfence();
     if (!kf_mono_barrier(cnt, ++passed * gridDim.x, err)) return;
   }
   for (uint32_t l = 0; l < nu; l++) {
     const uint32_t s1 = lev_u[l + 1];
-    for (uint32_t s = lev_u[l] + h; s < s1; s += H)
-      trsv_row16<T, true>(desc_u[s], ja, A, b, x, half, jj, r, l16, hmask);
+    uint32_t s = lev_u[l] + h;
+    uint4 d = s < s1 ? desc_u[s] : make_uint4(0, 0, 0, 0);
+    for (; s < s1; s += H) {
+      const uint4 dn = s + H < s1 ? desc_u[s + H] : d;
+      trsv_row_g<T, true, G>(d, ja, A, b, x, base, gl, gmask);
+      d = dn;
+    }
     __threadfence();
     if (l + 1 < nu && !kf_mono_barrier(cnt, ++passed * gridDim.x, err)) return;
   }
@@ -1726,13 +1770,14 @@ void residual(DevMesh &m, const double *q, double *r, int first_order, double u,
   if (m.two_pass) {
     const double4 *G[3] = {(const double4 *)m.gx, (const double4 *)m.gy, (const double4 *)m.gz};
     if (first_order)
-      k_flux_edges<true, KF_FAST><<<blocks(m.N, 128), 128, 0, m.stream>>>(
-          m.N, m.ord, m.eoff, m.n1, m.egeo_s, m.xyz, (const double4 *)q, nullptr, nullptr, nullptr, m.eres, m.s0);
+      k_flux_edges<true><<<blocks(m.E, 128), 128, 0, m.stream>>>(m.E, m.n0s, m.n1, m.egeo_s, m.xyz,
+                                                                  (const double4 *)q, nullptr, nullptr, nullptr,
+                                                                  m.eres);
     else
-      k_flux_edges<false, KF_FAST><<<blocks(m.N, 128), 128, 0, m.stream>>>(
-          m.N, m.ord, m.eoff, m.n1, m.egeo_s, m.xyz, (const double4 *)q, G[0], G[1], G[2], m.eres, m.s0);
-    k_flux_nodes<KF_FAST><<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.in1_ptr, m.in1_edge, m.eoff, m.eres, m.s0,
-                                                                  (double4 *)r);
+      k_flux_edges<false><<<blocks(m.E, 128), 128, 0, m.stream>>>(m.E, m.n0s, m.n1, m.egeo_s, m.xyz,
+                                                                   (const double4 *)q, G[0], G[1], G[2], m.eres);
+    k_flux_nodes<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.in1_ptr, m.in1_edge, m.eoff, m.eres,
+                                                         (double4 *)r);
     kf_count_launch(2);
   } else if (first_order)
     k_residual<true><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.ord, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo, m.xyz,
@@ -1872,13 +1917,20 @@ void sptrsv(DevMesh &m, const double *b, double *x, int precision)
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const void *fn;
+    const bool g8 = m.trsv_lanes == 8;
     switch (m.trsv_mgrid_per) {
-      case 1: fn = precision == 0 ? (const void *)k_trsv_persistent_mono<double, 1>
-                                  : (const void *)k_trsv_persistent_mono<float, 1>; break;
-      case 3: fn = precision == 0 ? (const void *)k_trsv_persistent_mono<double, 3>
-                                  : (const void *)k_trsv_persistent_mono<float, 3>; break;
-      default: fn = precision == 0 ? (const void *)k_trsv_persistent_mono<double, 2>
-                                   : (const void *)k_trsv_persistent_mono<float, 2>; break;
+      case 1: fn = precision == 0 ? (g8 ? (const void *)k_trsv_persistent_mono<double, 1, 8>
+                                        : (const void *)k_trsv_persistent_mono<double, 1, 16>)
+                                  : (g8 ? (const void *)k_trsv_persistent_mono<float, 1, 8>
+                                        : (const void *)k_trsv_persistent_mono<float, 1, 16>); break;
+      case 3: fn = precision == 0 ? (g8 ? (const void *)k_trsv_persistent_mono<double, 3, 8>
+                                        : (const void *)k_trsv_persistent_mono<double, 3, 16>)
+                                  : (g8 ? (const void *)k_trsv_persistent_mono<float, 3, 8>
+                                        : (const void *)k_trsv_persistent_mono<float, 3, 16>); break;
+      default: fn = precision == 0 ? (g8 ? (const void *)k_trsv_persistent_mono<double, 2, 8>
+                                         : (const void *)k_trsv_persistent_mono<double, 2, 16>)
+                                   : (g8 ? (const void *)k_trsv_persistent_mono<float, 2, 8>
+                                         : (const void *)k_trsv_persistent_mono<float, 2, 16>); break;
     }
     const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
     if (e != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e));

@@ -814,9 +814,11 @@ void write_pair(DevMesh &m, const Ops &o, int prec, const double *x, PairSink &p
 // preconditioned residual to an approximation of the correction x with
 // ILU(0)^-1 J x = v.  The network is a guest: each linear solve starts with
 // both candidate first directions and keeps the network only if its image
-// under ILU(0)^-1 J lies closer to v0 (one extra product per Newton step),
-// and only for as many iterations as the previous step's solve needed in all
-// (x 1.5), after which the solve goes on without it; three refusals in a row
+// under ILU(0)^-1 J lies closer to v0 (one extra product per Newton step);
+// it keeps its place only while the residual falls at least half as fast
+// (per iteration, in log) as in the previous step's solve, and for at most
+// 1.5x that solve's iterations, after which the solve goes on without it;
+// Newton step 0 runs without it to set the pace; three fallbacks in a row
 // switch it off for good; and an update after which
 // the FP64 nonlinear residual is non-finite or grows tenfold is undone and
 // redone without it.
@@ -843,6 +845,7 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
   double fnorm0 = 0.0, fnorm_prev = 0.0, cfl = p->cfl_init;
   bool use_net = net != nullptr, last_used_net = false;
   int misses = 0, prev_total = -1;
+  double rate_prev = 0.0;   // log residual reduction per iteration of the previous linear solve
   int nrec = 0, steps = 0;
   cudaEvent_t ev0, ev1, es0, es1;
   CK(cudaEventCreate(&ev0));
@@ -893,10 +896,12 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
         break;
       }
     }
-    bool step_net = use_net;
+    // Newton step 0 runs without the network: it measures the rate the
+    // network then has to beat
+    bool step_net = use_net && prev_total > 0;
     // iterations the network may use in this solve: 1.5 x the previous step's
-    // solve (two cycles for the first step)
     const int budget = prev_total > 0 ? (3 * prev_total + 1) / 2 : 2 * restart;
+    double rs_first = 0.0, res_last = 0.0;
     bool usez[KF_NBASIS] = {false};
     double tol = 0.0;
     unsigned int total = 0;
@@ -914,6 +919,7 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
       if (!std::isfinite(rs[0])) { failed = true; break; }
       if (total == 0) {
         tol = p->gmres_rtol * rs[0];
+        rs_first = rs[0];
         if (rs[0] == 0.0) { done = true; break; }
       }
       int k = 0;
@@ -980,8 +986,12 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
         k++;
         if (res <= tol) { done = true; break; }
         if (!std::isfinite(res)) { failed = true; break; }
-        if (step_net && (int)total + k > budget) {
-          // the network has had the iterations the previous solve needed in all: go on without it
+        res_last = res;
+        // the network must keep at least half the previous solve's rate (log
+        // residual per iteration) and stay within its iteration budget
+        if (step_net && (((int)total + k >= 6 && rate_prev < 0.0 &&
+                          log(res / rs_first) > 0.5 * ((int)total + k) * rate_prev) ||
+                         (int)total + k > budget)) {
           step_net = false;
           S.fallback_solves++;
           if (++misses >= 3) {
@@ -1014,6 +1024,7 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
     if (net && kf_mpnn_status(net, m.stream) != KFUN3D_OK) { steps = -1; break; }
     S.gmres_its += (int)total;
     prev_total = (int)total;
+    if (total > 0 && rs_first > 0.0 && res_last > 0.0) rate_prev = log(res_last / rs_first) / total;
     if (ps && ps->count < ps->cap) write_pair(m, o, prec, m.x, *ps);
     if (step_net) CK(cudaMemcpyAsync(m.qold, m.q, n * sizeof(double), cudaMemcpyDeviceToDevice, m.stream));
     last_used_net = step_net;

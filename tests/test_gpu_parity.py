@@ -200,11 +200,18 @@ def test_blas_entry_points():
     assert np.array_equal(z, x * (1.0 / nrm))
 
 
-@pytest.mark.parametrize("schedule", ["levels", "syncfree", "levels16", "persistent", "pdl", "mono"])
+@pytest.mark.parametrize("schedule", ["levels", "syncfree", "levels16", "persistent", "pdl", "mono", "mono:8",
+                                      "mono:16:1", "mono:8:3"])
 def test_exact_sptrsv_every_schedule(box_mesh, schedule, monkeypatch):
-    """Every triangular-solve schedule (chosen when the device mirror is built)
-    gives the oracle's solve bit for bit in exact mode, FP64 and FP32."""
-    monkeypatch.setenv("KFUN3D_SPTRSV", schedule)
+    """Every triangular-solve schedule (chosen when the device mirror is built;
+    for the persistent sweep also lanes per row and CTAs per SM) gives the
+    oracle's solve bit for bit in exact mode, FP64 and FP32."""
+    parts = schedule.split(":")
+    monkeypatch.setenv("KFUN3D_SPTRSV", parts[0])
+    if len(parts) > 1:
+        monkeypatch.setenv("KFUN3D_SPTRSV_LANES", parts[1])
+    if len(parts) > 2:
+        monkeypatch.setenv("KFUN3D_SPTRSV_CTAS", parts[2])
     kf.set_mode("exact")
     kf.set_aoa(3.06)
     m = kf.Mesh(box_mesh(12, seed=31))
