@@ -171,7 +171,7 @@ struct DevMesh {
   unsigned trsv_pgrid = 0;        // persistent sweep grid
   unsigned trsv_mgrid = 0;        // persistent sweep grid of mode 5 (SMs x trsv_mgrid_per)
   int trsv_mgrid_per = 2;         // 512-thread CTAs per SM in mode 5 (1, 2 or 3)
-  int trsv_lanes = 16;            // lanes per row in mode 5 (8 or 16)
+  int trsv_lanes = 8;             // lanes per row in mode 5 (8 or 16)
   double *h_scal = nullptr;       // pinned host mirror of scal
   // flexible GMRES (right preconditioning) and the learned preconditioner
   double *Z = nullptr;            // [30][4N] preconditioned basis vectors
