@@ -329,6 +329,7 @@ DevMesh *kf_device(const GEOMETRY *g)
     bool morton = N >= 500000u;
     if (env && strcmp(env, "natural") == 0) morton = false;
     if (env && strcmp(env, "morton") == 0) morton = true;
+    m->spatial_order = morton;
     if (morton && N > 0) {
       const double *X = g->n->xyz->x0, *Y = g->n->xyz->x1, *Z = g->n->xyz->x2;
       double lo[3] = {X[0], Y[0], Z[0]}, hi[3] = {X[0], Y[0], Z[0]};
@@ -406,7 +407,13 @@ DevMesh *kf_device(const GEOMETRY *g)
     }
     const size_t smem = 4 * ((maxcnt + 3) & ~(size_t)3) + 24 * maxcnt;
     const char *genv = getenv("KFUN3D_GRADIENT");
-    m->grad_smem = (smem <= 200 * 1024 && !(genv && strcmp(genv, "plain") == 0)) ? (unsigned)smem : 0;
+    // staged (TMA) gradient in the mesh's own order; in the spatial order
+    // consecutive rows are already read in sequence and the plain gather is
+    // the faster one.  KFUN3D_GRADIENT=plain|tma overrides.
+    bool tma = smem <= 200 * 1024 && !m->spatial_order;
+    if (genv && strcmp(genv, "plain") == 0) tma = false;
+    if (genv && strcmp(genv, "tma") == 0) tma = smem <= 200 * 1024;
+    m->grad_smem = tma ? (unsigned)smem : 0;
   }
   // two-pass residual structure: edges sorted by n0 with n0 < n1 everywhere
   {
@@ -513,8 +520,9 @@ DevMesh *kf_device(const GEOMETRY *g)
   KF_CUDA(upload(&m->last_lower, p.last_lower.data(), p.last_lower.size()));
   KF_CUDA(upload(&m->pair_ptr, p.pair_ptr.data(), p.pair_ptr.size()));
   KF_CUDA(upload(&m->pairs, reinterpret_cast<const uint2 *>(p.pairs.data()), p.pairs.size() / 2));
-  KF_CUDA(upload(&m->lev_l, p.lev_l.data(), p.lev_l.size()));
-  KF_CUDA(upload(&m->lev_u, p.lev_u.data(), p.lev_u.size()));
+  const std::vector<uint32_t> &lev_l = p.lev_l, &lev_u = p.lev_u;
+  KF_CUDA(upload(&m->lev_l, lev_l.data(), lev_l.size()));
+  KF_CUDA(upload(&m->lev_u, lev_u.data(), lev_u.size()));
   m->lev_l_ptr = p.lev_l_ptr;
   m->lev_u_ptr = p.lev_u_ptr;
   m->nlev_l = (uint32_t)p.lev_l_ptr.size() - 1;
@@ -563,9 +571,9 @@ DevMesh *kf_device(const GEOMETRY *g)
     if (lenv && (atoi(lenv) == 8 || atoi(lenv) == 16)) m->trsv_lanes = atoi(lenv);
     std::vector<uint4> dl(N), du(N);
     for (uint32_t s = 0; s < N; s++) {
-      const uint32_t i = p.lev_l[s];
+      const uint32_t i = lev_l[s];
       dl[s] = make_uint4(i, p.ia[i], p.diag[i], 0);
-      const uint32_t k = p.lev_u[s];
+      const uint32_t k = lev_u[s];
       du[s] = make_uint4(k, p.diag[k] + 1, p.ia[k + 1], 0);
     }
     KF_CUDA(upload(&m->desc_l, dl.data(), N));

@@ -98,6 +98,7 @@ struct DevMesh {
   double4 *xyz = nullptr;         // [N] coordinates, w = 0
   uint32_t *ord = nullptr;        // [N] node visited at position p by the node-centric gathers
   uint32_t *rowof = nullptr;      // [N] position (CSR row) of each node
+  bool spatial_order = false;     // ord is the Morton order (not the mesh's own)
   uint32_t *inc_ptr = nullptr;    // [N+1] incident edges of node ord[p] (row p), in edge order
   uint32_t *inc_oth = nullptr;    // [2E] the other end point
   uint32_t *inc_edge = nullptr;   // [2E] edge index | (1u<<31 when the node is n1)

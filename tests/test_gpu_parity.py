@@ -238,8 +238,9 @@ def test_exact_sptrsv_every_schedule(box_mesh, schedule, monkeypatch):
 @pytest.mark.parametrize("order", ["natural", "morton"])
 def test_exact_kernels_any_node_order(box_mesh, order, monkeypatch):
     """The order in which node-centric kernels visit nodes (and the storage
-    order of the edge arrays that follows it) leaves every result bit-identical
-    to the oracle: each node's sums still run over its edges in edge order."""
+    order of the edge arrays that follows it) leaves every result
+    bit-identical to the oracle, through the factor and the triangular
+    solves: each node's sums still run over its edges in edge order."""
     monkeypatch.setenv("KFUN3D_NODE_ORDER", order)
     kf.set_mode("exact")
     kf.set_precision(0)
@@ -257,4 +258,9 @@ def test_exact_kernels_any_node_order(box_mesh, order, monkeypatch):
         m.fill(q, c1)
         M.fill(3.06, q, c1)
         assert np.array_equal(m.matrix()[2], M.blocks()), (order, path)
+        m.ilu()
+        M.ilu()
+        assert np.array_equal(m.matrix()[2], M.blocks()), (order, path)
+        b = np.random.default_rng(42).standard_normal(v.dofs)
+        assert np.array_equal(m.sptrsv(b), M.sptrsv(b)), (order, path)
     assert kf.last_status() == 0
