@@ -291,22 +291,27 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(G gat, O out, uint32_t rows, co
   const uint32_t lane = (uint32_t)(warp * 32) << 16;
   uint32_t phase = 0;
   const uint32_t ntiles = (rows + 127) / 128;
+  // the next tile's rows are gathered into registers while this tile's GEMMs
+  // and epilogues run (software pipeline of depth one)
+  uint4 c[K1 / 8];
+  auto gather = [&](uint32_t tile) {
+    const uint32_t r = tile * 128 + t;
+    if (tile < ntiles && r < rows) gat.load(r, c);
+    else {
+#pragma unroll
+      for (int k = 0; k < K1 / 8; k++) c[k] = make_uint4(0, 0, 0, 0);
+    }
+  };
+  gather(blockIdx.x);
   for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const uint32_t row = tile * 128 + t;
     const bool valid = row < rows;
-    {
-      uint4 c[K1 / 8];
-      if (valid) gat.load(row, c);
-      else {
 #pragma unroll
-        for (int k = 0; k < K1 / 8; k++) c[k] = make_uint4(0, 0, 0, 0);
-      }
-#pragma unroll
-      for (int k = 0; k < K1 / 8; k++) st_chunk(Xs, t, k, K1, c[k]);
-    }
+    for (int k = 0; k < K1 / 8; k++) st_chunk(Xs, t, k, K1, c[k]);
     fence_proxy_async();
     sync_tc();
     if (t == 0) gemm_issue(tm, Xs, W1s, K1, 32, &mbar, false);
+    gather(tile + gridDim.x);
     if (!mbar_try(&mbar, phase)) { atomicExch(err, 1); s_abort = 1; }
     phase ^= 1;
     fence_after_sync();
