@@ -1363,24 +1363,10 @@ __device__ __forceinline__ void trsv_row16(const uint4 d, const uint32_t *__rest
 // One row of a triangular sweep for a group of G lanes (G = 8 or 16): lane
 // (jj, r) takes blocks c0 + (G/4) p + jj, row r of each; the partial products
 // are subtracted in column order, so the arithmetic is k_trsv_level16's.
-// The column indices of a row's first step for this lane (what trsv_row_g
-// reads first), loaded ahead of the row.
-template <int G>
-__device__ __forceinline__ void trsv_cols_g(const uint4 d, const uint32_t *__restrict__ ja, int gl, uint32_t *col)
-{
-  constexpr int S = G / 4;
-  const int jj = gl >> 2;
-#pragma unroll
-  for (int p = 0; p < 4; p++) {
-    const uint32_t j = d.y + S * p + jj;
-    col[p] = j < d.z ? ja[j] : 0u;
-  }
-}
-
 template <typename T, bool UPPER, int G>
 __device__ __forceinline__ void trsv_row_g(const uint4 d, const uint32_t *__restrict__ ja, const T *__restrict__ A,
                                            const double *__restrict__ b, double *x, int base, int gl,
-                                           unsigned gmask, const uint32_t *col0)
+                                           unsigned gmask)
 {
   constexpr int S = G / 4;   // block slots per step
   const int jj = gl >> 2, r = gl & 3;
@@ -1393,7 +1379,7 @@ __device__ __forceinline__ void trsv_row_g(const uint4 d, const uint32_t *__rest
       const uint32_t j = c0 + S * p + jj;
       t[p] = 0.0;
       if (j < je) {
-        const uint32_t col = c0 == jb ? col0[p] : ja[j];
+        const uint32_t col = ja[j];
         const T *blk = A + 16 * (size_t)j + 4 * r;
         const double2 x01 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)col);
         const double2 x23 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)col + 1);
@@ -1505,40 +1491,16 @@ __global__ void __launch_bounds__(512, MINB) k_trsv_persistent_mono(const uint32
   const uint32_t H = gridDim.x * (blockDim.x / G);
   const uint32_t h = blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
   unsigned passed = 0;
-  // each group's next row descriptor and first column indices are loaded
-  // while it solves the current row (the rows of one level are independent)
   for (uint32_t l = 0; l < nl; l++) {
     const uint32_t s1 = lev_l[l + 1];
     uint32_t s = lev_l[l] + h;
-    uint4 d = s < s1 ? desc_l[s] : make_uint4(0, 0, 0, 0);
-    uint32_t col[4];
-    trsv_cols_g<G>(d, ja, gl, col);
-    for (; s < s1; s += H) {
-      const uint4 dn = s + H < s1 ? desc_l[s + H] : d;
-      uint32_t coln[4];
-      trsv_cols_g<G>(dn, ja, gl, coln);
-      trsv_row_g<T, false, G>(d, ja, A, b, x, base, gl, gmask, col);
-      d = dn;
-#pragma unroll
-      for (int k = 0; k < 4; k++) col[k] = coln[k];
-    }
+    for (; s < s1; s += H) trsv_row_g<T, false, G>(desc_l[s], ja, A, b, x, base, gl, gmask);
     if (!kf_mono_barrier(cnt, ++passed * gridDim.x, err)) return;
   }
   for (uint32_t l = 0; l < nu; l++) {
     const uint32_t s1 = lev_u[l + 1];
     uint32_t s = lev_u[l] + h;
-    uint4 d = s < s1 ? desc_u[s] : make_uint4(0, 0, 0, 0);
-    uint32_t col[4];
-    trsv_cols_g<G>(d, ja, gl, col);
-    for (; s < s1; s += H) {
-      const uint4 dn = s + H < s1 ? desc_u[s + H] : d;
-      uint32_t coln[4];
-      trsv_cols_g<G>(dn, ja, gl, coln);
-      trsv_row_g<T, true, G>(d, ja, A, b, x, base, gl, gmask, col);
-      d = dn;
-#pragma unroll
-      for (int k = 0; k < 4; k++) col[k] = coln[k];
-    }
+    for (; s < s1; s += H) trsv_row_g<T, true, G>(desc_u[s], ja, A, b, x, base, gl, gmask);
     if (l + 1 < nu && !kf_mono_barrier(cnt, ++passed * gridDim.x, err)) return;
   }
 }
