@@ -9,6 +9,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <unordered_map>
 
 #include "internal.h"
@@ -94,6 +95,24 @@ void fun3d_printf(const uint32_t c, const char *format, ...)
 
 // matrix/init.cpp:7-74 (pattern), 194-274 (level sets) and the reference's
 // fill order (src/fill.c:496-511) for the persistent-L-slot rule.
+// f(begin, end) over [0, n) split across the host's threads (sequential for
+// small n); every index is handled by exactly one call.
+template <class F> static void parallel_ranges(size_t n, F f)
+{
+  const unsigned T = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  if (n < 65536 || T == 1) {
+    f((size_t)0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t chunk = (n + T - 1) / T;
+  for (unsigned t = 0; t < T; t++) {
+    const size_t a = t * chunk, b = std::min(n, a + chunk);
+    if (a < b) th.emplace_back(f, a, b);
+  }
+  for (auto &x : th) x.join();
+}
+
 void kf_build_pattern(HostPattern &p, size_t N, size_t E, const unsigned int *n0, const unsigned int *n1)
 {
   p.n = N;
@@ -110,20 +129,24 @@ void kf_build_pattern(HostPattern &p, size_t N, size_t E, const unsigned int *n0
   }
   p.diag.assign(N, 0);
   p.lpos.assign(N + 1, 0);
-  for (size_t i = 0; i < N; i++) {
-    std::sort(p.ja.begin() + p.ia[i], p.ja.begin() + p.ia[i + 1]);
-    for (uint32_t j = p.ia[i]; j < p.ia[i + 1]; j++)
-      if (p.ja[j] == i) { p.diag[i] = j; break; }
-    p.lpos[i + 1] = p.lpos[i] + (p.diag[i] - p.ia[i]);
-  }
+  parallel_ranges(N, [&](size_t r0, size_t r1) {
+    for (size_t i = r0; i < r1; i++) {
+      std::sort(p.ja.begin() + p.ia[i], p.ja.begin() + p.ia[i + 1]);
+      for (uint32_t j = p.ia[i]; j < p.ia[i + 1]; j++)
+        if (p.ja[j] == i) { p.diag[i] = j; break; }
+    }
+  });
+  for (size_t i = 0; i < N; i++) p.lpos[i + 1] = p.lpos[i] + (p.diag[i] - p.ia[i]);
   auto find = [&](uint32_t row, uint32_t col) -> uint32_t {
     auto b = p.ja.begin() + p.ia[row], e = p.ja.begin() + p.ia[row + 1];
     auto it = std::lower_bound(b, e, col);
     return (it != e && *it == col) ? (uint32_t)(it - p.ja.begin()) : 0xffffffffu;
   };
   p.tblk.assign(p.nnz, 0);
-  for (size_t i = 0; i < N; i++)
-    for (uint32_t j = p.ia[i]; j < p.ia[i + 1]; j++) p.tblk[j] = find(p.ja[j], (uint32_t)i);
+  parallel_ranges(N, [&](size_t r0, size_t r1) {
+    for (size_t i = r0; i < r1; i++)
+      for (uint32_t j = p.ia[i]; j < p.ia[i + 1]; j++) p.tblk[j] = find(p.ja[j], (uint32_t)i);
+  });
   p.last_lower.assign(N, 0xffffffffu);
   for (size_t e = 0; e < E; e++) {
     const uint32_t a = n0[e], b = n1[e];
@@ -155,25 +178,35 @@ void kf_build_pattern(HostPattern &p, size_t N, size_t E, const unsigned int *n0
   levels(false, p.lev_u, p.lev_u_ptr);
   // ILU(0) product lists: for block (i,k) merge row i's columns up to the
   // diagonal with row k's columns up to the diagonal (= U's column k)
+  // (two passes over the rows in parallel: count, then fill in place)
   p.pair_ptr.assign(p.nnz + 1, 0);
-  p.pairs.clear();
-  p.pairs.reserve(p.nnz * 10);
-  for (size_t i = 0; i < N; i++) {
-    for (uint32_t j = p.ia[i]; j < p.ia[i + 1]; j++) {
-      const uint32_t k = p.ja[j];
-      uint32_t pl = p.ia[i], pu = p.ia[k];
-      while (pl <= p.diag[i] && pu <= p.diag[k]) {
-        const uint32_t cl = p.ja[pl], cu = p.ja[pu];
-        if (cl == cu) {
-          p.pairs.push_back(cl == i ? 0xffffffffu : p.lpos[i] + (pl - p.ia[i]));
-          p.pairs.push_back(p.tblk[pu]);
-        }
-        if (cl <= cu) pl++;
-        if (cl >= cu) pu++;
-      }
-      p.pair_ptr[j + 1] = (uint32_t)(p.pairs.size() / 2);
+  auto merge = [&](size_t i, uint32_t j, auto emit) {
+    const uint32_t k = p.ja[j];
+    uint32_t pl = p.ia[i], pu = p.ia[k];
+    while (pl <= p.diag[i] && pu <= p.diag[k]) {
+      const uint32_t cl = p.ja[pl], cu = p.ja[pu];
+      if (cl == cu) emit(cl == i ? 0xffffffffu : p.lpos[i] + (pl - p.ia[i]), p.tblk[pu]);
+      if (cl <= cu) pl++;
+      if (cl >= cu) pu++;
     }
-  }
+  };
+  parallel_ranges(N, [&](size_t r0, size_t r1) {
+    for (size_t i = r0; i < r1; i++)
+      for (uint32_t j = p.ia[i]; j < p.ia[i + 1]; j++) {
+        uint32_t c = 0;
+        merge(i, j, [&](uint32_t, uint32_t) { c++; });
+        p.pair_ptr[j + 1] = c;
+      }
+  });
+  for (size_t j = 0; j < p.nnz; j++) p.pair_ptr[j + 1] += p.pair_ptr[j];
+  p.pairs.assign(2 * (size_t)p.pair_ptr[p.nnz], 0);
+  parallel_ranges(N, [&](size_t r0, size_t r1) {
+    for (size_t i = r0; i < r1; i++)
+      for (uint32_t j = p.ia[i]; j < p.ia[i + 1]; j++) {
+        size_t o = 2 * (size_t)p.pair_ptr[j];
+        merge(i, j, [&](uint32_t a, uint32_t b) { p.pairs[o++] = a; p.pairs[o++] = b; });
+      }
+  });
 }
 
 // ----------------------------------------------------------------- matrix handle ABI

@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "kfun3d_b200.h"
@@ -354,8 +355,11 @@ void merge_runs(const uint32_t *key, const uint32_t *a, const uint32_t *ae,
   while (b != be) *out++ = *b++;
 }
 
-// Sorts [lo,hi); the result lands in lo when in_place, else in tmp.
-void index_sort(const uint32_t *key, uint32_t *lo, uint32_t *hi, uint32_t *tmp, bool in_place)
+// Sorts [lo,hi); the result lands in lo when in_place, else in tmp.  The two
+// halves are disjoint, so the top `par` levels sort them on two threads:
+// every leaf and every merge is the same as in the sequential recursion, so
+// is the permutation.
+void index_sort(const uint32_t *key, uint32_t *lo, uint32_t *hi, uint32_t *tmp, bool in_place, int par = 0)
 {
   if (hi - lo <= LEAF) {
     leaf_sort(key, lo, hi);
@@ -364,13 +368,45 @@ void index_sort(const uint32_t *key, uint32_t *lo, uint32_t *hi, uint32_t *tmp, 
   }
   uint32_t *mid = lo + (hi - lo) / 2;
   uint32_t *tmid = tmp + (mid - lo), *thi = tmp + (hi - lo);
-  index_sort(key, lo, mid, tmp, !in_place);
-  index_sort(key, mid, hi, tmid, !in_place);
+  if (par > 0) {
+    std::thread left([=] { index_sort(key, lo, mid, tmp, !in_place, par - 1); });
+    index_sort(key, mid, hi, tmid, !in_place, par - 1);
+    left.join();
+  } else {
+    index_sort(key, lo, mid, tmp, !in_place);
+    index_sort(key, mid, hi, tmid, !in_place);
+  }
   if (in_place) merge_runs(key, tmp, tmid, tmid, thi, lo);
   else merge_runs(key, lo, mid, mid, hi, tmp);
 }
 
+int sort_levels()
+{
+  unsigned t = std::thread::hardware_concurrency();
+  int lv = 0;
+  while ((1u << (lv + 1)) <= t && lv < 6) lv++;
+  return lv;
+}
+
 template <class T> T *alloc(size_t n) { return (T *)calloc(n ? n : 1, sizeof(T)); }
+
+// f(begin, end) over [0, n) split across the host's threads (sequential for
+// small n); every index is handled by exactly one call.
+template <class F> void parallel_ranges(size_t n, F f)
+{
+  const unsigned T = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  if (n < 65536 || T == 1) {
+    f((size_t)0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t chunk = (n + T - 1) / T;
+  for (unsigned t = 0; t < T; t++) {
+    const size_t a = t * chunk, b = std::min(n, a + chunk);
+    if (a < b) th.emplace_back(f, a, b);
+  }
+  for (auto &x : th) x.join();
+}
 
 }  // namespace
 
@@ -397,7 +433,7 @@ extern "C" GEOMETRY *kfun3d_setup_load(const char *path)
   rd.f64(nbuf.data(), 4 * E);
   std::vector<uint32_t> order(E), tmp(E);
   for (size_t i = 0; i < E; i++) order[i] = (uint32_t)i;
-  if (E) index_sort(ebuf.data(), order.data(), order.data() + E, tmp.data(), true);
+  if (E) index_sort(ebuf.data(), order.data(), order.data() + E, tmp.data(), true, E > 100000 ? sort_levels() : 0);
   g->e = alloc<struct etbl>(1);
   g->e->sz = E;
   g->e->eptr = alloc<struct edge>(1);
@@ -501,106 +537,135 @@ extern "C" GEOMETRY *kfun3d_setup_load(const char *path)
     g->t->i[c] = sum;
   }
 
-  // least-squares weights (src/weights.c:299-398)
+  // least-squares weights (src/weights.c:299-398).  The reference's edge
+  // loops add into both end points; here every node gathers over its edges in
+  // edge order (the same additions in the same order) and the nodes run in
+  // parallel.
   {
     const unsigned int *n0 = g->e->eptr->n0, *n1 = g->e->eptr->n1;
     const double *X = g->n->xyz->x0, *Y = g->n->xyz->x1, *Z = g->n->xyz->x2;
+    std::vector<uint32_t> iptr(N + 1, 0), inc(2 * E);
+    for (size_t e = 0; e < E; e++) { iptr[n0[e] + 1]++; iptr[n1[e] + 1]++; }
+    for (size_t i = 0; i < N; i++) iptr[i + 1] += iptr[i];
+    {
+      std::vector<uint32_t> pos(iptr.begin(), iptr.end() - 1);
+      for (size_t e = 0; e < E; e++) { inc[pos[n0[e]]++] = (uint32_t)e; inc[pos[n1[e]]++] = (uint32_t)e; }
+    }
     std::vector<double> w(7 * N, 0.0);
-    for (size_t e = 0; e < E; e++) {                 // weights.c:237-297
-      const size_t a = n0[e], b = n1[e];
-      double rx = X[b] - X[a], ry = Y[b] - Y[a], rz = Z[b] - Z[a];
-      w[7 * a + 0] += rx * rx; w[7 * a + 1] += rx * ry; w[7 * a + 2] += rx * rz;
-      rx = X[a] - X[b]; ry = Y[a] - Y[b]; rz = Z[a] - Z[b];
-      w[7 * b + 0] += rx * rx; w[7 * b + 1] += rx * ry; w[7 * b + 2] += rx * rz;
-    }
-    for (size_t i = 0; i < N; i++) {
-      w[7 * i + 0] = std::sqrt(w[7 * i + 0]);
-      w[7 * i + 1] /= w[7 * i + 0];
-      w[7 * i + 2] /= w[7 * i + 0];
-    }
-    for (size_t e = 0; e < E; e++) {                 // weights.c:173-232
-      const size_t a = n0[e], b = n1[e];
-      const double dx = X[b] - X[a], dy = Y[b] - Y[a], dz = Z[b] - Z[a];
-      double d = w[7 * a + 1] / w[7 * a + 0];
-      double d_ = dy - dx * d;
-      w[7 * a + 3] += d_ * d_;
-      w[7 * a + 4] += d_ * dz;
-      d = w[7 * b + 1] / w[7 * b + 0];
-      d_ = -dy + dx * d;
-      w[7 * b + 3] += d_ * d_;
-      w[7 * b + 4] -= d_ * dz;
-    }
-    for (size_t i = 0; i < N; i++) {
-      w[7 * i + 3] = std::sqrt(w[7 * i + 3]);
-      w[7 * i + 4] /= w[7 * i + 3];
-    }
-    for (size_t e = 0; e < E; e++) {                 // weights.c:102-170
-      const size_t a = n0[e], b = n1[e];
-      const double dx = X[b] - X[a], dy = Y[b] - Y[a], dz = Z[b] - Z[a];
-      {
-        const double d0 = w[7 * a + 1] / w[7 * a + 0];
-        const double d0_ = dy - dx * d0;
-        const double d1 = w[7 * a + 2] / w[7 * a + 0];
-        const double d1_ = dz - dx * d1;
-        const double d2 = w[7 * a + 4] / w[7 * a + 3];
-        const double d2_ = d1_ - d2 * d0_;
-        w[7 * a + 5] += d2_ * d2_;
+    parallel_ranges(N, [&](size_t r0, size_t r1) {     // weights.c:237-297
+      for (size_t i = r0; i < r1; i++)
+        for (uint32_t k = iptr[i]; k < iptr[i + 1]; k++) {
+          const size_t e = inc[k], a = n0[e], b = n1[e];
+          double rx, ry, rz;
+          if (a == i) { rx = X[b] - X[a]; ry = Y[b] - Y[a]; rz = Z[b] - Z[a]; }
+          else { rx = X[a] - X[b]; ry = Y[a] - Y[b]; rz = Z[a] - Z[b]; }
+          w[7 * i + 0] += rx * rx; w[7 * i + 1] += rx * ry; w[7 * i + 2] += rx * rz;
+        }
+    });
+    parallel_ranges(N, [&](size_t r0, size_t r1) {
+      for (size_t i = r0; i < r1; i++) {
+        w[7 * i + 0] = std::sqrt(w[7 * i + 0]);
+        w[7 * i + 1] /= w[7 * i + 0];
+        w[7 * i + 2] /= w[7 * i + 0];
       }
-      {
-        const double d0 = w[7 * b + 1] / w[7 * b + 0];
-        const double d0_ = -dy + dx * d0;
-        const double d1 = w[7 * b + 2] / w[7 * b + 0];
-        const double d1_ = -dz + dx * d1;
-        const double d2 = w[7 * b + 4] / w[7 * b + 3];
-        const double d2_ = d1_ - d2 * d0_;
-        w[7 * b + 5] += d2_ * d2_;
+    });
+    parallel_ranges(N, [&](size_t r0, size_t r1) {     // weights.c:173-232
+      for (size_t i = r0; i < r1; i++)
+        for (uint32_t k = iptr[i]; k < iptr[i + 1]; k++) {
+          const size_t e = inc[k], a = n0[e], b = n1[e];
+          const double dx = X[b] - X[a], dy = Y[b] - Y[a], dz = Z[b] - Z[a];
+          if (a == i) {
+            const double d = w[7 * a + 1] / w[7 * a + 0];
+            const double d_ = dy - dx * d;
+            w[7 * a + 3] += d_ * d_;
+            w[7 * a + 4] += d_ * dz;
+          } else {
+            const double d = w[7 * b + 1] / w[7 * b + 0];
+            const double d_ = -dy + dx * d;
+            w[7 * b + 3] += d_ * d_;
+            w[7 * b + 4] -= d_ * dz;
+          }
+        }
+    });
+    parallel_ranges(N, [&](size_t r0, size_t r1) {
+      for (size_t i = r0; i < r1; i++) {
+        w[7 * i + 3] = std::sqrt(w[7 * i + 3]);
+        w[7 * i + 4] /= w[7 * i + 3];
       }
-    }
-    for (size_t i = 0; i < N; i++) {                 // weights.c:335-366
-      double *wi = &w[7 * i];
-      wi[5] = std::sqrt(wi[5]);
-      const double sw00 = wi[0] * wi[0], sw11 = wi[3] * wi[3], sw22 = wi[5] * wi[5];
-      const double w00 = 1.0 / sw00, w11 = 1.0 / sw11, w22 = 1.0 / sw22;
-      const double w01 = wi[1] / wi[0], w02 = wi[2] / wi[0], w12 = wi[4] / wi[3];
-      double m0 = wi[1] * wi[4];
-      m0 -= wi[2] * wi[3];
-      const double m1 = wi[0] * wi[3] * sw22;
-      const double w33 = m0 / m1;
-      wi[0] = w00; wi[3] = w11; wi[5] = w22; wi[1] = w01; wi[2] = w02; wi[4] = w12; wi[6] = w33;
-    }
+    });
+    parallel_ranges(N, [&](size_t r0, size_t r1) {     // weights.c:102-170
+      for (size_t i = r0; i < r1; i++)
+        for (uint32_t k = iptr[i]; k < iptr[i + 1]; k++) {
+          const size_t e = inc[k], a = n0[e], b = n1[e];
+          const double dx = X[b] - X[a], dy = Y[b] - Y[a], dz = Z[b] - Z[a];
+          if (a == i) {
+            const double d0 = w[7 * a + 1] / w[7 * a + 0];
+            const double d0_ = dy - dx * d0;
+            const double d1 = w[7 * a + 2] / w[7 * a + 0];
+            const double d1_ = dz - dx * d1;
+            const double d2 = w[7 * a + 4] / w[7 * a + 3];
+            const double d2_ = d1_ - d2 * d0_;
+            w[7 * a + 5] += d2_ * d2_;
+          } else {
+            const double d0 = w[7 * b + 1] / w[7 * b + 0];
+            const double d0_ = -dy + dx * d0;
+            const double d1 = w[7 * b + 2] / w[7 * b + 0];
+            const double d1_ = -dz + dx * d1;
+            const double d2 = w[7 * b + 4] / w[7 * b + 3];
+            const double d2_ = d1_ - d2 * d0_;
+            w[7 * b + 5] += d2_ * d2_;
+          }
+        }
+    });
+    parallel_ranges(N, [&](size_t r0, size_t r1) {     // weights.c:335-366
+      for (size_t i = r0; i < r1; i++) {
+        double *wi = &w[7 * i];
+        wi[5] = std::sqrt(wi[5]);
+        const double sw00 = wi[0] * wi[0], sw11 = wi[3] * wi[3], sw22 = wi[5] * wi[5];
+        const double w00 = 1.0 / sw00, w11 = 1.0 / sw11, w22 = 1.0 / sw22;
+        const double w01 = wi[1] / wi[0], w02 = wi[2] / wi[0], w12 = wi[4] / wi[3];
+        double m0 = wi[1] * wi[4];
+        m0 -= wi[2] * wi[3];
+        const double m1 = wi[0] * wi[3] * sw22;
+        const double w33 = m0 / m1;
+        wi[0] = w00; wi[3] = w11; wi[5] = w22; wi[1] = w01; wi[2] = w02; wi[4] = w12; wi[6] = w33;
+      }
+    });
     g->e->w = alloc<struct weights>(1);
     g->e->w->w0 = alloc<struct xyz>(1);
     g->e->w->w1 = alloc<struct xyz>(1);
     double *t0x = alloc<double>(E), *t0y = alloc<double>(E), *t0z = alloc<double>(E);
     double *t1x = alloc<double>(E), *t1y = alloc<double>(E), *t1z = alloc<double>(E);
-    for (size_t e = 0; e < E; e++) {                 // weights.c:9-100
-      const size_t a = n0[e], b = n1[e];
-      const double dx = X[b] - X[a], dy = Y[b] - Y[a], dz = Z[b] - Z[a];
-      {
-        const double *wa = &w[7 * a];
-        double c0 = -dx * wa[1] + dy;
-        double c1 = -dx * wa[2] + dz;
-        c1 = -wa[4] * c0 + c1;
-        double tx = wa[3] * wa[1] * c0;
-        tx = dx * wa[0] - tx;
-        tx += wa[6] * c1;
-        double ty = wa[4] * wa[5] * c1;
-        ty = wa[3] * c0 - ty;
-        t0x[e] = tx; t0y[e] = ty; t0z[e] = wa[5] * c1;
+    parallel_ranges(E, [&](size_t r0, size_t r1) {     // weights.c:9-100
+      for (size_t e = r0; e < r1; e++) {
+        const size_t a = n0[e], b = n1[e];
+        const double dx = X[b] - X[a], dy = Y[b] - Y[a], dz = Z[b] - Z[a];
+        {
+          const double *wa = &w[7 * a];
+          double c0 = -dx * wa[1] + dy;
+          double c1 = -dx * wa[2] + dz;
+          c1 = -wa[4] * c0 + c1;
+          double tx = wa[3] * wa[1] * c0;
+          tx = dx * wa[0] - tx;
+          tx += wa[6] * c1;
+          double ty = wa[4] * wa[5] * c1;
+          ty = wa[3] * c0 - ty;
+          t0x[e] = tx; t0y[e] = ty; t0z[e] = wa[5] * c1;
+        }
+        {
+          const double *wb = &w[7 * b];
+          double c0 = dx * wb[1] - dy;
+          double c1 = dx * wb[2] - dz;
+          c1 = -wb[4] * c0 + c1;
+          double tx = wb[3] * wb[1] * c0;
+          tx = -dx * wb[0] - tx;
+          tx += wb[6] * c1;
+          double ty = wb[4] * wb[5] * c1;
+          ty = wb[3] * c0 - ty;
+          t1x[e] = tx; t1y[e] = ty; t1z[e] = wb[5] * c1;
+        }
       }
-      {
-        const double *wb = &w[7 * b];
-        double c0 = dx * wb[1] - dy;
-        double c1 = dx * wb[2] - dz;
-        c1 = -wb[4] * c0 + c1;
-        double tx = wb[3] * wb[1] * c0;
-        tx = -dx * wb[0] - tx;
-        tx += wb[6] * c1;
-        double ty = wb[4] * wb[5] * c1;
-        ty = wb[3] * c0 - ty;
-        t1x[e] = tx; t1y[e] = ty; t1z[e] = wb[5] * c1;
-      }
-    }
+    });
     g->e->w->w0->x0 = t0x; g->e->w->w0->x1 = t0y; g->e->w->w0->x2 = t0z;
     g->e->w->w1->x0 = t1x; g->e->w->w1->x1 = t1y; g->e->w->w1->x2 = t1z;
   }

@@ -264,3 +264,26 @@ def test_exact_kernels_any_node_order(box_mesh, order, monkeypatch):
         b = np.random.default_rng(42).standard_normal(v.dofs)
         assert np.array_equal(m.sptrsv(b), M.sptrsv(b)), (order, path)
     assert kf.last_status() == 0
+
+
+def test_exact_factor_on_a_mesh_built_by_the_threaded_host_paths(box_mesh):
+    """42^3 (74,088 rows) builds the block pattern, the level sets and the
+    ILU(0) product lists on several host threads; factor and solves must
+    still equal the oracle's bit for bit."""
+    kf.set_mode("exact")
+    kf.set_precision(0)
+    kf.set_aoa(3.06)
+    m = kf.Mesh(box_mesh(42, seed=13))
+    v = m.view
+    q = seeded_state(v.q.copy(), 13)
+    cdt = port.timestep(m.g, v.nnodes, 40.0, q)
+    M = port.Matrix(m.g)
+    for step in range(2):
+        m.fill(q, cdt)
+        M.fill(3.06, q, cdt)
+        m.ilu()
+        M.ilu()
+        assert np.array_equal(m.matrix()[2], M.blocks()), step
+        b = np.random.default_rng(13 + step).standard_normal(v.dofs)
+        assert np.array_equal(m.sptrsv(b), M.sptrsv(b)), step
+    assert kf.last_status() == 0

@@ -50,8 +50,10 @@ def test_generator_seed_changes_mesh(box_mesh):
 
 
 @pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
-@pytest.mark.parametrize("n,seed", [(5, 0), (11, 9)])
+@pytest.mark.parametrize("n,seed", [(5, 0), (11, 9), (42, 13)])
 def test_loader_bit_identical_to_reference_setup(box_mesh, n, seed):
+    """42^3 (74,088 nodes) takes the loader's multi-threaded paths (index
+    sort, least-squares weights), which must give the same bits."""
     p = box_mesh(n, seed=seed)
     a = kf.Mesh(p).view
     b = ref.RefMesh(p, 3.0, 1).view
