@@ -609,6 +609,16 @@ DevMesh *kf_device(const GEOMETRY *g)
       const uint32_t k = lev_u[s];
       du[s] = make_uint4(k, p.diag[k] + 1, p.ia[k + 1], 0);
     }
+    // within a level the rows are independent: longest first, so that the
+    // groups that take a second row take short ones (less waiting at the
+    // level barrier)
+    auto by_length = [](std::vector<uint4> &d, const std::vector<uint32_t> &ptr) {
+      for (size_t l = 0; l + 1 < ptr.size(); l++)
+        std::stable_sort(d.begin() + ptr[l], d.begin() + ptr[l + 1],
+                         [](const uint4 &a, const uint4 &b) { return a.z - a.y > b.z - b.y; });
+    };
+    by_length(dl, p.lev_l_ptr);
+    by_length(du, p.lev_u_ptr);
     KF_CUDA(upload(&m->desc_l, dl.data(), N));
     KF_CUDA(upload(&m->desc_u, du.data(), N));
     // triangular-solve schedule: "pdl" (default: one launch per level with
