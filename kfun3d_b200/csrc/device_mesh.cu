@@ -600,8 +600,8 @@ DevMesh *kf_device(const GEOMETRY *g)
     const char *cenv = getenv("KFUN3D_SPTRSV_CTAS");
     if (cenv && (atoi(cenv) >= 1 && atoi(cenv) <= 3)) m->trsv_mgrid_per = atoi(cenv);
     m->trsv_mgrid = (unsigned)nsm * (unsigned)m->trsv_mgrid_per;
-    const char *lenv = getenv("KFUN3D_SPTRSV_LANES");   // rows per 8 lanes (default) or 16
-    if (lenv && (atoi(lenv) == 8 || atoi(lenv) == 16)) m->trsv_lanes = atoi(lenv);
+    const char *lenv = getenv("KFUN3D_SPTRSV_LANES");   // lanes per row: 8 (default), 4 or 16
+    if (lenv && (atoi(lenv) == 4 || atoi(lenv) == 8 || atoi(lenv) == 16)) m->trsv_lanes = atoi(lenv);
     std::vector<uint4> dl(N), du(N);
     for (uint32_t s = 0; s < N; s++) {
       const uint32_t i = lev_l[s];

@@ -1905,22 +1905,21 @@ void sptrsv(DevMesh &m, const double *b, double *x, int precision)
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const void *fn;
-    const bool g8 = m.trsv_lanes == 8;
-    switch (m.trsv_mgrid_per) {
-      case 1: fn = precision == 0 ? (g8 ? (const void *)k_trsv_persistent_mono<double, 1, 8>
-                                        : (const void *)k_trsv_persistent_mono<double, 1, 16>)
-                                  : (g8 ? (const void *)k_trsv_persistent_mono<float, 1, 8>
-                                        : (const void *)k_trsv_persistent_mono<float, 1, 16>); break;
-      case 3: fn = precision == 0 ? (g8 ? (const void *)k_trsv_persistent_mono<double, 3, 8>
-                                        : (const void *)k_trsv_persistent_mono<double, 3, 16>)
-                                  : (g8 ? (const void *)k_trsv_persistent_mono<float, 3, 8>
-                                        : (const void *)k_trsv_persistent_mono<float, 3, 16>); break;
-      default: fn = precision == 0 ? (g8 ? (const void *)k_trsv_persistent_mono<double, 2, 8>
-                                         : (const void *)k_trsv_persistent_mono<double, 2, 16>)
-                                   : (g8 ? (const void *)k_trsv_persistent_mono<float, 2, 8>
-                                         : (const void *)k_trsv_persistent_mono<float, 2, 16>); break;
-    }
+    // instance for (precision, CTAs per SM, lanes per row)
+    auto pick = [&](auto ctas) -> const void * {
+      constexpr int C = decltype(ctas)::value;
+      switch (m.trsv_lanes) {
+        case 4: return precision == 0 ? (const void *)k_trsv_persistent_mono<double, C, 4>
+                                      : (const void *)k_trsv_persistent_mono<float, C, 4>;
+        case 16: return precision == 0 ? (const void *)k_trsv_persistent_mono<double, C, 16>
+                                       : (const void *)k_trsv_persistent_mono<float, C, 16>;
+        default: return precision == 0 ? (const void *)k_trsv_persistent_mono<double, C, 8>
+                                       : (const void *)k_trsv_persistent_mono<float, C, 8>;
+      }
+    };
+    const void *fn = m.trsv_mgrid_per == 1 ? pick(std::integral_constant<int, 1>())
+                   : m.trsv_mgrid_per == 3 ? pick(std::integral_constant<int, 3>())
+                                           : pick(std::integral_constant<int, 2>());
     const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
     if (e != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e));
     kf_count_launch();
