@@ -103,3 +103,29 @@ def test_learned_ablation(box_mesh, tmp_path, capsys):
     assert np.mean(losses[-50:]) < z          # the network learned something about the pairs
     assert np.allclose(_forces(h_net), _forces(h_ilu), rtol=1e-6, atol=0)
     assert st_net["gmres_its"] <= 1.25 * st_ilu["gmres_its"]
+
+
+def test_committed_network_ablation(box_mesh, capsys):
+    """The shipped network (trained on 128 seeded 40^3 meshes by
+    kfun3d_b200.train_mpnn) against the same flexible solve without it, on a
+    held-out 40^3 mesh (bump 0.12, 4.5 degrees).  Reports the gain; requires
+    the same converged state and an overhead the fallback keeps under 25 %."""
+    import os
+    from kfun3d_b200 import learned
+    w = os.path.join(os.path.dirname(kf.__file__), "weights", "mpnn_box40.npy")
+    net = learned.Network.load(w)
+    kf.set_precision(1)
+    kf.set_aoa(4.5)
+    m = kf.Mesh(box_mesh(40, seed=77, bump=0.12))
+    q0 = m.view.q.copy()
+    t0, h0, s0 = m.time_solve_flexible(**P)
+    m.view.q[:] = q0
+    t1, h1, s1 = m.time_solve_flexible(net=net, **P)
+    kf.set_precision(0)
+    with capsys.disabled():
+        print(f"\nshipped network, held-out 40^3: without {s0['gmres_its']} its {t0:.4f} s; with "
+              f"{s1['gmres_its']} its {t1:.4f} s ({100 * (1 - s1['gmres_its'] / s0['gmres_its']):+.1f}% iterations, "
+              f"{100 * (1 - t1 / t0):+.1f}% time); {s1}")
+    assert h1[0]["fnorm"] / h1[-1]["fnorm"] >= 1e7
+    assert np.allclose(_forces(h1), _forces(h0), rtol=1e-6, atol=0)
+    assert t1 <= 1.25 * t0
