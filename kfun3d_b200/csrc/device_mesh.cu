@@ -420,12 +420,16 @@ DevMesh *kf_device(const GEOMETRY *g)
     for (uint32_t e = 0; e < E; e++) {
       const uint32_t a = n0[e], b = n1[e];
       uint32_t k = pos[a]++;
-      oth[k] = b; edg[k] = e; blk[k] = find(a, b);
+      oth[k] = b; edg[k] = e;
       for (int c = 0; c < 3; c++) w[c * wst + k] = w0[c][e];
       k = pos[b]++;
-      oth[k] = a; edg[k] = e | 0x80000000u; blk[k] = find(b, a);
+      oth[k] = a; edg[k] = e | 0x80000000u;
       for (int c = 0; c < 3; c++) w[c * wst + k] = w1[c][e];
     }
+    parallel_ranges(N, [&](size_t r0, size_t r1) {   // block of (node, other), row by row
+      for (size_t row = r0; row < r1; row++)
+        for (uint32_t k = ptr[row]; k < ptr[row + 1]; k++) blk[k] = find(ord[row], oth[k]);
+    });
     KF_CUDA(upload(&m->inc_ptr, ptr.data(), N + 1));
     KF_CUDA(upload(&m->inc_oth, oth.data(), oth.size()));
     KF_CUDA(upload(&m->inc_edge, edg.data(), ninc));
