@@ -131,6 +131,27 @@ int kfun3d_get_mode(void);
 /* Preconditioner precision: 0 = FP64 (the reference), 1 = FP32 Jacobian
    blocks, FP32 ILU(0) factors and FP32-block triangular solves. */
 void kfun3d_set_precision(int p);
+/* Elimination order of ILU(0) and the triangular solves.
+   0 = the mesh's node numbering (the reference: matrix/matrix.cpp factors
+       rows in node order);
+   1 = spatial: rows and columns renumbered by a sweep of the node
+       coordinates (the mesh cut into one column per SM along (1,1,1),
+       column by column, ascending x + y + z within a column; P A P^T is
+       factored, x = P^T (LU)^-1 P b).  Same Jacobian blocks and sparsity, a different
+       (and on randomly numbered meshes a much stronger) preconditioner; not
+       a parity path.  Built on first use per mesh.  While it is active
+       kfun3d_matrix_read(blocks) and kfun3d_sptrsv_device_noalloc return
+       KFUN3D_ERR_ARG.
+   KFUN3D_ILU_PERM in the environment, read when the order is built:
+   "sweep" renumbers by ascending x + y + z over the whole mesh, "morton" by
+   the Morton order of the coordinates;
+   "identity" keeps the mesh numbering through the same renumbering code
+   (a test hook). */
+void kfun3d_set_ilu_order(int order);
+int kfun3d_get_ilu_order(void);
+/* Row of every node (rank[node], N entries) in the spatial order built for
+   this GEOMETRY; returns N, or -1 when it has not been built. */
+long kfun3d_ilu_rank(const GEOMETRY *g, unsigned int *rank);
 /* 1: residual reconstructed without gradients (first-order flux). */
 void kfun3d_set_first_order(int on);
 /* 0 silences Kernel()'s per-step report. */
@@ -172,7 +193,8 @@ void kfun3d_initial_guess(GEOMETRY *g);
 /* Synthetic Kuhn-box mesh writer: n^3 nodes on [0,1]^3, each hex split into
    six tets, interior nodes jittered by U(+-jitter h), bottom face a slip wall
    with a Gaussian bump height*exp(-r^2/(2 sigma^2))*(1-z), other faces far
-   field, optional seeded random node numbering.  Returns 0 on success. */
+   field, node numbering by permute: 0 the lattice order, 1 seeded random,
+   2 Morton order of the lattice.  Returns 0 on success. */
 typedef struct {
   unsigned int n;
   double bump_height;

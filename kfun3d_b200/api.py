@@ -86,6 +86,9 @@ def lib():
         "kfun3d_set_mode": (None, [C.c_int]),
         "kfun3d_get_mode": (C.c_int, []),
         "kfun3d_set_precision": (None, [C.c_int]),
+        "kfun3d_set_ilu_order": (None, [C.c_int]),
+        "kfun3d_get_ilu_order": (C.c_int, []),
+        "kfun3d_ilu_rank": (C.c_long, [G, C.POINTER(C.c_uint)]),
         "kfun3d_set_first_order": (None, [C.c_int]),
         "kfun3d_set_verbose": (None, [C.c_int]),
         "kfun3d_default_params": (None, [P(SolverParams)]),
@@ -169,6 +172,18 @@ def set_precision(p):
     if isinstance(p, str):
         p = {"fp64": 0, "fp32": 1, "mixed": 1}[p]
     lib().kfun3d_set_precision(int(p))
+
+
+def set_ilu_order(order):
+    """Elimination order of ILU(0): 0 / "mesh" (the reference) or 1 / "spatial"
+    (the block pattern renumbered by a sweep of the node coordinates; not a parity path)."""
+    if isinstance(order, str):
+        order = {"mesh": 0, "spatial": 1}[order]
+    lib().kfun3d_set_ilu_order(int(order))
+
+
+def get_ilu_order():
+    return lib().kfun3d_get_ilu_order()
 
 
 def set_first_order(on):
@@ -306,6 +321,13 @@ class Mesh:
             raise RuntimeError(f"kfun3d_solve failed: {last_error()}")
         return [dict(step=h.step, gmres_its=h.gmres_its, cfl=h.cfl, fnorm=h.fnorm, lift=h.lift,
                      drag=h.drag, momn=h.momn, seconds=h.seconds) for h in hist[:n]]
+
+    def ilu_rank(self):
+        """Row of every node in the spatial ILU order (built on first use of order 1)."""
+        rank = np.zeros(self.view.nnodes, dtype=np.uint32)
+        if lib().kfun3d_ilu_rank(self.g, rank.ctypes.data_as(C.POINTER(C.c_uint))) < 0:
+            raise RuntimeError(f"kfun3d_ilu_rank failed: {last_error()}")
+        return rank.astype(np.int64)
 
     def time_kernel(self, which, reps=10):
         names = {"flux": 0, "timestep": 1, "fill": 2, "ilu": 3, "sptrsv": 4, "gmres_iter": 5,

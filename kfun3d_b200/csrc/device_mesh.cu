@@ -24,6 +24,7 @@ int g_abort = 1;
 double g_aoa = 3.0;
 int g_mode = KFUN3D_MODE_EXACT;
 int g_precision = 0;
+int g_ilu_order = 0;
 int g_first_order = 0;
 std::atomic<unsigned long long> g_launches{0};
 }  // namespace
@@ -45,6 +46,7 @@ void kf_set_error(int code, const char *msg)
 
 int kf_mode() { return g_mode; }
 int kf_precision() { return g_precision; }
+int kf_ilu_order() { return g_ilu_order; }
 int kf_first_order() { return g_first_order; }
 void kf_count_launch(unsigned n) { g_launches += n; }
 void kfun3d_reset_launch_count_by(unsigned long long n) { g_launches -= n; }
@@ -71,6 +73,8 @@ void kfun3d_get_freestream(double *u, double *v)
 void kfun3d_set_mode(int mode) { g_mode = mode == KFUN3D_MODE_FAST ? KFUN3D_MODE_FAST : KFUN3D_MODE_EXACT; }
 int kfun3d_get_mode(void) { return g_mode; }
 void kfun3d_set_precision(int p) { g_precision = p ? 1 : 0; }
+void kfun3d_set_ilu_order(int o) { g_ilu_order = o ? 1 : 0; }
+int kfun3d_get_ilu_order(void) { return g_ilu_order; }
 void kfun3d_set_first_order(int on) { g_first_order = on ? 1 : 0; }
 void kfun3d_set_verbose(int on) { g_kf_verbose = on; }
 unsigned long long kfun3d_launch_count(void) { return g_launches; }
@@ -270,10 +274,13 @@ template <class T> static cudaError_t upload(T **dst, const T *src, size_t n)
   return cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
 }
 
+void kf_ilu_release(DevMesh &m);
+
 static void release_device(MatrixHandle *h)
 {
   DevMesh *m = h->dev;
   if (!m) return;
+  kf_ilu_release(*m);   // the spatial ILU set's arrays; the reference set's fields are back in place
   void *ptrs[] = {m->col, m->egeo, m->xyz, m->inc_ptr, m->inc_oth, m->inc_edge, m->inc_blk, m->inc_w, m->wf_nodes,
                   m->wf_n, m->s_n, m->f_n, m->bnd_of, m->bnd_node, m->bnd_ptr, m->bnd_ent, m->ia, m->ja,
                   m->diag, m->tblk, m->lpos, m->last_lower, m->lev_l, m->lev_u, m->A, m->lslot, m->dinv,
@@ -650,6 +657,19 @@ DevMesh *kf_device(const GEOMETRY *g)
     m->use_graphs = !(genv && strcmp(genv, "0") == 0);
   }
   KF_CUDA(cudaMallocHost(&m->h_scal, 256 * sizeof(double)));
+  {
+    IluSet &s0 = m->iset[0];
+    s0.ia = m->ia; s0.ja = m->ja; s0.diag = m->diag; s0.tblk = m->tblk; s0.lpos = m->lpos;
+    s0.last_lower = m->last_lower; s0.pair_ptr = m->pair_ptr; s0.pairs = m->pairs;
+    s0.lev_l = m->lev_l; s0.lev_u = m->lev_u; s0.lev_ptr_d = m->lev_ptr_d;
+    s0.lev_l_ptr = m->lev_l_ptr; s0.lev_u_ptr = m->lev_u_ptr;
+    s0.nlev_l = m->nlev_l; s0.nlev_u = m->nlev_u;
+    s0.desc_l = m->desc_l; s0.desc_u = m->desc_u;
+    s0.trsv_mode = m->trsv_mode;
+    s0.fill_blk = m->inc_blk; s0.fill_diag = m->diag; s0.fill_last = m->last_lower; s0.fill_lpos = m->lpos;
+    s0.valid = true;
+    m->fill_blk = m->inc_blk; m->fill_diag = m->diag; m->fill_last = m->last_lower; m->fill_lpos = m->lpos;
+  }
   KF_CUDA(cudaDeviceSynchronize());
   return m;
 }

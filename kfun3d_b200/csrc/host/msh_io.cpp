@@ -139,14 +139,29 @@ extern "C" int kfun3d_mesh_generate(const char *path, const kfun3d_mesh_spec *sp
         X[nid(i, j, k)] = p;
       }
 
-  // node permutation (Fisher-Yates)
+  // node numbering: the lattice order (permute = 0), a seeded random
+  // permutation (1, Fisher-Yates) or the Morton order of the lattice (2)
   std::vector<uint32_t> perm(N);
   for (long i = 0; i < N; i++) perm[i] = (uint32_t)i;
-  if (spec->permute)
+  if (spec->permute == 1)
     for (long i = N - 1; i > 0; i--) {
       long r = (long)(rng.next() % (uint64_t)(i + 1));
       std::swap(perm[i], perm[r]);
     }
+  if (spec->permute == 2) {
+    auto spread = [](uint64_t v) {
+      uint64_t r = 0;
+      for (int b = 0; b < 21; b++) r |= ((v >> b) & 1ull) << (3 * b);
+      return r;
+    };
+    std::vector<std::pair<uint64_t, uint32_t>> key(N);
+    for (long k = 0; k < n; k++)
+      for (long j = 0; j < n; j++)
+        for (long i = 0; i < n; i++)
+          key[nid(i, j, k)] = {spread(i) | spread(j) << 1 | spread(k) << 2, (uint32_t)nid(i, j, k)};
+    std::sort(key.begin(), key.end());
+    for (long r = 0; r < N; r++) perm[key[r].second] = (uint32_t)r;
+  }
 
   // median-dual face vectors, accumulated per (node, direction) slot
   std::vector<V3> S(7 * N, V3{0, 0, 0});

@@ -1,0 +1,475 @@
+// kfun3d_b200: ILU(0) in a spatial ordering (option for the fast forms).
+//
+// With a random node numbering (the meshes here are numbered at random, as
+// the reference's inputs may be) ILU(0) of the Jacobian in the mesh's own
+// order is weak: on the 120^3 box the solve needs 1556 GMRES iterations
+// against 761 when rows and columns are eliminated in a spatially coherent
+// order.  Set 1 renumbers the block pattern by a spatial order of the nodes:
+// the matrix becomes P A P^T, ILU(0) factors that (same sparsity, different
+// elimination order) and a triangular solve runs x = P^T (L U)^-1 P b.  The
+// Jacobian blocks themselves are unchanged; the fill writes them into the
+// renumbered pattern.  Not a parity path: the reference factors in its own
+// order, which stays the default (kfun3d_set_ilu_order(0)).
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "internal.h"
+
+namespace {
+
+template <class T> cudaError_t upload(T **dst, const T *src, size_t n)
+{
+  cudaError_t e = cudaMalloc((void **)dst, std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess || n == 0) return e;
+  return cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+template <class F> void parallel_ranges(size_t n, F f)
+{
+  const unsigned T = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  if (n < 65536 || T == 1) {
+    f((size_t)0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t chunk = (n + T - 1) / T;
+  for (unsigned t = 0; t < T; t++) {
+    const size_t a = t * chunk, b = std::min(n, a + chunk);
+    if (a < b) th.emplace_back(f, a, b);
+  }
+  for (auto &x : th) x.join();
+}
+
+void activate(DevMesh &m, const IluSet &s)
+{
+  m.ia = s.ia; m.ja = s.ja; m.diag = s.diag; m.tblk = s.tblk; m.lpos = s.lpos;
+  m.last_lower = s.last_lower; m.pair_ptr = s.pair_ptr; m.pairs = s.pairs;
+  m.lev_l = s.lev_l; m.lev_u = s.lev_u; m.lev_ptr_d = s.lev_ptr_d;
+  m.lev_l_ptr = s.lev_l_ptr; m.lev_u_ptr = s.lev_u_ptr;
+  m.nlev_l = s.nlev_l; m.nlev_u = s.nlev_u;
+  m.desc_l = s.desc_l; m.desc_u = s.desc_u;
+  m.trsv_mode = s.trsv_mode;
+  m.syncfree = s.trsv_mode == 1;
+  m.fill_blk = s.fill_blk; m.fill_diag = s.fill_diag; m.fill_last = s.fill_last; m.fill_lpos = s.fill_lpos;
+  m.ntiles = s.ntiles; m.tile_ptr = s.tile_ptr; m.tile_step = s.tile_step; m.tile_pub = s.tile_pub;
+  m.tile_wait = s.tile_wait; m.tile_desc = s.tile_desc; m.tile_prog = s.tile_prog;
+}
+
+// Tiles of the tiled triangular sweep: columns along the sweep direction
+// (1,1,1), cut in the plane across it (u = x - y, w = x + y - 2z) into
+// floor(sqrt(T)) strips of equal node count by u, each strip into cells of
+// equal node count by w.  Tile ids run strip by strip.
+std::vector<uint32_t> partition_tiles(const double *X, const double *Y, const double *Z, size_t N, uint32_t T)
+{
+  std::vector<uint32_t> tile(N, 0);
+  if (T <= 1 || N == 0) return tile;
+  const uint32_t Tu = std::max(1u, (uint32_t)std::floor(std::sqrt((double)T)));
+  std::vector<uint32_t> idx(N);
+  std::vector<double> u(N), w(N);
+  for (size_t i = 0; i < N; i++) {
+    idx[i] = (uint32_t)i;
+    u[i] = X[i] - Y[i];
+    w[i] = (X[i] + Y[i]) - 2.0 * Z[i];
+  }
+  std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return u[a] < u[b]; });
+  size_t start = 0;
+  uint32_t t0 = 0;
+  for (uint32_t k = 0; k < Tu; k++) {
+    const uint32_t cells = T / Tu + (k < T % Tu ? 1u : 0u);
+    const size_t end = (size_t)((unsigned __int128)N * (t0 + cells) / T);
+    std::stable_sort(idx.begin() + start, idx.begin() + end, [&](uint32_t a, uint32_t b) { return w[a] < w[b]; });
+    const size_t len = end - start;
+    for (uint32_t c = 0; c < cells; c++) {
+      const size_t c0 = start + len * c / cells, c1 = start + len * (c + 1) / cells;
+      for (size_t q = c0; q < c1; q++) tile[idx[q]] = t0 + c;
+    }
+    start = end;
+    t0 += cells;
+  }
+  return tile;
+}
+
+// Position of every node in the spatial elimination order.  ILU(0) depends
+// only on which of two neighbours is eliminated first.
+//   tiles (default): tile by tile (ids as above), within a tile ascending
+//     x + y + z.  Inside a tile the edges are oriented as a sweep orients
+//     them -- much as the lexicographic order of a lattice does, the strong
+//     ordering -- and between tiles from the lower tile id to the higher, so
+//     that the tiled sweep's CTAs depend on their neighbours in one direction
+//     only and run as a pipeline;
+//   KFUN3D_ILU_PERM=sweep: ascending x + y + z over the whole mesh, ties in
+//     node order (level sets: about 3n on an n^3 Kuhn box, against about
+//     9n for the Morton order of the jittered coordinates);
+//   KFUN3D_ILU_PERM=morton: Morton order of the coordinates, 21 bits per axis
+//     over the bounding box, ties in node order;
+//   KFUN3D_ILU_PERM=identity: the mesh's own order through the renumbering
+//     code (reproduces the mesh order bit for bit; a test hook).
+std::vector<uint32_t> spatial_rank(const GEOMETRY *g, size_t N, const std::vector<uint32_t> &tile)
+{
+  std::vector<uint32_t> rank(N), ord(N);
+  for (size_t i = 0; i < N; i++) ord[i] = (uint32_t)i;
+  const char *env = getenv("KFUN3D_ILU_PERM");
+  if (env && strcmp(env, "identity") == 0) return ord;
+  const double *X = g->n->xyz->x0, *Y = g->n->xyz->x1, *Z = g->n->xyz->x2;
+  if (env && strcmp(env, "morton") == 0) {
+    double lo[3] = {X[0], Y[0], Z[0]}, hi[3] = {X[0], Y[0], Z[0]};
+    for (size_t i = 0; i < N; i++) {
+      const double c[3] = {X[i], Y[i], Z[i]};
+      for (int d = 0; d < 3; d++) { lo[d] = std::min(lo[d], c[d]); hi[d] = std::max(hi[d], c[d]); }
+    }
+    auto spread = [](uint64_t v) {
+      v &= 0x1fffffull;
+      v = (v | v << 32) & 0x1f00000000ffffull;
+      v = (v | v << 16) & 0x1f0000ff0000ffull;
+      v = (v | v << 8) & 0x100f00f00f00f00full;
+      v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+      v = (v | v << 2) & 0x1249249249249249ull;
+      return v;
+    };
+    std::vector<uint64_t> key(N);
+    for (size_t i = 0; i < N; i++) {
+      const double c[3] = {X[i], Y[i], Z[i]};
+      uint64_t k = 0;
+      for (int d = 0; d < 3; d++) {
+        const double span = hi[d] > lo[d] ? hi[d] - lo[d] : 1.0;
+        const uint64_t b = (uint64_t)std::min(2097151.0, std::max(0.0, (c[d] - lo[d]) / span * 2097151.0));
+        k |= spread(b) << d;
+      }
+      key[i] = k;
+    }
+    std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+  } else {
+    std::vector<double> key(N);
+    for (size_t i = 0; i < N; i++) key[i] = (X[i] + Y[i]) + Z[i];
+    if (env && strcmp(env, "sweep") == 0)
+      std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+    else
+      std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
+        return tile[a] != tile[b] ? tile[a] < tile[b] : key[a] < key[b];
+      });
+  }
+  for (size_t p = 0; p < N; p++) rank[ord[p]] = (uint32_t)p;
+  return rank;
+}
+
+// Host form of the tiled sweep: per tile its rows of each sweep grouped by
+// level (a step; longest rows first), and before each step the progress it
+// needs from other tiles -- for every row of the step and every column row
+// j held by another tile t', progress[t'] >= (level of j) + 1 in the lower
+// sweep, nlev_l + (backward level of j) + 1 in the upper sweep -- keeping
+// only requirements that earlier steps of the tile did not already cover.
+// A tile publishes level + 1 (lower) or nlev_l + level + 1 (upper) after a
+// step that another tile waits for (flagged by bit 31 of pub).  Every
+// requirement names a strictly earlier level, so with all tiles resident the
+// sweep cannot deadlock.
+//
+// When every wait of the lower sweep points to a lower tile id and every
+// wait of the upper sweep to a higher one (the tile-major numbering), the
+// tiles form a pipeline and a requirement may ask for `slack` more steps of
+// the other tile than the rows need (capped at its last step of the sweep):
+// the downstream tile then trails far enough behind that it rarely finds a
+// requirement unmet, without any wait cycle.
+struct TileHost {
+  std::vector<uint32_t> ptr, pub;
+  std::vector<uint4> step, desc;
+  std::vector<uint2> wait;
+  std::vector<uint2> raw;            // requirements before slack and filtering
+  std::vector<uint32_t> raw_ptr;     // per step into raw
+};
+
+TileHost build_tiles(const HostPattern &p, const std::vector<uint32_t> &rank, const std::vector<uint32_t> &tile,
+                     uint32_t T, size_t N, uint32_t slack)
+{
+  std::vector<uint32_t> rt(N), ll(N), ul(N);
+  for (size_t i = 0; i < N; i++) rt[rank[i]] = tile[i];
+  const uint32_t nl = (uint32_t)p.lev_l_ptr.size() - 1, nu = (uint32_t)p.lev_u_ptr.size() - 1;
+  for (uint32_t l = 0; l < nl; l++)
+    for (uint32_t q = p.lev_l_ptr[l]; q < p.lev_l_ptr[l + 1]; q++) ll[p.lev_l[q]] = l;
+  for (uint32_t l = 0; l < nu; l++)
+    for (uint32_t q = p.lev_u_ptr[l]; q < p.lev_u_ptr[l + 1]; q++) ul[p.lev_u[q]] = l;
+  std::vector<uint32_t> tcnt(T + 1, 0), trow(N);
+  for (size_t i = 0; i < N; i++) tcnt[rt[i] + 1]++;
+  for (uint32_t t = 0; t < T; t++) tcnt[t + 1] += tcnt[t];
+  {
+    std::vector<uint32_t> fillp(tcnt.begin(), tcnt.end() - 1);
+    for (size_t i = 0; i < N; i++) trow[fillp[rt[i]]++] = (uint32_t)i;
+  }
+  std::vector<TileHost> part(T);
+  std::vector<char> two_way(T, 0);
+  auto for_tiles = [T](auto &&fn) {
+    const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (unsigned k = 0; k < nth; k++) {
+      const size_t a = (size_t)T * k / nth, b = (size_t)T * (k + 1) / nth;
+      if (a < b) th.emplace_back([&fn, a, b] { for (size_t t = a; t < b; t++) fn(t); });
+    }
+    for (auto &x : th) x.join();
+  };
+  // 1. steps, row descriptors and the raw requirements
+  for_tiles([&](size_t t) {
+    TileHost &h = part[t];
+    for (int upper = 0; upper < 2; upper++) {
+      h.ptr.push_back((uint32_t)h.step.size());
+      std::vector<uint32_t> rows(trow.begin() + tcnt[t], trow.begin() + tcnt[t + 1]);
+      auto len = [&](uint32_t i) { return upper ? p.ia[i + 1] - p.diag[i] - 1 : p.diag[i] - p.ia[i]; };
+      auto lev = [&](uint32_t i) { return upper ? ul[i] : ll[i]; };
+      std::stable_sort(rows.begin(), rows.end(), [&](uint32_t a, uint32_t b) {
+        return lev(a) != lev(b) ? lev(a) < lev(b) : len(a) > len(b);
+      });
+      for (size_t q0 = 0; q0 < rows.size();) {
+        size_t q1 = q0;
+        const uint32_t L = lev(rows[q0]);
+        while (q1 < rows.size() && lev(rows[q1]) == L) q1++;
+        uint4 st = make_uint4((uint32_t)h.desc.size(), 0, 0, 0);
+        h.raw_ptr.push_back((uint32_t)h.raw.size());
+        const size_t r0 = h.raw.size();
+        for (size_t q = q0; q < q1; q++) {
+          const uint32_t i = rows[q];
+          const uint32_t jb = upper ? p.diag[i] + 1 : p.ia[i], je = upper ? p.ia[i + 1] : p.diag[i];
+          h.desc.push_back(make_uint4(i, jb, je, 0));
+          for (uint32_t j = jb; j < je; j++) {
+            const uint32_t c = p.ja[j], tc = rt[c];
+            if (tc == t) continue;
+            if (upper ? tc < t : tc > t) two_way[t] = 1;
+            const uint32_t v = upper ? nl + ul[c] + 1 : ll[c] + 1;
+            auto it = std::find_if(h.raw.begin() + r0, h.raw.end(), [&](const uint2 &x) { return x.x == tc; });
+            if (it == h.raw.end()) h.raw.push_back(make_uint2(tc, v));
+            else it->y = std::max(it->y, v);
+          }
+        }
+        st.y = (uint32_t)h.desc.size();
+        h.step.push_back(st);
+        h.pub.push_back(upper ? nl + L + 1 : L + 1);
+        q0 = q1;
+      }
+    }
+    h.ptr.push_back((uint32_t)h.step.size());
+    h.raw_ptr.push_back((uint32_t)h.raw.size());
+  });
+  if (std::find(two_way.begin(), two_way.end(), 1) != two_way.end()) slack = 0;
+  // 2. slack, then only the requirements earlier steps do not cover
+  for_tiles([&](size_t t) {
+    TileHost &h = part[t];
+    std::vector<std::pair<uint32_t, uint32_t>> have;
+    for (uint32_t k = 0; k < (uint32_t)h.step.size(); k++) {
+      const int upper = k >= h.ptr[1];
+      h.step[k].z = (uint32_t)h.wait.size();
+      for (uint32_t q = h.raw_ptr[k]; q < h.raw_ptr[k + 1]; q++) {
+        uint2 nd = h.raw[q];
+        if (slack) {
+          const TileHost &o = part[nd.x];
+          auto b = o.pub.begin() + o.ptr[upper], e = o.pub.begin() + o.ptr[upper + 1];
+          const uint32_t target = std::min(nd.y + slack, *(e - 1));
+          nd.y = *std::lower_bound(b, e, target);
+        }
+        auto it = std::find_if(have.begin(), have.end(), [&](const auto &x) { return x.first == nd.x; });
+        if (it != have.end() && it->second >= nd.y) continue;
+        if (it == have.end()) have.push_back({nd.x, nd.y});
+        else it->second = nd.y;
+        h.wait.push_back(nd);
+      }
+      h.step[k].w = (uint32_t)h.wait.size();
+    }
+  });
+  // 3. one array of each, steps' offsets rebased
+  TileHost out;
+  for (uint32_t t = 0; t < T; t++) {
+    const TileHost &h = part[t];
+    const uint32_t s0 = (uint32_t)out.step.size(), d0 = (uint32_t)out.desc.size(), w0 = (uint32_t)out.wait.size();
+    out.ptr.push_back(s0 + h.ptr[0]);
+    out.ptr.push_back(s0 + h.ptr[1]);
+    for (const uint4 &st : h.step) out.step.push_back(make_uint4(st.x + d0, st.y + d0, st.z + w0, st.w + w0));
+    out.pub.insert(out.pub.end(), h.pub.begin(), h.pub.end());
+    out.desc.insert(out.desc.end(), h.desc.begin(), h.desc.end());
+    out.wait.insert(out.wait.end(), h.wait.begin(), h.wait.end());
+  }
+  out.ptr.push_back((uint32_t)out.step.size());
+  // a step's completion is published only when another tile waits for it
+  std::vector<std::vector<uint32_t>> needed(T);
+  for (const uint2 &w : out.wait) needed[w.x].push_back(w.y);
+  for (auto &v : needed) std::sort(v.begin(), v.end());
+  for (uint32_t t = 0; t < T; t++)
+    for (uint32_t k = out.ptr[2 * t]; k < out.ptr[2 * t + 2]; k++)
+      if (std::binary_search(needed[t].begin(), needed[t].end(), out.pub[k])) out.pub[k] |= 0x80000000u;
+  return out;
+}
+
+int build_spatial(DevMesh &m, const GEOMETRY *g)
+{
+  const size_t N = m.N, E = m.E;
+  const unsigned int *n0 = g->e->eptr->n0, *n1 = g->e->eptr->n1;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m.device);
+  const uint32_t T = (uint32_t)std::max(1, nsm);
+  const std::vector<uint32_t> tile = partition_tiles(g->n->xyz->x0, g->n->xyz->x1, g->n->xyz->x2, N, T);
+  const std::vector<uint32_t> rank = spatial_rank(g, N, tile);
+  std::vector<uint32_t> pn0(E), pn1(E);
+  for (size_t e = 0; e < E; e++) { pn0[e] = rank[n0[e]]; pn1[e] = rank[n1[e]]; }
+  HostPattern p;
+  kf_build_pattern(p, N, E, pn0.data(), pn1.data());
+  IluSet &s = m.iset[1];
+  bool ok = true;
+  auto up = [&](auto **dst, const auto &vec) {
+    if (ok && upload(dst, vec.data(), vec.size()) != cudaSuccess) ok = false;
+  };
+  up(&s.ia, p.ia);
+  up(&s.ja, p.ja);
+  up(&s.diag, p.diag);
+  up(&s.tblk, p.tblk);
+  up(&s.lpos, p.lpos);
+  up(&s.last_lower, p.last_lower);
+  up(&s.pair_ptr, p.pair_ptr);
+  if (ok && upload(&s.pairs, reinterpret_cast<const uint2 *>(p.pairs.data()), p.pairs.size() / 2) != cudaSuccess)
+    ok = false;
+  up(&s.lev_l, p.lev_l);
+  up(&s.lev_u, p.lev_u);
+  s.lev_l_ptr = p.lev_l_ptr;
+  s.lev_u_ptr = p.lev_u_ptr;
+  s.nlev_l = (uint32_t)p.lev_l_ptr.size() - 1;
+  s.nlev_u = (uint32_t)p.lev_u_ptr.size() - 1;
+  {
+    std::vector<uint32_t> lp(p.lev_l_ptr);
+    lp.insert(lp.end(), p.lev_u_ptr.begin(), p.lev_u_ptr.end());
+    up(&s.lev_ptr_d, lp);
+  }
+  {
+    std::vector<uint4> dl(N), du(N);
+    for (size_t q = 0; q < N; q++) {
+      const uint32_t i = p.lev_l[q];
+      dl[q] = make_uint4(i, p.ia[i], p.diag[i], 0);
+      const uint32_t k = p.lev_u[q];
+      du[q] = make_uint4(k, p.diag[k] + 1, p.ia[k + 1], 0);
+    }
+    auto by_length = [](std::vector<uint4> &d, const std::vector<uint32_t> &ptr) {
+      for (size_t l = 0; l + 1 < ptr.size(); l++)
+        std::stable_sort(d.begin() + ptr[l], d.begin() + ptr[l + 1],
+                         [](const uint4 &a, const uint4 &b) { return a.z - a.y > b.z - b.y; });
+    };
+    by_length(dl, p.lev_l_ptr);
+    by_length(du, p.lev_u_ptr);
+    up(&s.desc_l, dl);
+    up(&s.desc_u, du);
+  }
+  // the fill's view of the renumbered pattern, per node of the mesh
+  {
+    std::vector<uint32_t> inc_ptr(N + 1), inc_oth(2 * E), ord(N);
+    if (ok && cudaMemcpy(inc_ptr.data(), m.inc_ptr, (N + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+      ok = false;
+    if (ok && cudaMemcpy(inc_oth.data(), m.inc_oth, 2 * E * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+      ok = false;
+    if (ok && cudaMemcpy(ord.data(), m.ord, N * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess) ok = false;
+    std::vector<uint32_t> blk(2 * E), fd(N), fl(N), fp(N);
+    if (ok) {
+      auto find = [&](uint32_t row, uint32_t col) -> uint32_t {
+        auto b = p.ja.begin() + p.ia[row], en = p.ja.begin() + p.ia[row + 1];
+        return (uint32_t)(std::lower_bound(b, en, col) - p.ja.begin());
+      };
+      parallel_ranges(N, [&](size_t r0, size_t r1) {
+        for (size_t row = r0; row < r1; row++) {
+          const uint32_t node = ord[row];
+          for (uint32_t k = inc_ptr[row]; k < inc_ptr[row + 1]; k++) blk[k] = find(rank[node], rank[inc_oth[k]]);
+        }
+      });
+      for (size_t i = 0; i < N; i++) {
+        fd[i] = p.diag[rank[i]];
+        fl[i] = p.last_lower[rank[i]];
+        fp[i] = p.lpos[rank[i]];
+      }
+    }
+    up(&s.fill_blk, blk);
+    up(&s.fill_diag, fd);
+    up(&s.fill_last, fl);
+    up(&s.fill_lpos, fp);
+  }
+  {
+    uint32_t slack = 2;
+    const char *senv = getenv("KFUN3D_TILE_SLACK");   // steps of slack in the pipeline (0-64)
+    if (senv && atoi(senv) >= 0 && atoi(senv) <= 64) slack = (uint32_t)atoi(senv);
+    const TileHost th = build_tiles(p, rank, tile, T, N, slack);
+    s.ntiles = T;
+    up(&s.tile_ptr, th.ptr);
+    up(&s.tile_step, th.step);
+    up(&s.tile_pub, th.pub);
+    up(&s.tile_wait, th.wait);
+    up(&s.tile_desc, th.desc);
+    if (ok && cudaMalloc(&s.tile_prog, T * sizeof(unsigned)) != cudaSuccess) ok = false;
+  }
+  up(&m.ilu_rank, rank);
+  if (ok && cudaMalloc(&m.pb, 4 * N * sizeof(double)) != cudaSuccess) ok = false;
+  if (ok && cudaMalloc(&m.px, 4 * N * sizeof(double)) != cudaSuccess) ok = false;
+  // many thin levels in a spatial order: one launch per level (programmatic
+  // dependent launch) is the fastest schedule measured there (120^3 box,
+  // FP32 factor: 3.2 ms against 5.0 ms for the persistent sweep and 5.3 ms
+  // for the tiled one); KFUN3D_SPTRSV picks another
+  s.trsv_mode = 4;
+  const char *env = getenv("KFUN3D_SPTRSV");
+  if (env && strcmp(env, "tiled") == 0) s.trsv_mode = 6;
+  if (env && strcmp(env, "mono") == 0) s.trsv_mode = 5;
+  if (env && strcmp(env, "levels16") == 0) s.trsv_mode = 2;
+  if (env && strcmp(env, "syncfree") == 0) s.trsv_mode = 1;
+  if (!ok) {
+    kf_set_error(KFUN3D_ERR_CUDA, "spatial ILU(0) order: out of device memory");
+    return KFUN3D_ERR_CUDA;
+  }
+  s.valid = true;
+  return KFUN3D_OK;
+}
+
+}  // namespace
+
+int kf_ilu_select(DevMesh &m, const GEOMETRY *g, int order)
+{
+  order = order ? 1 : 0;
+  if (order == m.ilu_active) return KFUN3D_OK;
+  if (order == 1 && !m.iset[1].valid) {
+    const int rc = build_spatial(m, g);
+    if (rc != KFUN3D_OK) return rc;
+  }
+  activate(m, m.iset[order]);
+  m.ilu_active = order;
+  m.factored = false;
+  // the persistent L slots hold the other numbering's factor: start afresh
+  if (cudaMemsetAsync(m.lslot, 0, (16 * (size_t)m.nlower + 16) * sizeof(double), m.stream) != cudaSuccess) {
+    kf_set_error(KFUN3D_ERR_CUDA, "spatial ILU(0) order: clearing the L slots failed");
+    return KFUN3D_ERR_CUDA;
+  }
+  return KFUN3D_OK;
+}
+
+void kf_ilu_release(DevMesh &m)
+{
+  if (m.ilu_active && m.iset[0].valid) {
+    activate(m, m.iset[0]);
+    m.ilu_active = 0;
+  }
+  IluSet &s = m.iset[1];
+  void *ptrs[] = {s.ia, s.ja, s.diag, s.tblk, s.lpos, s.last_lower, s.pair_ptr, s.pairs, s.lev_l, s.lev_u,
+                  s.lev_ptr_d, s.desc_l, s.desc_u, s.fill_blk, s.fill_diag, s.fill_last, s.fill_lpos,
+                  s.tile_ptr, s.tile_step, s.tile_pub, s.tile_wait, s.tile_desc, s.tile_prog,
+                  m.ilu_rank, m.pb, m.px};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  s = IluSet{};
+  m.ilu_rank = nullptr;
+  m.pb = m.px = nullptr;
+}
+
+extern "C" long kfun3d_ilu_rank(const GEOMETRY *g, unsigned int *rank)
+{
+  MatrixHandle *h = kf_handle(g);
+  if (!h || !h->dev || !h->dev->iset[1].valid || !h->dev->ilu_rank) {
+    kf_set_error(KFUN3D_ERR_ARG, "kfun3d_ilu_rank: the spatial ILU order has not been built for this GEOMETRY");
+    return -1;
+  }
+  DevMesh &m = *h->dev;
+  if (rank && cudaMemcpy(rank, m.ilu_rank, (size_t)m.N * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    kf_set_error(KFUN3D_ERR_CUDA, "kfun3d_ilu_rank: copy failed");
+    return -1;
+  }
+  return (long)m.N;
+}

@@ -87,6 +87,34 @@ __device__ __forceinline__ bool kf_grid_barrier(unsigned *bar, int *err)
   return ok_s != 0;
 }
 
+// The matrix pattern the Jacobian fill, ILU(0) and the triangular solves use:
+// the reference's numbering (set 0), or its rows and columns renumbered in a
+// spatial order (set 1, kfun3d_set_ilu_order).  fill_* are indexed by node in
+// the mesh's numbering and point into the set's pattern.  tile_*: the tiled
+// triangular sweep of set 1 (one CTA per tile, trsv_mode 6).
+struct IluSet {
+  bool valid = false;
+  uint32_t *ia = nullptr, *ja = nullptr, *diag = nullptr, *tblk = nullptr, *lpos = nullptr;
+  uint32_t *last_lower = nullptr, *pair_ptr = nullptr;
+  uint2 *pairs = nullptr;
+  uint32_t *lev_l = nullptr, *lev_u = nullptr, *lev_ptr_d = nullptr;
+  std::vector<uint32_t> lev_l_ptr, lev_u_ptr;
+  uint32_t nlev_l = 0, nlev_u = 0;
+  uint4 *desc_l = nullptr, *desc_u = nullptr;
+  int trsv_mode = 4;
+  uint32_t *fill_blk = nullptr;    // [2E] block of (node, other) per incidence (CSR order)
+  uint32_t *fill_diag = nullptr;   // [N] diagonal block of each node
+  uint32_t *fill_last = nullptr;   // [N] the node's row's last-touched lower block (or ~0)
+  uint32_t *fill_lpos = nullptr;   // [N] the node's row's first persistent L slot
+  uint32_t ntiles = 0;
+  uint32_t *tile_ptr = nullptr;    // [2T+1] tile t: lower steps [2t, 2t+1), upper steps [2t+1, 2t+2)
+  uint4 *tile_step = nullptr;      // per step: rows [x, y) of tile_desc, waits [z, w)
+  uint32_t *tile_pub = nullptr;    // per step: progress the tile publishes after it
+  uint2 *tile_wait = nullptr;      // (tile, progress it must have reached)
+  uint4 *tile_desc = nullptr;      // [2N] row descriptors (row, first block, end block), by tile and step
+  unsigned *tile_prog = nullptr;   // [T] progress counters, cleared before each solve
+};
+
 // Device mirror of one GEOMETRY.  Node-indexed arrays follow the reference's
 // numbering; edge-indexed arrays its (sorted) edge order.
 struct DevMesh {
@@ -174,6 +202,18 @@ struct DevMesh {
   int trsv_mgrid_per = 2;         // 512-thread CTAs per SM in mode 5 (1, 2 or 3)
   int trsv_lanes = 8;             // lanes per row in mode 5 (8 or 16)
   double *h_scal = nullptr;       // pinned host mirror of scal
+  // ILU(0) ordering: the active set's fields are copied into the fields above
+  IluSet iset[2];
+  uint32_t ntiles = 0;            // active set's tiled sweep (trsv_mode 6)
+  uint32_t *tile_ptr = nullptr, *tile_pub = nullptr;
+  uint4 *tile_step = nullptr, *tile_desc = nullptr;
+  uint2 *tile_wait = nullptr;
+  unsigned *tile_prog = nullptr;
+  int ilu_active = 0;             // 1: the spatial set is active
+  uint32_t *ilu_rank = nullptr;   // [N] row of each node in the spatial set
+  double *pb = nullptr, *px = nullptr;   // [4N] right-hand side and solution, spatial numbering
+  int graph_ilu = 0;              // ILU set the Arnoldi graphs were captured with
+  uint32_t *fill_blk = nullptr, *fill_diag = nullptr, *fill_last = nullptr, *fill_lpos = nullptr;
   // flexible GMRES (right preconditioning) and the learned preconditioner
   double *Z = nullptr;            // [30][4N] preconditioned basis vectors
   double *qold = nullptr;         // [4N] state before the last update
@@ -186,6 +226,10 @@ struct DevMesh {
 };
 
 DevMesh *kf_device(const GEOMETRY *g);   // creates and uploads on first use
+int kf_ilu_order();
+// Makes the ILU(0) ordering `order` (0 the mesh's numbering, 1 spatial) the
+// active one, building set 1 on first use; KFUN3D_OK or an error code.
+int kf_ilu_select(DevMesh &m, const GEOMETRY *g, int order);
 
 void kf_count_launch(unsigned n = 1);
 void kfun3d_reset_launch_count_by(unsigned long long n);   // undo counts taken during graph capture

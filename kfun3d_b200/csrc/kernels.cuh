@@ -1707,6 +1707,197 @@ __global__ void __launch_bounds__(256, 4) k_trsv_syncfree(uint32_t N, const uint
   }
 }
 
+// The tiled sweep of the spatial ILU(0) order: both triangular sweeps in one
+// cooperative launch of one 512-thread CTA per tile (rows of a tile: a column
+// of the mesh along the sweep direction).  Warps 0-14 work the tile's steps
+// in order -- the rows of one level that it holds, G lanes per row,
+// arithmetic as in k_trsv_level16 -- separated by a barrier of those warps
+// only.  Before a step warp 0 makes sure the other tiles the step reads from
+// have reached the progress computed on the host: it issues those reads one
+// step ahead and polls only what was not yet there.  Warp 15 publishes: it
+// follows the count of completed steps in shared memory and stores the
+// tile's progress (release) when a step another tile waits for (bit 31 of
+// pub) is complete, so the fence stays off the compute warps' path.
+// Everything that does not depend on x -- row descriptors two steps ahead,
+// columns, first blocks, diagonal block and right-hand side one step ahead --
+// is loaded before it is needed.  With every tile resident and every
+// requirement naming a strictly earlier level, the sweep cannot deadlock.  A
+// wait that exceeds its bound records an error in *err and the tile stops;
+// the others give up at their next look at *err.
+constexpr uint32_t KF_TILE_IDLE_LIMIT = 1u << 27;   // publisher polls of shared memory without news
+
+template <typename T, int G>
+__global__ void __launch_bounds__(512, 1) k_trsv_tiled(const uint32_t *__restrict__ tptr,
+                                                       const uint4 *__restrict__ steps,
+                                                       const uint32_t *__restrict__ pub,
+                                                       const uint2 *__restrict__ waits,
+                                                       const uint4 *__restrict__ tdesc,
+                                                       const uint32_t *__restrict__ ja, const T *__restrict__ A,
+                                                       const double *__restrict__ b, double *x, uint32_t *prog,
+                                                       int *err)
+{
+  constexpr int S = G / 4;
+  constexpr int NCW = 15;                       // compute warps
+  constexpr uint32_t NCT = NCW * 32;
+  __shared__ int fail_s;
+  __shared__ uint32_t done_s;                   // steps completed
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t t = blockIdx.x;
+  const uint32_t k0 = tptr[2 * t], k1 = tptr[2 * t + 1], k2 = tptr[2 * t + 2];
+  if (threadIdx.x == 0) { fail_s = 0; done_s = k0; }
+  __syncthreads();
+  if (warp == NCW) {
+    // publisher
+    if (lane == 0) {
+      uint32_t published = k0, idle = 0;
+      while (published < k2) {
+        uint32_t done;
+        asm volatile("ld.acquire.cta.shared.u32 %0, [%1];" : "=r"(done) : "r"((uint32_t)__cvta_generic_to_shared(&done_s)) : "memory");
+        if (done > published) {
+          for (uint32_t kk = done; kk-- > published;) {
+            const uint32_t pv = pub[kk];
+            if (pv >> 31) { st_release(prog + t, pv & 0x7fffffffu); break; }
+          }
+          published = done;
+          idle = 0;
+        } else if (++idle > KF_TILE_IDLE_LIMIT || ((idle & 255) == 0 && (*(volatile int *)&fail_s || *(volatile int *)err))) {
+          break;
+        }
+      }
+    }
+    return;
+  }
+  const int gl = lane & (G - 1), base = lane - gl, jj = gl >> 2, r = gl & 3;
+  const unsigned gmask = ((1u << G) - 1u) << base;
+  const uint32_t R = NCT / G, h = threadIdx.x / G;
+  // descriptor of this group's first row in step k (w = 1 when there is one)
+  auto load_desc = [&](uint32_t k) -> uint4 {
+    uint4 dd = make_uint4(0, 0, 0, 0);
+    if (k < k2) {
+      const uint4 sk = steps[k];
+      if (sk.x + h < sk.y) { dd = tdesc[sk.x + h]; dd.w = 1; }
+    }
+    return dd;
+  };
+  uint32_t col[4];
+  T a[4][4], dg[4];
+  double xb = 0.0;
+  auto load_blocks = [&](uint32_t k, const uint4 dd) {
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      col[p] = 0xffffffffu;
+#pragma unroll
+      for (int c = 0; c < 4; c++) a[p][c] = (T)0;
+    }
+    if (!dd.w) return;
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+      const uint32_t j = dd.y + S * p + jj;
+      if (j < dd.z) {
+        col[p] = ja[j];
+        const T *blk = A + 16 * (size_t)j + 4 * r;
+#pragma unroll
+        for (int c = 0; c < 4; c++) a[p][c] = blk[c];
+      }
+    }
+    if (k >= k1) {
+      const T *blk = A + 16 * (size_t)(dd.y - 1) + 4 * r;
+#pragma unroll
+      for (int c = 0; c < 4; c++) dg[c] = blk[c];
+    } else {
+      xb = b[4 * (size_t)dd.x + r];
+    }
+  };
+  uint4 st = k0 < k2 ? steps[k0] : make_uint4(0, 0, 0, 0);
+  uint4 d = load_desc(k0);
+  load_blocks(k0, d);
+  uint4 d1 = load_desc(k0 + 1);
+  uint32_t pre = 0;   // warp 0: progress of the lane's first requirement of the coming step, read ahead
+  if (warp == 0 && st.z + lane < st.w) pre = ld_acquire(prog + waits[st.z + lane].x);
+  for (uint32_t k = k0; k < k2; k++) {
+    if (warp == 0 && st.z < st.w) {
+      bool bad = false;
+      for (uint32_t w = st.z + lane; w < st.w && !bad; w += 32) {
+        const uint2 wt = waits[w];
+        if (w == st.z + lane && pre >= wt.y) continue;
+        uint32_t spins = 0;
+        while (ld_acquire(prog + wt.x) < wt.y) {
+          if (++spins > KF_SPIN_LIMIT) { atomicExch(err, 1); bad = true; break; }
+          if ((spins & 255) == 0 && *(volatile int *)err) { bad = true; break; }
+        }
+      }
+      if (bad) fail_s = 1;
+    }
+    asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
+    if (*(volatile int *)&fail_s) return;
+    const uint4 cur = st;
+    const bool upper = k >= k1;
+    // ahead: the next step's record and requirements, the descriptor two steps on
+    if (k + 1 < k2) st = steps[k + 1];
+    const uint4 d2 = load_desc(k + 2);
+    if (warp == 0 && k + 1 < k2 && st.z + lane < st.w) pre = ld_acquire(prog + waits[st.z + lane].x);
+    if (d.w) {
+      // the prefetched first pass: arithmetic as trsv_row_g
+      const uint32_t i = d.x, jb = d.y, je = d.z;
+      double xi = upper ? __ldcg(x + 4 * (size_t)i + r) : xb;
+      for (uint32_t c0 = jb; c0 < je; c0 += 4 * S) {
+        double tp[4];
+#pragma unroll
+        for (int p = 0; p < 4; p++) {
+          const uint32_t j = c0 + S * p + jj;
+          tp[p] = 0.0;
+          if (j < je) {
+            uint32_t cc = col[p];
+            double a0 = (double)a[p][0], a1 = (double)a[p][1], a2 = (double)a[p][2], a3 = (double)a[p][3];
+            if (c0 != jb) {
+              cc = ja[j];
+              const T *blk = A + 16 * (size_t)j + 4 * r;
+              a0 = (double)blk[0]; a1 = (double)blk[1]; a2 = (double)blk[2]; a3 = (double)blk[3];
+            }
+            const double2 x01 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)cc);
+            const double2 x23 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)cc + 1);
+            double sum = 0.0;
+            sum += a0 * x01.x;
+            sum += a1 * x01.y;
+            sum += a2 * x23.x;
+            sum += a3 * x23.y;
+            tp[p] = sum;
+          }
+        }
+        const uint32_t cnt = (je - c0) < (uint32_t)(4 * S) ? (je - c0) : (uint32_t)(4 * S);
+#pragma unroll
+        for (int p = 0; p < 4; p++)
+          for (int q = 0; q < S; q++) {
+            if ((uint32_t)(S * p + q) >= cnt) break;
+            xi = -1.0 * __shfl_sync(gmask, tp[p], base + 4 * q + r) + xi;
+          }
+      }
+      if (upper) {
+        const double x0 = __shfl_sync(gmask, xi, base + 0), x1 = __shfl_sync(gmask, xi, base + 1);
+        const double x2 = __shfl_sync(gmask, xi, base + 2), x3 = __shfl_sync(gmask, xi, base + 3);
+        double y = 0.0;
+        y += (double)dg[0] * x0;
+        y += (double)dg[1] * x1;
+        y += (double)dg[2] * x2;
+        y += (double)dg[3] * x3;
+        xi = y;
+      }
+      if (gl < 4) __stcg(x + 4 * (size_t)i + r, xi);
+    }
+    // rows beyond the first pass
+    if (upper)
+      for (uint32_t s = cur.x + h + R; s < cur.y; s += R) trsv_row_g<T, true, G>(tdesc[s], ja, A, b, x, base, gl, gmask);
+    else
+      for (uint32_t s = cur.x + h + R; s < cur.y; s += R) trsv_row_g<T, false, G>(tdesc[s], ja, A, b, x, base, gl, gmask);
+    load_blocks(k + 1, d1);
+    d = d1;
+    d1 = d2;
+    asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
+    if (threadIdx.x == 0)
+      asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(&done_s)), "r"(k + 1) : "memory");
+  }
+}
+
 // ------------------------------------------------------------------ J.v
 
 // src/kernel.c:35-44: y = (y - r + cdt (w - q)) * a, a = |x| / h from the
@@ -1800,24 +1991,24 @@ void timestep(DevMesh &m, const double *q, double cfl)
 void fill(DevMesh &m, const double *q, double u, double v, int precision)
 {
   if (precision == 0) {
-    k_fill<double><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.rowof, m.inc_ptr, m.inc_oth, m.inc_edge, m.inc_blk, m.egeo,
-                                                          (const double4 *)q, m.cdt, m.diag, m.last_lower,
-                                                          m.lpos, m.A, m.lslot, m.bnd_of, nullptr);
+    k_fill<double><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.rowof, m.inc_ptr, m.inc_oth, m.inc_edge, m.fill_blk,
+                                                          m.egeo, (const double4 *)q, m.cdt, m.fill_diag, m.fill_last,
+                                                          m.fill_lpos, m.A, m.lslot, m.bnd_of, nullptr);
     kf_count_launch();
     if (m.nb) {
       k_fill_boundary<double><<<blocks(m.nb, 64), 64, 0, m.stream>>>(m.nb, m.bnd_node, m.bnd_ptr, m.bnd_ent, m.s_n,
-                                                                     m.f_n, (const double4 *)q, m.diag, m.A, u, v,
+                                                                     m.f_n, (const double4 *)q, m.fill_diag, m.A, u, v,
                                                                      nullptr);
       kf_count_launch();
     }
   } else {
-    k_fill<float><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.rowof, m.inc_ptr, m.inc_oth, m.inc_edge, m.inc_blk, m.egeo,
-                                                         (const double4 *)q, m.cdt, m.diag, m.last_lower, m.lpos,
-                                                         m.Af, nullptr, m.bnd_of, m.dscr);
+    k_fill<float><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.rowof, m.inc_ptr, m.inc_oth, m.inc_edge, m.fill_blk,
+                                                         m.egeo, (const double4 *)q, m.cdt, m.fill_diag, m.fill_last,
+                                                         m.fill_lpos, m.Af, nullptr, m.bnd_of, m.dscr);
     kf_count_launch();
     if (m.nb) {
       k_fill_boundary<float><<<blocks(m.nb, 64), 64, 0, m.stream>>>(m.nb, m.bnd_node, m.bnd_ptr, m.bnd_ent, m.s_n,
-                                                                    m.f_n, (const double4 *)q, m.diag, m.Af, u, v,
+                                                                    m.f_n, (const double4 *)q, m.fill_diag, m.Af, u, v,
                                                                     m.dscr);
       kf_count_launch();
     }
@@ -1854,6 +2045,29 @@ void ilu(DevMesh &m, int precision)
 
 void sptrsv(DevMesh &m, const double *b, double *x, int precision)
 {
+  if (m.trsv_mode == 6 && m.ntiles) {
+    cudaMemsetAsync(m.tile_prog, 0, m.ntiles * sizeof(unsigned), m.stream);
+    const double *bb = b;
+    int *err = m.status + 1;
+    const void *Ap = precision == 0 ? (const void *)m.A : (const void *)m.Af;
+    void *args[] = {(void *)&m.tile_ptr, (void *)&m.tile_step, (void *)&m.tile_pub, (void *)&m.tile_wait,
+                    (void *)&m.tile_desc, (void *)&m.ja, (void *)&Ap, (void *)&bb, (void *)&x,
+                    (void *)&m.tile_prog, (void *)&err};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(m.ntiles);
+    cfg.blockDim = dim3(512);
+    cfg.stream = m.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const void *fn = precision == 0 ? (const void *)k_trsv_tiled<double, 8> : (const void *)k_trsv_tiled<float, 8>;
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
+    if (e != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e));
+    kf_count_launch();
+    return;
+  }
   if (m.trsv_mode == 4) {
     for (int pass = 0; pass < 2; pass++) {
       const std::vector<uint32_t> &ptr = pass == 0 ? m.lev_l_ptr : m.lev_u_ptr;

@@ -56,6 +56,11 @@ extern "C" int kfun3d_sptrsv_device_noalloc(const GEOMETRY *g, const double *d_b
     return KFUN3D_ERR_ARG;
   }
   DevMesh &m = *h->dev;
+  if (m.ilu_active) {
+    kf_set_error(KFUN3D_ERR_ARG, "kfun3d_sptrsv_device_noalloc: the factor is in the spatial ILU order; "
+                                 "use ComputeSparseTriangularSolve or the mesh order");
+    return KFUN3D_ERR_ARG;
+  }
   if (!m.factored) {
     kf_set_error(KFUN3D_ERR_ARG, "kfun3d_sptrsv_device_noalloc: the matrix has not been factored "
                                  "(call ComputeNumericalILU)");

@@ -349,6 +349,18 @@ bool check_cuda(const char *what)
     }                                                                              \
   } while (0)
 
+// Rows between the mesh numbering and the spatial ILU numbering:
+// to_spatial: dst[rank[i]] = src[i]; from_spatial: dst[i] = src[rank[i]].
+__global__ void k_rows_permute(uint32_t N, const uint32_t *__restrict__ rank, const double4 *__restrict__ src,
+                               double4 *__restrict__ dst, int to_spatial)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const uint32_t r = rank[i];
+  if (to_spatial) dst[r] = src[i];
+  else dst[i] = src[r];
+}
+
 // Kernel set of the current arithmetic mode.
 struct Ops {
   bool fast;
@@ -368,6 +380,15 @@ struct Ops {
   void ilu(DevMesh &m, int p) const { fast ? kf_fast::ilu(m, p) : kf_exact::ilu(m, p); }
   void sptrsv(DevMesh &m, const double *b, double *x, int p) const
   {
+    if (m.ilu_active) {
+      // spatial ILU(0): x = P^T (LU)^-1 P b
+      const unsigned nb = (m.N + 255) / 256;
+      k_rows_permute<<<nb, 256, 0, m.stream>>>(m.N, m.ilu_rank, (const double4 *)b, (double4 *)m.pb, 1);
+      fast ? kf_fast::sptrsv(m, m.pb, m.px, p) : kf_exact::sptrsv(m, m.pb, m.px, p);
+      k_rows_permute<<<nb, 256, 0, m.stream>>>(m.N, m.ilu_rank, (const double4 *)m.px, (double4 *)x, 0);
+      kf_count_launch(2);
+      return;
+    }
     fast ? kf_fast::sptrsv(m, b, x, p) : kf_exact::sptrsv(m, b, x, p);
   }
   void jv_combine(DevMesh &m, double *y, const double *r, const double *w, const double *q) const
@@ -511,12 +532,13 @@ void arnoldi_step_graph(DevMesh &m, const Ops &o, int k, int prec)
   const int fo = kf_first_order();
   double u, v;
   kfun3d_get_freestream(&u, &v);
-  if (m.graph_aoa != kfun3d_get_aoa()) {
+  if (m.graph_aoa != kfun3d_get_aoa() || m.graph_ilu != m.ilu_active) {
     for (auto &a : m.arnoldi)
       for (auto &b : a)
         for (auto &g : b)
           if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     m.graph_aoa = kfun3d_get_aoa();
+    m.graph_ilu = m.ilu_active;
   }
   cudaGraphExec_t &ge = m.arnoldi[prec][fo][k];
   if (!ge) {
@@ -1069,6 +1091,7 @@ namespace {
 DevMesh *dev_or_fail(const GEOMETRY *g)
 {
   DevMesh *m = kf_device(g);
+  if (m && kf_ilu_select(*m, g, kf_ilu_order()) != KFUN3D_OK) return nullptr;
   return m;
 }
 
@@ -1374,6 +1397,11 @@ extern "C" long kfun3d_matrix_read(const GEOMETRY *g, unsigned int *ia, unsigned
   if (blocks) {
     DevMesh *m = dev_or_fail(g);
     if (!m) return -1;
+    if (m->ilu_active) {
+      kf_set_error(KFUN3D_ERR_ARG, "kfun3d_matrix_read: the blocks are stored in the spatial ILU order; "
+                                   "select the mesh order (kfun3d_set_ilu_order(0)) first");
+      return -1;
+    }
     const size_t nv = 16 * p.nnz;
     if (kf_precision() == 0) {
       d2h(*m, blocks, m->A, nv);
