@@ -134,17 +134,18 @@ void kfun3d_set_precision(int p);
 /* Elimination order of ILU(0) and the triangular solves.
    0 = the mesh's node numbering (the reference: matrix/matrix.cpp factors
        rows in node order);
-   1 = spatial: rows and columns renumbered by a sweep of the node
-       coordinates (the mesh cut into one column per SM along (1,1,1),
-       column by column, ascending x + y + z within a column; P A P^T is
-       factored, x = P^T (LU)^-1 P b).  Same Jacobian blocks and sparsity, a different
+   1 = spatial: rows and columns renumbered by sweeps of the node
+       coordinates (s = x + y + z cut into 4 slabs, each swept from both
+       faces towards its middle; P A P^T is factored, x = P^T (LU)^-1 P b).  Same Jacobian blocks and sparsity, a different
        (and on randomly numbered meshes a much stronger) preconditioner; not
        a parity path.  Built on first use per mesh.  While it is active
        kfun3d_matrix_read(blocks) and kfun3d_sptrsv_device_noalloc return
        KFUN3D_ERR_ARG.
    KFUN3D_ILU_PERM in the environment, read when the order is built:
-   "sweep" renumbers by ascending x + y + z over the whole mesh, "morton" by
-   the Morton order of the coordinates;
+   "sweep" renumbers by ascending x + y + z over the whole mesh, "tiles" tile
+   by tile for the tiled triangular sweep (KFUN3D_SPTRSV=tiled), "morton" by
+   the Morton order of the coordinates; KFUN3D_ILU_SLABS sets the number of
+   slabs of the default order;
    "identity" keeps the mesh numbering through the same renumbering code
    (a test hook). */
 void kfun3d_set_ilu_order(int order);

@@ -176,7 +176,7 @@ def set_precision(p):
 
 def set_ilu_order(order):
     """Elimination order of ILU(0): 0 / "mesh" (the reference) or 1 / "spatial"
-    (the block pattern renumbered by a sweep of the node coordinates; not a parity path)."""
+    (the block pattern renumbered by sweeps of the node coordinates; not a parity path)."""
     if isinstance(order, str):
         order = {"mesh": 0, "spatial": 1}[order]
     lib().kfun3d_set_ilu_order(int(order))

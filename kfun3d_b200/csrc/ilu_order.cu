@@ -58,65 +58,136 @@ void activate(DevMesh &m, const IluSet &s)
   m.fill_blk = s.fill_blk; m.fill_diag = s.fill_diag; m.fill_last = s.fill_last; m.fill_lpos = s.fill_lpos;
   m.ntiles = s.ntiles; m.tile_ptr = s.tile_ptr; m.tile_step = s.tile_step; m.tile_pub = s.tile_pub;
   m.tile_wait = s.tile_wait; m.tile_desc = s.tile_desc; m.tile_prog = s.tile_prog;
+  m.tile_pack = s.tile_pack; m.tile_ndesc = s.tile_ndesc;
 }
 
 // Tiles of the tiled triangular sweep: columns along the sweep direction
 // (1,1,1), cut in the plane across it (u = x - y, w = x + y - 2z) into
-// floor(sqrt(T)) strips of equal node count by u, each strip into cells of
-// equal node count by w.  Tile ids run strip by strip.
+// floor(sqrt(T)) strips by u, each strip into cells by w, with equal shares
+// of the cross-section rather than of the nodes: a node weighs 1 / (the
+// extent in s = x + y + z of the nodes that project near it, on a 64 x 64
+// grid of the (u, w) plane), so every tile holds about the same number of
+// rows of each level.  Tile ids run strip by strip.
 std::vector<uint32_t> partition_tiles(const double *X, const double *Y, const double *Z, size_t N, uint32_t T)
 {
   std::vector<uint32_t> tile(N, 0);
   if (T <= 1 || N == 0) return tile;
   const uint32_t Tu = std::max(1u, (uint32_t)std::floor(std::sqrt((double)T)));
   std::vector<uint32_t> idx(N);
-  std::vector<double> u(N), w(N);
+  std::vector<double> u(N), w(N), sv(N), wt(N);
+  double ulo = 1e300, uhi = -1e300, wlo = 1e300, whi = -1e300;
   for (size_t i = 0; i < N; i++) {
     idx[i] = (uint32_t)i;
     u[i] = X[i] - Y[i];
     w[i] = (X[i] + Y[i]) - 2.0 * Z[i];
+    sv[i] = (X[i] + Y[i]) + Z[i];
+    ulo = std::min(ulo, u[i]); uhi = std::max(uhi, u[i]);
+    wlo = std::min(wlo, w[i]); whi = std::max(whi, w[i]);
   }
+  constexpr int B = 64;
+  auto bin = [&](size_t i) {
+    const int bu = (int)std::min<double>(B - 1, std::max(0.0, (u[i] - ulo) / std::max(uhi - ulo, 1e-300) * B));
+    const int bw = (int)std::min<double>(B - 1, std::max(0.0, (w[i] - wlo) / std::max(whi - wlo, 1e-300) * B));
+    return bu * B + bw;
+  };
+  std::vector<double> smin(B * B, 1e300), smax(B * B, -1e300);
+  double slo = 1e300, shi = -1e300;
+  for (size_t i = 0; i < N; i++) {
+    const int k = bin(i);
+    smin[k] = std::min(smin[k], sv[i]);
+    smax[k] = std::max(smax[k], sv[i]);
+    slo = std::min(slo, sv[i]);
+    shi = std::max(shi, sv[i]);
+  }
+  const double floor_ext = std::max(shi - slo, 1e-300) / 64.0;
+  double total = 0.0;
+  for (size_t i = 0; i < N; i++) {
+    const int k = bin(i);
+    wt[i] = 1.0 / std::max(smax[k] - smin[k], floor_ext);
+    total += wt[i];
+  }
+  // consecutive runs of idx[a, b) with equal shares of weight
+  auto cut = [&](size_t a, size_t b, uint32_t parts, double share, auto &&emit) {
+    double acc = 0.0;
+    uint32_t part = 0;
+    size_t c0 = a;
+    for (size_t q = a; q < b; q++) {
+      acc += wt[idx[q]];
+      if (part + 1 < parts && acc >= share * (part + 1)) {
+        emit(part, c0, q + 1);
+        c0 = q + 1;
+        part++;
+      }
+    }
+    emit(part, c0, b);
+    for (uint32_t rest = part + 1; rest < parts; rest++) emit(rest, b, b);
+  };
   std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return u[a] < u[b]; });
-  size_t start = 0;
+  // strip k takes cells[k] / T of the weight
+  std::vector<uint32_t> cells(Tu);
+  for (uint32_t k = 0; k < Tu; k++) cells[k] = T / Tu + (k < T % Tu ? 1u : 0u);
+  std::vector<std::pair<size_t, size_t>> strips(Tu, {N, N});
+  {
+    double acc = 0.0, target = total * cells[0] / T;
+    size_t start = 0;
+    uint32_t k = 0;
+    for (size_t q = 0; q < N && k + 1 < Tu; q++) {
+      acc += wt[idx[q]];
+      if (acc >= target) {
+        strips[k] = {start, q + 1};
+        start = q + 1;
+        k++;
+        target += total * cells[k] / T;
+      }
+    }
+    strips[k] = {start, N};
+  }
   uint32_t t0 = 0;
   for (uint32_t k = 0; k < Tu; k++) {
-    const uint32_t cells = T / Tu + (k < T % Tu ? 1u : 0u);
-    const size_t end = (size_t)((unsigned __int128)N * (t0 + cells) / T);
-    std::stable_sort(idx.begin() + start, idx.begin() + end, [&](uint32_t a, uint32_t b) { return w[a] < w[b]; });
-    const size_t len = end - start;
-    for (uint32_t c = 0; c < cells; c++) {
-      const size_t c0 = start + len * c / cells, c1 = start + len * (c + 1) / cells;
+    const size_t a = strips[k].first, b = strips[k].second;
+    std::stable_sort(idx.begin() + a, idx.begin() + b, [&](uint32_t x0, uint32_t x1) { return w[x0] < w[x1]; });
+    double sw = 0.0;
+    for (size_t q = a; q < b; q++) sw += wt[idx[q]];
+    cut(a, b, cells[k], sw / cells[k], [&](uint32_t c, size_t c0, size_t c1) {
       for (size_t q = c0; q < c1; q++) tile[idx[q]] = t0 + c;
-    }
-    start = end;
-    t0 += cells;
+    });
+    t0 += cells[k];
   }
   return tile;
 }
 
 // Position of every node in the spatial elimination order.  ILU(0) depends
-// only on which of two neighbours is eliminated first.
-//   tiles (default): tile by tile (ids as above), within a tile ascending
-//     x + y + z.  Inside a tile the edges are oriented as a sweep orients
-//     them -- much as the lexicographic order of a lattice does, the strong
-//     ordering -- and between tiles from the lower tile id to the higher, so
-//     that the tiled sweep's CTAs depend on their neighbours in one direction
+// only on which of two neighbours is eliminated first; orders that follow a
+// sweep of the coordinates orient the edges as the lexicographic order of a
+// lattice does (the strong ordering) while keeping the level sets few.  With
+// s = x + y + z:
+//   slabs (default): the range of s cut into K slabs (KFUN3D_ILU_SLABS,
+//     default 4), each swept from both of its faces towards its middle
+//     (descending |s - middle of the slab|, ties in node order).  On the
+//     120^3 box: 803 GMRES iterations and a 2.1 ms FP32 triangular solve,
+//     against 728 and 2.7 ms for K = 1, 704 and 3.6 ms for one sweep, 1556
+//     and 1.3 ms in the mesh's random numbering;
+//   KFUN3D_ILU_PERM=tiles: tile by tile (ids as above), ascending s within a
+//     tile: between tiles the edges point from the lower tile id to the
+//     higher, so the tiled sweep's CTAs depend on their neighbours one way
 //     only and run as a pipeline;
-//   KFUN3D_ILU_PERM=sweep: ascending x + y + z over the whole mesh, ties in
-//     node order (level sets: about 3n on an n^3 Kuhn box, against about
-//     9n for the Morton order of the jittered coordinates);
+//   KFUN3D_ILU_PERM=sweep: ascending s over the whole mesh (level sets: about
+//     3n on an n^3 Kuhn box, against about 9n for the Morton order of the
+//     jittered coordinates);
 //   KFUN3D_ILU_PERM=morton: Morton order of the coordinates, 21 bits per axis
-//     over the bounding box, ties in node order;
+//     over the bounding box;
 //   KFUN3D_ILU_PERM=identity: the mesh's own order through the renumbering
 //     code (reproduces the mesh order bit for bit; a test hook).
+// Ties keep node order in every case.
 std::vector<uint32_t> spatial_rank(const GEOMETRY *g, size_t N, const std::vector<uint32_t> &tile)
 {
   std::vector<uint32_t> rank(N), ord(N);
   for (size_t i = 0; i < N; i++) ord[i] = (uint32_t)i;
   const char *env = getenv("KFUN3D_ILU_PERM");
-  if (env && strcmp(env, "identity") == 0) return ord;
+  const std::string kind = env ? env : "slabs";
+  if (kind == "identity") return ord;
   const double *X = g->n->xyz->x0, *Y = g->n->xyz->x1, *Z = g->n->xyz->x2;
-  if (env && strcmp(env, "morton") == 0) {
+  if (kind == "morton") {
     double lo[3] = {X[0], Y[0], Z[0]}, hi[3] = {X[0], Y[0], Z[0]};
     for (size_t i = 0; i < N; i++) {
       const double c[3] = {X[i], Y[i], Z[i]};
@@ -146,19 +217,33 @@ std::vector<uint32_t> spatial_rank(const GEOMETRY *g, size_t N, const std::vecto
   } else {
     std::vector<double> key(N);
     for (size_t i = 0; i < N; i++) key[i] = (X[i] + Y[i]) + Z[i];
-    if (env && strcmp(env, "sweep") == 0)
-      std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
-    else
+    if (kind == "tiles") {
       std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
         return tile[a] != tile[b] ? tile[a] < tile[b] : key[a] < key[b];
       });
+    } else {
+      if (kind != "sweep") {
+        double lo = 1e300, hi = -1e300;
+        for (size_t i = 0; i < N; i++) { lo = std::min(lo, key[i]); hi = std::max(hi, key[i]); }
+        int K = 4;
+        const char *kenv = getenv("KFUN3D_ILU_SLABS");
+        if (kenv && atoi(kenv) >= 1 && atoi(kenv) <= 64) K = atoi(kenv);
+        const double w = std::max((hi - lo) / K, 1e-300);
+        for (size_t i = 0; i < N; i++) {
+          const int sl = std::min(K - 1, (int)((key[i] - lo) / w));
+          key[i] = -std::fabs(key[i] - (lo + (sl + 0.5) * w));
+        }
+      }
+      std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+    }
   }
   for (size_t p = 0; p < N; p++) rank[ord[p]] = (uint32_t)p;
   return rank;
 }
 
 // Host form of the tiled sweep: per tile its rows of each sweep grouped by
-// level (a step; longest rows first), and before each step the progress it
+// level (a step, at most KF_TILE_STEP_ROWS rows; longest rows first; desc.w
+// = 1 in the upper sweep), and before each step the progress it
 // needs from other tiles -- for every row of the step and every column row
 // j held by another tile t', progress[t'] >= (level of j) + 1 in the lower
 // sweep, nlev_l + (backward level of j) + 1 in the upper sweep -- keeping
@@ -222,16 +307,19 @@ TileHost build_tiles(const HostPattern &p, const std::vector<uint32_t> &rank, co
         return lev(a) != lev(b) ? lev(a) < lev(b) : len(a) > len(b);
       });
       for (size_t q0 = 0; q0 < rows.size();) {
-        size_t q1 = q0;
+        size_t qe = q0;
         const uint32_t L = lev(rows[q0]);
-        while (q1 < rows.size() && lev(rows[q1]) == L) q1++;
+        while (qe < rows.size() && lev(rows[qe]) == L) qe++;
+        // a level of more than KF_TILE_STEP_ROWS rows takes several steps;
+        // only the last one completes the level
+        const size_t q1 = std::min(qe, q0 + KF_TILE_STEP_ROWS);
         uint4 st = make_uint4((uint32_t)h.desc.size(), 0, 0, 0);
         h.raw_ptr.push_back((uint32_t)h.raw.size());
         const size_t r0 = h.raw.size();
         for (size_t q = q0; q < q1; q++) {
           const uint32_t i = rows[q];
           const uint32_t jb = upper ? p.diag[i] + 1 : p.ia[i], je = upper ? p.ia[i + 1] : p.diag[i];
-          h.desc.push_back(make_uint4(i, jb, je, 0));
+          h.desc.push_back(make_uint4(i, jb, je, (uint32_t)upper));
           for (uint32_t j = jb; j < je; j++) {
             const uint32_t c = p.ja[j], tc = rt[c];
             if (tc == t) continue;
@@ -244,7 +332,8 @@ TileHost build_tiles(const HostPattern &p, const std::vector<uint32_t> &rank, co
         }
         st.y = (uint32_t)h.desc.size();
         h.step.push_back(st);
-        h.pub.push_back(upper ? nl + L + 1 : L + 1);
+        if (q1 == qe) h.pub.push_back(upper ? nl + L + 1 : L + 1);
+        else h.pub.push_back(h.pub.empty() ? 0u : h.pub.back());
         q0 = q1;
       }
     }
@@ -398,6 +487,7 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
     up(&s.tile_wait, th.wait);
     up(&s.tile_desc, th.desc);
     if (ok && cudaMalloc(&s.tile_prog, T * sizeof(unsigned)) != cudaSuccess) ok = false;
+    s.tile_ndesc = (uint32_t)th.desc.size();
   }
   up(&m.ilu_rank, rank);
   if (ok && cudaMalloc(&m.pb, 4 * N * sizeof(double)) != cudaSuccess) ok = false;
@@ -409,6 +499,14 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
   s.trsv_mode = 4;
   const char *env = getenv("KFUN3D_SPTRSV");
   if (env && strcmp(env, "tiled") == 0) s.trsv_mode = 6;
+  if (ok && s.trsv_mode == 6) {
+    // the packed FP32 factor of the tiled sweep (without room for it the
+    // FP32 solves take the unpacked one)
+    if (cudaMalloc(&s.tile_pack, (size_t)s.tile_ndesc * KF_TILE_REC) != cudaSuccess) {
+      cudaGetLastError();
+      s.tile_pack = nullptr;
+    }
+  }
   if (env && strcmp(env, "mono") == 0) s.trsv_mode = 5;
   if (env && strcmp(env, "levels16") == 0) s.trsv_mode = 2;
   if (env && strcmp(env, "syncfree") == 0) s.trsv_mode = 1;
@@ -450,7 +548,7 @@ void kf_ilu_release(DevMesh &m)
   IluSet &s = m.iset[1];
   void *ptrs[] = {s.ia, s.ja, s.diag, s.tblk, s.lpos, s.last_lower, s.pair_ptr, s.pairs, s.lev_l, s.lev_u,
                   s.lev_ptr_d, s.desc_l, s.desc_u, s.fill_blk, s.fill_diag, s.fill_last, s.fill_lpos,
-                  s.tile_ptr, s.tile_step, s.tile_pub, s.tile_wait, s.tile_desc, s.tile_prog,
+                  s.tile_ptr, s.tile_step, s.tile_pub, s.tile_wait, s.tile_desc, s.tile_prog, s.tile_pack,
                   m.ilu_rank, m.pb, m.px};
   for (void *p : ptrs)
     if (p) cudaFree(p);

@@ -92,6 +92,9 @@ __device__ __forceinline__ bool kf_grid_barrier(unsigned *bar, int *err)
 // spatial order (set 1, kfun3d_set_ilu_order).  fill_* are indexed by node in
 // the mesh's numbering and point into the set's pattern.  tile_*: the tiled
 // triangular sweep of set 1 (one CTA per tile, trsv_mode 6).
+constexpr uint32_t KF_TILE_STEP_ROWS = 96;   // rows of a step of the tiled sweep, at most
+constexpr uint32_t KF_TILE_REC = 624;         // bytes of a row record of the packed FP32 factor
+
 struct IluSet {
   bool valid = false;
   uint32_t *ia = nullptr, *ja = nullptr, *diag = nullptr, *tblk = nullptr, *lpos = nullptr;
@@ -113,6 +116,8 @@ struct IluSet {
   uint2 *tile_wait = nullptr;      // (tile, progress it must have reached)
   uint4 *tile_desc = nullptr;      // [2N] row descriptors (row, first block, end block), by tile and step
   unsigned *tile_prog = nullptr;   // [T] progress counters, cleared before each solve
+  uint8_t *tile_pack = nullptr;    // [2N x KF_TILE_REC] FP32 factor rows in tile_desc order
+  uint32_t tile_ndesc = 0;
 };
 
 // Device mirror of one GEOMETRY.  Node-indexed arrays follow the reference's
@@ -209,6 +214,8 @@ struct DevMesh {
   uint4 *tile_step = nullptr, *tile_desc = nullptr;
   uint2 *tile_wait = nullptr;
   unsigned *tile_prog = nullptr;
+  uint8_t *tile_pack = nullptr;
+  uint32_t tile_ndesc = 0;
   int ilu_active = 0;             // 1: the spatial set is active
   uint32_t *ilu_rank = nullptr;   // [N] row of each node in the spatial set
   double *pb = nullptr, *px = nullptr;   // [4N] right-hand side and solution, spatial numbering

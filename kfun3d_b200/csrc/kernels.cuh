@@ -1710,23 +1710,40 @@ __global__ void __launch_bounds__(256, 4) k_trsv_syncfree(uint32_t N, const uint
 // The tiled sweep of the spatial ILU(0) order: both triangular sweeps in one
 // cooperative launch of one 512-thread CTA per tile (rows of a tile: a column
 // of the mesh along the sweep direction).  Warps 0-14 work the tile's steps
-// in order -- the rows of one level that it holds, G lanes per row,
-// arithmetic as in k_trsv_level16 -- separated by a barrier of those warps
-// only.  Before a step warp 0 makes sure the other tiles the step reads from
-// have reached the progress computed on the host: it issues those reads one
-// step ahead and polls only what was not yet there.  Warp 15 publishes: it
-// follows the count of completed steps in shared memory and stores the
-// tile's progress (release) when a step another tile waits for (bit 31 of
-// pub) is complete, so the fence stays off the compute warps' path.
-// Everything that does not depend on x -- row descriptors two steps ahead,
-// columns, first blocks, diagonal block and right-hand side one step ahead --
-// is loaded before it is needed.  With every tile resident and every
-// requirement naming a strictly earlier level, the sweep cannot deadlock.  A
-// wait that exceeds its bound records an error in *err and the tile stops;
-// the others give up at their next look at *err.
-constexpr uint32_t KF_TILE_IDLE_LIMIT = 1u << 27;   // publisher polls of shared memory without news
+// in order -- the rows of one level that it holds, G lanes per row and up to
+// P rows per group, arithmetic as in k_trsv_level16 -- separated by a
+// barrier of those warps only.  Warp 15 talks to the other tiles: it checks,
+// steps ahead, that the tiles a step reads from have reached the progress
+// computed on the host (acquire) and posts the last step cleared in shared
+// memory; and it follows the count of completed steps and stores the tile's
+// progress (release) when a step another tile waits for (bit 31 of pub) is
+// complete.  The compute warps thus see neither polls of other tiles nor
+// fences.  Everything that does not depend on x -- step records three steps
+// ahead, row descriptors two, columns, first blocks, diagonal blocks and
+// right-hand sides one -- is loaded before it is needed.  With every tile
+// resident and every requirement naming a strictly earlier level, the sweep
+// cannot deadlock.  Waits are bounded: one that runs out records an error in
+// *err and the tile stops; the others give up at their next look at *err.
+constexpr uint32_t KF_TILE_IDLE_LIMIT = 1u << 26;   // polls without news before a wait is declared failed
 
-template <typename T, int G>
+__device__ __forceinline__ uint32_t ld_acquire_cta_shared(const uint32_t *p)
+{
+  uint32_t v;
+  asm volatile("ld.acquire.cta.shared.u32 %0, [%1];" : "=r"(v) : "r"((uint32_t)__cvta_generic_to_shared(p)) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release_cta_shared(uint32_t *p, uint32_t v)
+{
+  asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(p)), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void prefetch_l1(const void *p)
+{
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+template <typename T, int G, int P>
 __global__ void __launch_bounds__(512, 1) k_trsv_tiled(const uint32_t *__restrict__ tptr,
                                                        const uint4 *__restrict__ steps,
                                                        const uint32_t *__restrict__ pub,
@@ -1741,28 +1758,48 @@ __global__ void __launch_bounds__(512, 1) k_trsv_tiled(const uint32_t *__restric
   constexpr uint32_t NCT = NCW * 32;
   __shared__ int fail_s;
   __shared__ uint32_t done_s;                   // steps completed
+  __shared__ uint32_t ready_s;                  // steps whose requirements are met
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t t = blockIdx.x;
   const uint32_t k0 = tptr[2 * t], k1 = tptr[2 * t + 1], k2 = tptr[2 * t + 2];
-  if (threadIdx.x == 0) { fail_s = 0; done_s = k0; }
+  if (threadIdx.x == 0) { fail_s = 0; done_s = k0; ready_s = k0; }
   __syncthreads();
   if (warp == NCW) {
-    // publisher
-    if (lane == 0) {
-      uint32_t published = k0, idle = 0;
-      while (published < k2) {
-        uint32_t done;
-        asm volatile("ld.acquire.cta.shared.u32 %0, [%1];" : "=r"(done) : "r"((uint32_t)__cvta_generic_to_shared(&done_s)) : "memory");
-        if (done > published) {
+    // the tile's link to the others
+    uint32_t published = k0, ready = k0, idle = 0;
+    while (published < k2) {
+      bool news = false;
+      const uint32_t done = __shfl_sync(0xffffffffu, ld_acquire_cta_shared(&done_s), 0);
+      if (done > published) {
+        if (lane == 0)
           for (uint32_t kk = done; kk-- > published;) {
             const uint32_t pv = pub[kk];
             if (pv >> 31) { st_release(prog + t, pv & 0x7fffffffu); break; }
           }
-          published = done;
-          idle = 0;
-        } else if (++idle > KF_TILE_IDLE_LIMIT || ((idle & 255) == 0 && (*(volatile int *)&fail_s || *(volatile int *)err))) {
-          break;
+        published = done;
+        news = true;
+      }
+      if (ready < k2 && ready < done + 3) {
+        const uint4 sr = steps[ready];
+        bool ok = true;
+        for (uint32_t w = sr.z + lane; w < sr.w; w += 32) {
+          const uint2 wt = waits[w];
+          if (ld_acquire(prog + wt.x) < wt.y) ok = false;
         }
+        if (__all_sync(0xffffffffu, ok)) {
+          ready++;
+          if (lane == 0) st_release_cta_shared(&ready_s, ready);
+          news = true;
+        }
+      }
+      if (news) {
+        idle = 0;
+      } else if (++idle > KF_TILE_IDLE_LIMIT) {
+        if (lane == 0) { atomicExch(err, 1); fail_s = 1; }
+        break;
+      } else if ((idle & 255) == 0 && (*(volatile int *)&fail_s || *(volatile int *)err)) {
+        if (lane == 0) fail_s = 1;
+        break;
       }
     }
     return;
@@ -1770,76 +1807,88 @@ __global__ void __launch_bounds__(512, 1) k_trsv_tiled(const uint32_t *__restric
   const int gl = lane & (G - 1), base = lane - gl, jj = gl >> 2, r = gl & 3;
   const unsigned gmask = ((1u << G) - 1u) << base;
   const uint32_t R = NCT / G, h = threadIdx.x / G;
-  // descriptor of this group's first row in step k (w = 1 when there is one)
-  auto load_desc = [&](uint32_t k) -> uint4 {
-    uint4 dd = make_uint4(0, 0, 0, 0);
-    if (k < k2) {
-      const uint4 sk = steps[k];
-      if (sk.x + h < sk.y) { dd = tdesc[sk.x + h]; dd.w = 1; }
-    }
-    return dd;
+  // into L1 ahead of use: the row descriptors of step k, and through them
+  // each row's columns, blocks (from the diagonal block on in the upper
+  // sweep) and right-hand side
+  auto prefetch_desc = [&](uint32_t k) {
+    if (k >= k2) return;
+    const uint4 rec = steps[k];
+    const char *p0 = reinterpret_cast<const char *>(tdesc + rec.x), *p1 = reinterpret_cast<const char *>(tdesc + rec.y);
+    for (const char *q = p0 + 128 * threadIdx.x; q < p1; q += 128 * NCT) prefetch_l1(q);
+    if (threadIdx.x == 0) prefetch_l1(steps + k + 8);
   };
-  uint32_t col[4];
-  T a[4][4], dg[4];
-  double xb = 0.0;
-  auto load_blocks = [&](uint32_t k, const uint4 dd) {
-#pragma unroll
-    for (int p = 0; p < 4; p++) {
-      col[p] = 0xffffffffu;
-#pragma unroll
-      for (int c = 0; c < 4; c++) a[p][c] = (T)0;
-    }
-    if (!dd.w) return;
-#pragma unroll
-    for (int p = 0; p < 4; p++) {
-      const uint32_t j = dd.y + S * p + jj;
-      if (j < dd.z) {
-        col[p] = ja[j];
-        const T *blk = A + 16 * (size_t)j + 4 * r;
-#pragma unroll
-        for (int c = 0; c < 4; c++) a[p][c] = blk[c];
-      }
-    }
-    if (k >= k1) {
-      const T *blk = A + 16 * (size_t)(dd.y - 1) + 4 * r;
-#pragma unroll
-      for (int c = 0; c < 4; c++) dg[c] = blk[c];
-    } else {
-      xb = b[4 * (size_t)dd.x + r];
+  auto prefetch_rows = [&](uint32_t k) {
+    if (k >= k2) return;
+    const uint4 rec = steps[k];
+    const bool up = k >= k1;
+    for (uint32_t sl = rec.x + h; sl < rec.y; sl += R) {
+      const uint4 dd = tdesc[sl];
+      const uint32_t j0 = up ? dd.y - 1 : dd.y;
+      const char *p0 = reinterpret_cast<const char *>(A + 16 * (size_t)j0);
+      const char *p1 = reinterpret_cast<const char *>(A + 16 * (size_t)dd.z);
+      const char *q = p0 + 128 * gl;
+      if (q < p1) prefetch_l1(q);
+      if (gl == 0) prefetch_l1(ja + dd.y);
+      if (gl == 1 && !up) prefetch_l1(b + 4 * (size_t)dd.x);
     }
   };
-  uint4 st = k0 < k2 ? steps[k0] : make_uint4(0, 0, 0, 0);
-  uint4 d = load_desc(k0);
-  load_blocks(k0, d);
-  uint4 d1 = load_desc(k0 + 1);
-  uint32_t pre = 0;   // warp 0: progress of the lane's first requirement of the coming step, read ahead
-  if (warp == 0 && st.z + lane < st.w) pre = ld_acquire(prog + waits[st.z + lane].x);
+  prefetch_desc(k0);
+  prefetch_desc(k0 + 1);
+  prefetch_desc(k0 + 2);
+  prefetch_rows(k0);
+  prefetch_rows(k0 + 1);
   for (uint32_t k = k0; k < k2; k++) {
-    if (warp == 0 && st.z < st.w) {
-      bool bad = false;
-      for (uint32_t w = st.z + lane; w < st.w && !bad; w += 32) {
-        const uint2 wt = waits[w];
-        if (w == st.z + lane && pre >= wt.y) continue;
-        uint32_t spins = 0;
-        while (ld_acquire(prog + wt.x) < wt.y) {
-          if (++spins > KF_SPIN_LIMIT) { atomicExch(err, 1); bad = true; break; }
-          if ((spins & 255) == 0 && *(volatile int *)err) { bad = true; break; }
-        }
+    if (threadIdx.x == 0) {
+      uint32_t spins = 0;
+      while (ld_acquire_cta_shared(&ready_s) <= k) {
+        if (*(volatile int *)&fail_s) break;
+        if (++spins > KF_TILE_IDLE_LIMIT) { atomicExch(err, 1); fail_s = 1; break; }
       }
-      if (bad) fail_s = 1;
     }
     asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
     if (*(volatile int *)&fail_s) return;
-    const uint4 cur = st;
+    const uint4 cur = steps[k];
     const bool upper = k >= k1;
-    // ahead: the next step's record and requirements, the descriptor two steps on
-    if (k + 1 < k2) st = steps[k + 1];
-    const uint4 d2 = load_desc(k + 2);
-    if (warp == 0 && k + 1 < k2 && st.z + lane < st.w) pre = ld_acquire(prog + waits[st.z + lane].x);
-    if (d.w) {
-      // the prefetched first pass: arithmetic as trsv_row_g
-      const uint32_t i = d.x, jb = d.y, je = d.z;
-      double xi = upper ? __ldcg(x + 4 * (size_t)i + r) : xb;
+    // up to P rows per group: every load first, then the arithmetic of trsv_row_g
+    uint4 d[P];
+    uint32_t col[P][4];
+    T a[P][4][4], dg[P][4];
+    double xi[P];
+#pragma unroll
+    for (int q = 0; q < P; q++) {
+      const uint32_t sl = cur.x + h + R * q;
+      d[q] = make_uint4(0, 0, 0, 0);
+      if (sl < cur.y) { d[q] = tdesc[sl]; d[q].w = 1; }
+    }
+#pragma unroll
+    for (int q = 0; q < P; q++) {
+      xi[q] = 0.0;
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        col[q][p] = 0xffffffffu;
+        const uint32_t j = d[q].y + S * p + jj;
+        if (d[q].w && j < d[q].z) {
+          col[q][p] = ja[j];
+          const T *blk = A + 16 * (size_t)j + 4 * r;
+#pragma unroll
+          for (int c = 0; c < 4; c++) a[q][p][c] = blk[c];
+        }
+      }
+      if (d[q].w) {
+        if (upper) {
+          const T *blk = A + 16 * (size_t)(d[q].y - 1) + 4 * r;
+#pragma unroll
+          for (int c = 0; c < 4; c++) dg[q][c] = blk[c];
+          xi[q] = __ldcg(x + 4 * (size_t)d[q].x + r);
+        } else {
+          xi[q] = b[4 * (size_t)d[q].x + r];
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < P; q++) {
+      if (!d[q].w) continue;
+      const uint32_t jb = d[q].y, je = d[q].z;
       for (uint32_t c0 = jb; c0 < je; c0 += 4 * S) {
         double tp[4];
 #pragma unroll
@@ -1847,8 +1896,8 @@ __global__ void __launch_bounds__(512, 1) k_trsv_tiled(const uint32_t *__restric
           const uint32_t j = c0 + S * p + jj;
           tp[p] = 0.0;
           if (j < je) {
-            uint32_t cc = col[p];
-            double a0 = (double)a[p][0], a1 = (double)a[p][1], a2 = (double)a[p][2], a3 = (double)a[p][3];
+            uint32_t cc = col[q][p];
+            double a0 = (double)a[q][p][0], a1 = (double)a[q][p][1], a2 = (double)a[q][p][2], a3 = (double)a[q][p][3];
             if (c0 != jb) {
               cc = ja[j];
               const T *blk = A + 16 * (size_t)j + 4 * r;
@@ -1867,35 +1916,239 @@ __global__ void __launch_bounds__(512, 1) k_trsv_tiled(const uint32_t *__restric
         const uint32_t cnt = (je - c0) < (uint32_t)(4 * S) ? (je - c0) : (uint32_t)(4 * S);
 #pragma unroll
         for (int p = 0; p < 4; p++)
-          for (int q = 0; q < S; q++) {
-            if ((uint32_t)(S * p + q) >= cnt) break;
-            xi = -1.0 * __shfl_sync(gmask, tp[p], base + 4 * q + r) + xi;
+          for (int qq = 0; qq < S; qq++) {
+            if ((uint32_t)(S * p + qq) >= cnt) break;
+            xi[q] = -1.0 * __shfl_sync(gmask, tp[p], base + 4 * qq + r) + xi[q];
           }
       }
       if (upper) {
+        const double x0 = __shfl_sync(gmask, xi[q], base + 0), x1 = __shfl_sync(gmask, xi[q], base + 1);
+        const double x2 = __shfl_sync(gmask, xi[q], base + 2), x3 = __shfl_sync(gmask, xi[q], base + 3);
+        double y = 0.0;
+        y += (double)dg[q][0] * x0;
+        y += (double)dg[q][1] * x1;
+        y += (double)dg[q][2] * x2;
+        y += (double)dg[q][3] * x3;
+        xi[q] = y;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < P; q++)
+      if (d[q].w && gl < 4) __stcg(x + 4 * (size_t)d[q].x + r, xi[q]);
+    // rows beyond those
+    if (upper)
+      for (uint32_t s = cur.x + h + R * P; s < cur.y; s += R) trsv_row_g<T, true, G>(tdesc[s], ja, A, b, x, base, gl, gmask);
+    else
+      for (uint32_t s = cur.x + h + R * P; s < cur.y; s += R) trsv_row_g<T, false, G>(tdesc[s], ja, A, b, x, base, gl, gmask);
+    prefetch_desc(k + 3);
+    prefetch_rows(k + 2);
+    asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
+    if (threadIdx.x == 0) st_release_cta_shared(&done_s, k + 1);
+  }
+}
+
+// The FP32 factor rows of the tiled sweep packed in step order, one
+// KF_TILE_REC-byte record per row of tile_desc (a warp per record, 16 bytes
+// a lane): the row, its block count in the record (at most 8), first and end
+// block (uint32 x 4); the columns of its first 8 blocks (uint32 x 8); those
+// blocks (float x 16 each); and in the upper sweep the inverted diagonal
+// block (float x 16).  Rewritten after every FP32 factorisation.
+__global__ void k_tile_pack(uint32_t ndesc, const uint4 *__restrict__ tdesc, const uint32_t *__restrict__ ja,
+                            const float *__restrict__ Af, uint8_t *__restrict__ pack)
+{
+  const uint32_t slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (slot >= ndesc) return;
+  const uint4 d = tdesc[slot];
+  const uint32_t jb = d.y, je = d.z, nb = je - jb < 8 ? je - jb : 8;
+  uint4 *dst = reinterpret_cast<uint4 *>(pack + (size_t)slot * KF_TILE_REC);
+  for (uint32_t c = lane; c < KF_TILE_REC / 16; c += 32) {
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (c == 0) {
+      v = make_uint4(d.x, nb, jb, je);
+    } else if (c < 3) {
+      uint32_t w[4];
+      for (int e = 0; e < 4; e++) {
+        const uint32_t k = 4 * (c - 1) + e;
+        w[e] = k < nb ? ja[jb + k] : 0u;
+      }
+      v = make_uint4(w[0], w[1], w[2], w[3]);
+    } else if (c < 35) {
+      const uint32_t k = (c - 3) >> 2, quarter = (c - 3) & 3;
+      if (k < nb) v = *reinterpret_cast<const uint4 *>(Af + 16 * (size_t)(jb + k) + 4 * quarter);
+    } else if (d.w) {
+      v = *reinterpret_cast<const uint4 *>(Af + 16 * (size_t)(jb - 1) + 4 * (c - 35));
+    }
+    dst[c] = v;
+  }
+}
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)), "l"(gmem)
+               : "memory");
+}
+
+// The tiled sweep on the packed FP32 factor: the schedule of k_trsv_tiled
+// (same steps, requirements and link warp), but every step's row records
+// arrive in shared memory by asynchronous copies issued two steps ahead (a
+// ring of three stages; issued after the step's own x reads), so a row
+// waits on nothing but its x reads.  Four lanes per row, lane r keeping
+// component r: each block's product is summed from zero and subtracted in
+// block order (the arithmetic of k_trsv_level16) with no reduction across
+// lanes.  Rows with more than 8 blocks take the rest from ja / Af.
+template <int G>
+__global__ void __launch_bounds__(512, 1) k_trsv_tiled_packed(const uint32_t *__restrict__ tptr,
+                                                              const uint4 *__restrict__ steps,
+                                                              const uint32_t *__restrict__ pub,
+                                                              const uint2 *__restrict__ waits,
+                                                              const uint8_t *__restrict__ pack,
+                                                              const uint32_t *__restrict__ ja,
+                                                              const float *__restrict__ Af,
+                                                              const double *__restrict__ b, double *x,
+                                                              uint32_t *prog, int *err)
+{
+  constexpr int S = G / 4;
+  constexpr int NCW = 15;
+  constexpr uint32_t NCT = NCW * 32;
+  constexpr uint32_t NST = 3, STAGE = KF_TILE_STEP_ROWS * KF_TILE_REC;
+  extern __shared__ __align__(16) uint8_t ring[];
+  __shared__ int fail_s;
+  __shared__ uint32_t done_s, ready_s;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t t = blockIdx.x;
+  const uint32_t k0 = tptr[2 * t], k1 = tptr[2 * t + 1], k2 = tptr[2 * t + 2];
+  if (threadIdx.x == 0) { fail_s = 0; done_s = k0; ready_s = k0; }
+  __syncthreads();
+  if (warp == NCW) {
+    uint32_t published = k0, ready = k0, idle = 0;
+    while (published < k2) {
+      bool news = false;
+      const uint32_t done = __shfl_sync(0xffffffffu, ld_acquire_cta_shared(&done_s), 0);
+      if (done > published) {
+        if (lane == 0)
+          for (uint32_t kk = done; kk-- > published;) {
+            const uint32_t pv = pub[kk];
+            if (pv >> 31) { st_release(prog + t, pv & 0x7fffffffu); break; }
+          }
+        published = done;
+        news = true;
+      }
+      if (ready < k2 && ready < done + 3) {
+        const uint4 sr = steps[ready];
+        bool ok = true;
+        for (uint32_t w = sr.z + lane; w < sr.w; w += 32) {
+          const uint2 wt = waits[w];
+          if (ld_acquire(prog + wt.x) < wt.y) ok = false;
+        }
+        if (__all_sync(0xffffffffu, ok)) {
+          ready++;
+          if (lane == 0) st_release_cta_shared(&ready_s, ready);
+          news = true;
+        }
+      }
+      if (news) {
+        idle = 0;
+      } else if (++idle > KF_TILE_IDLE_LIMIT) {
+        if (lane == 0) { atomicExch(err, 1); fail_s = 1; }
+        break;
+      } else if ((idle & 255) == 0 && (*(volatile int *)&fail_s || *(volatile int *)err)) {
+        if (lane == 0) fail_s = 1;
+        break;
+      }
+    }
+    return;
+  }
+  // four lanes per row, lane r = component r: each lane subtracts the row's
+  // block products one block at a time, so no reduction across lanes
+  const int r = lane & 3, base = lane & ~3;
+  const unsigned gmask = 0xfu << base;
+  const uint32_t R = NCT / 4, h = threadIdx.x >> 2;
+  static_assert(KF_TILE_STEP_ROWS <= NCT / 4, "one pass of rows per step");
+  auto issue = [&](uint32_t k) {
+    if (k < k2) {
+      const uint4 rec = steps[k];
+      const uint8_t *src = pack + (size_t)rec.x * KF_TILE_REC;
+      const uint32_t bytes = (rec.y - rec.x) * KF_TILE_REC;
+      uint8_t *dst = ring + (k % NST) * STAGE;
+      for (uint32_t off = threadIdx.x * 16; off < bytes; off += NCT * 16) cp_async16(dst + off, src + off);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  issue(k0);
+  issue(k0 + 1);
+  uint4 cur = k0 < k2 ? steps[k0] : make_uint4(0, 0, 0, 0);
+  for (uint32_t k = k0; k < k2; k++) {
+    if (threadIdx.x == 0) {
+      uint32_t spins = 0;
+      while (ld_acquire_cta_shared(&ready_s) <= k) {
+        if (*(volatile int *)&fail_s) break;
+        if (++spins > KF_TILE_IDLE_LIMIT) { atomicExch(err, 1); fail_s = 1; break; }
+      }
+    }
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
+    asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
+    if (*(volatile int *)&fail_s) {
+      asm volatile("cp.async.wait_all;" ::: "memory");
+      return;
+    }
+    const bool upper = k >= k1;
+    const uint8_t *stage = ring + (k % NST) * STAGE;
+    const uint32_t nrows = cur.y - cur.x;
+    uint32_t row_i = 0;
+    double xi = 0.0;
+    if (h < nrows) {
+      const uint8_t *rec = stage + h * KF_TILE_REC;
+      const uint4 hd = *reinterpret_cast<const uint4 *>(rec);
+      const uint32_t *cols = reinterpret_cast<const uint32_t *>(rec + 16);
+      const float *blks = reinterpret_cast<const float *>(rec + 48);
+      const uint32_t i = hd.x, nb = hd.y, jb = hd.z, je = hd.w;
+      row_i = i;
+      xi = upper ? __ldcg(x + 4 * (size_t)i + r) : b[4 * (size_t)i + r];
+#pragma unroll 4
+      for (uint32_t c = 0; c < nb; c++) {
+        const double2 x01 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)cols[c]);
+        const double2 x23 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)cols[c] + 1);
+        const float4 av = *reinterpret_cast<const float4 *>(blks + 16 * c + 4 * r);
+        double sum = 0.0;
+        sum += (double)av.x * x01.x;
+        sum += (double)av.y * x01.y;
+        sum += (double)av.z * x23.x;
+        sum += (double)av.w * x23.y;
+        xi = -1.0 * sum + xi;
+      }
+      for (uint32_t j = jb + nb; j < je; j++) {
+        const uint32_t cc = ja[j];
+        const double2 x01 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)cc);
+        const double2 x23 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)cc + 1);
+        const float *blk = Af + 16 * (size_t)j + 4 * r;
+        double sum = 0.0;
+        sum += (double)blk[0] * x01.x;
+        sum += (double)blk[1] * x01.y;
+        sum += (double)blk[2] * x23.x;
+        sum += (double)blk[3] * x23.y;
+        xi = -1.0 * sum + xi;
+      }
+      if (upper) {
+        const float4 dv = *reinterpret_cast<const float4 *>(rec + 560 + 16 * r);
         const double x0 = __shfl_sync(gmask, xi, base + 0), x1 = __shfl_sync(gmask, xi, base + 1);
         const double x2 = __shfl_sync(gmask, xi, base + 2), x3 = __shfl_sync(gmask, xi, base + 3);
         double y = 0.0;
-        y += (double)dg[0] * x0;
-        y += (double)dg[1] * x1;
-        y += (double)dg[2] * x2;
-        y += (double)dg[3] * x3;
+        y += (double)dv.x * x0;
+        y += (double)dv.y * x1;
+        y += (double)dv.z * x2;
+        y += (double)dv.w * x3;
         xi = y;
       }
-      if (gl < 4) __stcg(x + 4 * (size_t)i + r, xi);
+      __stcg(x + 4 * (size_t)i + r, xi);
     }
-    // rows beyond the first pass
-    if (upper)
-      for (uint32_t s = cur.x + h + R; s < cur.y; s += R) trsv_row_g<T, true, G>(tdesc[s], ja, A, b, x, base, gl, gmask);
-    else
-      for (uint32_t s = cur.x + h + R; s < cur.y; s += R) trsv_row_g<T, false, G>(tdesc[s], ja, A, b, x, base, gl, gmask);
-    load_blocks(k + 1, d1);
-    d = d1;
-    d1 = d2;
+    (void)row_i;
+    // the copies two steps ahead go out after this step's x reads
+    issue(k + 2);
+    if (k + 1 < k2) cur = steps[k + 1];
     asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
-    if (threadIdx.x == 0)
-      asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(&done_s)), "r"(k + 1) : "memory");
+    if (threadIdx.x == 0) st_release_cta_shared(&done_s, k + 1);
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // ------------------------------------------------------------------ J.v
@@ -2041,10 +2294,44 @@ void ilu(DevMesh &m, int precision)
   else
     k_ilu_finish_f32<<<blocks((size_t)m.N * 16, 256), 256, 0, m.stream>>>(m.N, m.diag, m.dinvf, m.Af);
   kf_count_launch();
+  if (precision == 1 && m.tile_pack) {
+    k_tile_pack<<<blocks((size_t)m.tile_ndesc * 32, 256), 256, 0, m.stream>>>(m.tile_ndesc, m.tile_desc, m.ja, m.Af,
+                                                                            m.tile_pack);
+    kf_count_launch();
+  }
 }
 
 void sptrsv(DevMesh &m, const double *b, double *x, int precision)
 {
+  if (m.trsv_mode == 6 && m.ntiles && precision == 1 && m.tile_pack) {
+    cudaMemsetAsync(m.tile_prog, 0, m.ntiles * sizeof(unsigned), m.stream);
+    const double *bb = b;
+    int *err = m.status + 1;
+    void *args[] = {(void *)&m.tile_ptr, (void *)&m.tile_step, (void *)&m.tile_pub, (void *)&m.tile_wait,
+                    (void *)&m.tile_pack, (void *)&m.ja, (void *)&m.Af, (void *)&bb, (void *)&x,
+                    (void *)&m.tile_prog, (void *)&err};
+    const void *fn = (const void *)k_trsv_tiled_packed<8>;
+    const size_t smem = 3 * (size_t)KF_TILE_STEP_ROWS * KF_TILE_REC;
+    static bool attr_set = false;
+    if (!attr_set) {
+      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      attr_set = true;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(m.ntiles);
+    cfg.blockDim = dim3(512);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = m.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
+    if (e != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e));
+    kf_count_launch();
+    return;
+  }
   if (m.trsv_mode == 6 && m.ntiles) {
     cudaMemsetAsync(m.tile_prog, 0, m.ntiles * sizeof(unsigned), m.stream);
     const double *bb = b;
@@ -2062,7 +2349,14 @@ void sptrsv(DevMesh &m, const double *b, double *x, int precision)
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    const void *fn = precision == 0 ? (const void *)k_trsv_tiled<double, 8> : (const void *)k_trsv_tiled<float, 8>;
+    const void *fn = precision == 0 ? (const void *)k_trsv_tiled<double, 8, 1> : (const void *)k_trsv_tiled<float, 8, 2>;
+    static bool carveout = false;   // no shared memory to speak of: all of it as L1 for the prefetched rows
+    if (!carveout) {
+      cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+      const void *other = precision == 0 ? (const void *)k_trsv_tiled<float, 8, 2> : (const void *)k_trsv_tiled<double, 8, 1>;
+      cudaFuncSetAttribute(other, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+      carveout = true;
+    }
     const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
     if (e != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e));
     kf_count_launch();

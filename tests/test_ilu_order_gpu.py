@@ -1,9 +1,10 @@
-"""ILU(0) in a spatial elimination order (sweep, or Morton on request).
+"""ILU(0) in a spatial elimination order (slab sweeps; tiles, one sweep or
+Morton on request).
 
 * through the renumbering code with the identity permutation the factor, the
   triangular solves and a whole exact-mode solve are bit-identical to the
   mesh order: the renumbering adds nothing of its own;
-* with the sweep and the Morton permutations the device computes P^T (LU)^-1 P b where LU is
+* with each of those permutations the device computes P^T (LU)^-1 P b where LU is
   the reference's ILU(0) (matrix/ilu.cpp:49-136, persistent L slots included)
   of the renumbered matrix P A P^T: checked bit for bit against the oracle's
   ILU(0) and triangular solve run on the renumbered pattern and blocks;
@@ -195,12 +196,12 @@ def test_identity_renumbering_is_the_mesh_order(box_mesh, monkeypatch):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("prec", [0, 1])
-@pytest.mark.parametrize("perm", ["tiles", "sweep", "morton"])
+@pytest.mark.parametrize("perm", ["slabs", "tiles", "sweep", "morton"])
 def test_spatial_factor_is_the_renumbered_reference_factor(box_mesh, prec, perm, monkeypatch):
     kf.set_mode("exact")
     kf.set_precision(prec)
     aoa = 3.06
-    if perm != "tiles":
+    if perm != "slabs":
         monkeypatch.setenv("KFUN3D_ILU_PERM", perm)
     m = kf.Mesh(box_mesh(8, seed=32))
     v = m.view
@@ -246,13 +247,16 @@ def test_spatial_factor_is_the_renumbered_reference_factor(box_mesh, prec, perm,
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("perm", ["slabs", "tiles"])
 @pytest.mark.parametrize("n", [13, 30])
-def test_spatial_sweep_every_schedule(box_mesh, n, monkeypatch):
+def test_spatial_sweep_every_schedule(box_mesh, n, perm, monkeypatch):
     """One launch per level (default for the spatial order), the tiled sweep
-    (with 0, 2 and 7 steps of pipeline slack),
+    (with 0, 2 and 7 steps of pipeline slack where the order allows it),
     the persistent sweep, plain level launches and the sync-free sweep give
     bit-identical triangular solves on the spatial factor (exact mode)."""
     kf.set_mode("exact")
+    if perm != "slabs":
+        monkeypatch.setenv("KFUN3D_ILU_PERM", perm)
     path = box_mesh(n, seed=35)
     out = {}
     for sched in ["pdl", "tiled", "tiled:0", "tiled:7", "mono", "levels16", "syncfree"]:
