@@ -6,12 +6,14 @@ Workload (N = 1): the config-4 comparison -- the 120^3 seeded Kuhn-box mesh
 held out of the network's training set, jitter 0.2h, random numbering),
 second-order residual, SER CFL from 50, at most 20 Newton steps, stopped at a
 1e-8 drop of the residual norm.  A step is one solve from the free-stream
-state in the mixed-precision + learned form (FP32 Jacobian blocks, ILU(0) and
-triangular solves; FP64 residual, norms, CFL, Gram-Schmidt and Givens;
-flexible GMRES(30) with the trained network as right preconditioner and its
-fallback).  `comparison` holds, on the same mesh, the plain FP64 solve (the
-reference's method), the same mixed solve without the network, and the wall
-forces' relative error against FP64.  The metric is seconds to the 1e-8 drop
+state in the mixed-precision + learned form (FP32 Jacobian blocks, ILU(0) in
+the spatial elimination order and FP32 triangular solves; FP64 residual,
+norms, CFL, Gram-Schmidt and Givens; flexible GMRES(30) with the trained
+network as right preconditioner and its fallback).  `comparison` holds, on
+the same mesh, the plain FP64 solve (the reference's method: FP64, ILU(0) in
+the mesh's numbering), the same mixed solve without the network, the mixed
+solve in the mesh's numbering, and the wall forces' relative error against
+FP64.  The metric is seconds to the 1e-8 drop
 (lower is better), with flux edges/s and the other kernel throughputs beside
 it.  --config 1 runs the 70^3 plain FP64 solve instead.
 
@@ -55,9 +57,9 @@ CONFIGS = {
             n=70, seed=1, bump=0.1, aoa=3.06, precision=1, mode="fast", first_order=False,
             ts_max=20, stop_ratio=1e8),
     4: dict(workload="config4: 120^3 Kuhn box (bump 0.12, AoA 4.5, held out of training), mixed precision + "
-                     "learned FGMRES against plain FP64, to 1e-8 drop",
+                     "spatial ILU(0) + learned FGMRES against plain FP64, to 1e-8 drop",
             n=120, seed=4, bump=0.12, aoa=4.5, precision=1, mode="fast", first_order=False,
-            ts_max=20, stop_ratio=1e8, learned=True, ref_ts=1, ref_total_its=1556),
+            ts_max=20, stop_ratio=1e8, learned=True, ilu_order=1, ref_ts=1, ref_total_its=1556),
 }
 WEIGHTS = os.path.join(ROOT, "kfun3d_b200", "weights", "mpnn_box40.npy")
 DEFAULT_CONFIG = 4
@@ -295,6 +297,7 @@ def mesh_path(cfg):
 def configure(kf, cfg):
     kf.set_mode(cfg["mode"])
     kf.set_precision(cfg["precision"])
+    kf.set_ilu_order(cfg.get("ilu_order", 0))
     kf.set_first_order(cfg["first_order"])
     kf.set_aoa(cfg["aoa"])
     kf.set_verbose(False)
@@ -361,21 +364,29 @@ def run_gpu_arm(args, cfg):
     v.q[:] = q0
     e2e_value = dist.max(statistics.mean(e2e))
 
-    # the learned form against plain FP64 (the reference's method) and against
-    # the same mixed-precision FGMRES without the network, one solve each
+    # the learned form against plain FP64 (the reference's method: FP64, ILU(0)
+    # in the mesh's numbering), against the same mixed-precision FGMRES without
+    # the network, and against plain GMRES in mixed precision in the mesh's
+    # numbering; one solve each
     comparison = None
     if net is not None:
         f_ours = [hist[-1][k] for k in ("lift", "drag", "momn")]
         t_ilu, h_ilu, st_ilu = m.time_solve_flexible(net=None, reps=1, **params)
+        kf.set_ilu_order(0)
+        t_mesh, h_mesh = m.time_solve(reps=1, **params)
         kf.set_precision(0)
         t_plain, h_plain = m.time_solve(reps=1, **params)
         kf.set_precision(cfg["precision"])
+        kf.set_ilu_order(cfg.get("ilu_order", 0))
         f_plain = [h_plain[-1][k] for k in ("lift", "drag", "momn")]
         comparison = {
             "plain_fp64_s": t_plain, "plain_fp64_gmres_its": sum(h["gmres_its"] for h in h_plain),
             "plain_fp64_newton_steps": len(h_plain),
             "speedup_vs_plain_fp64": t_plain / value,
             "mixed_ilu_fgmres_s": t_ilu, "mixed_ilu_fgmres_gmres_its": st_ilu["gmres_its"],
+            "mixed_mesh_order_gmres_s": t_mesh,
+            "mixed_mesh_order_gmres_its": sum(h["gmres_its"] for h in h_mesh),
+            "ilu_order": "spatial (slab sweeps)" if cfg.get("ilu_order", 0) else "mesh numbering",
             "learned_stats": fstats,
             "forces_rel_err_vs_fp64": max(abs(a - b) / abs(b) for a, b in zip(f_ours, f_plain)),
         }
@@ -396,7 +407,9 @@ def run_gpu_arm(args, cfg):
     traffic = None
     tp = os.path.join(ROOT, "profiles", f"traffic_config{args.config}.json")
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(dominant)
+        # measured DRAM bytes per call, per kernel family and ILU(0) order
+        key = dominant + ("@spatial" if cfg.get("ilu_order", 0) else "")
+        traffic = json.load(open(tp)).get(key)
     achieved = B[dominant] / (t[dominant] * 1e-3) / 1e9
     roofline = {"kernel": dominant, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -408,11 +421,13 @@ def run_gpu_arm(args, cfg):
         if ref.available():
             threads = host_cores()
             with CStdoutToStderr():
-                s = reference_sample(path, cfg, gmres_its, threads)
+                ref_its = cfg.get("ref_total_its", gmres_its)
+                s = reference_sample(path, cfg, ref_its, threads)
             cpu = {"value": s["seconds"], "unit": "s", "cores": threads, "kind": "reference",
                    "sample": (f"reference (oracle/_ref) first {cfg.get('ref_ts', 2)} Newton step(s) of this workload: "
                               f"{s['sample_its']} GMRES iterations in {s['sample_seconds']:.2f} s at "
-                              f"{threads} threads, extrapolated to this solve's {gmres_its} iterations"),
+                              f"{threads} threads, extrapolated to the reference's own {ref_its} iterations "
+                              f"to the 1e-8 drop (FP64, ILU(0) in the mesh's numbering)"),
                    "flux_edges_per_s": s["flux_edges_per_s"]}
     if dist.rank == 0:
         line = {
@@ -475,10 +490,14 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--precision", type=int, default=None, choices=[0, 1],
                     help="override the workload's preconditioner precision (with --kernel)")
+    ap.add_argument("--ilu-order", type=int, default=None, choices=[0, 1],
+                    help="override the workload's ILU(0) elimination order: 0 mesh numbering, 1 spatial (with --kernel)")
     args = ap.parse_args()
     cfg = dict(CONFIGS[args.config])
     if args.precision is not None:
         cfg["precision"] = args.precision
+    if args.ilu_order is not None:
+        cfg["ilu_order"] = args.ilu_order
     if args.kernel:
         run_kernel_probe(args, cfg)
     elif args.impl == "reference":

@@ -492,12 +492,12 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
   up(&m.ilu_rank, rank);
   if (ok && cudaMalloc(&m.pb, 4 * N * sizeof(double)) != cudaSuccess) ok = false;
   if (ok && cudaMalloc(&m.px, 4 * N * sizeof(double)) != cudaSuccess) ok = false;
-  // many thin levels in a spatial order: one launch per level (programmatic
-  // dependent launch) is the fastest schedule measured there (120^3 box,
-  // FP32 factor: 3.2 ms against 5.0 ms for the persistent sweep and 5.3 ms
-  // for the tiled one); KFUN3D_SPTRSV picks another
-  s.trsv_mode = 4;
+  // more levels than in a random numbering: one launch per level
+  // (programmatic dependent launch, four lanes per row) by default;
+  // KFUN3D_SPTRSV picks another schedule
+  s.trsv_mode = 7;
   const char *env = getenv("KFUN3D_SPTRSV");
+  if (env && strcmp(env, "pdl") == 0) s.trsv_mode = 4;
   if (env && strcmp(env, "tiled") == 0) s.trsv_mode = 6;
   if (ok && s.trsv_mode == 6) {
     // the packed FP32 factor of the tiled sweep (without room for it the

@@ -1592,6 +1592,91 @@ __global__ void __launch_bounds__(256) k_trsv_level_pdl(uint32_t s0, uint32_t s1
   if (l16 < 4) x[4 * (size_t)i + r] = xi;
 }
 
+// One launch per level with programmatic dependent launch, four lanes per
+// row: lane r keeps component r and subtracts the row's block products one
+// block at a time (each summed from zero, in block order: the arithmetic of
+// k_trsv_level16), so there is no reduction across lanes and a level needs a
+// quarter of the threads of k_trsv_level_pdl.  Before waiting for the
+// previous level (griddepcontrol.wait) a row loads everything that does not
+// depend on x: its descriptor, the columns and rows of its first 8 blocks,
+// and its diagonal block (upper sweep) or right-hand side (lower sweep).
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(256) k_trsv_level_pdl4(uint32_t s0, uint32_t s1, const uint4 *__restrict__ desc,
+                                                         const uint32_t *__restrict__ ja, const T *__restrict__ A,
+                                                         const double *__restrict__ b, double *x)
+{
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t slot = s0 + (gid >> 2);
+  const int r = threadIdx.x & 3, base = (threadIdx.x & 31) & ~3;
+  const unsigned gmask = 0xfu << base;
+  const bool active = slot < s1;
+  uint4 d = make_uint4(0, 0, 0, 0);
+  uint32_t nb = 0;
+  uint32_t col[8];
+  T a[8][4], dg[4];
+  double xi = 0.0;
+  if (active) {
+    d = desc[slot];
+    nb = d.z - d.y < 8u ? d.z - d.y : 8u;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      col[c] = 0;
+#pragma unroll
+      for (int e = 0; e < 4; e++) a[c][e] = (T)0;
+      if ((uint32_t)c < nb) {
+        col[c] = ja[d.y + c];
+        const T *blk = A + 16 * (size_t)(d.y + c) + 4 * r;
+#pragma unroll
+        for (int e = 0; e < 4; e++) a[c][e] = blk[e];
+      }
+    }
+    if (UPPER) {
+      const T *blk = A + 16 * (size_t)(d.y - 1) + 4 * r;
+#pragma unroll
+      for (int e = 0; e < 4; e++) dg[e] = blk[e];
+    } else {
+      xi = b[4 * (size_t)d.x + r];
+    }
+  }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (!active) return;
+  if (UPPER) xi = x[4 * (size_t)d.x + r];
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    if ((uint32_t)c < nb) {
+      const double4 xc = reinterpret_cast<const double4 *>(x)[col[c]];
+      double sum = 0.0;
+      sum += (double)a[c][0] * xc.x;
+      sum += (double)a[c][1] * xc.y;
+      sum += (double)a[c][2] * xc.z;
+      sum += (double)a[c][3] * xc.w;
+      xi = -1.0 * sum + xi;
+    }
+  }
+  for (uint32_t j = d.y + 8; j < d.z; j++) {
+    const double4 xc = reinterpret_cast<const double4 *>(x)[ja[j]];
+    const T *blk = A + 16 * (size_t)j + 4 * r;
+    double sum = 0.0;
+    sum += (double)blk[0] * xc.x;
+    sum += (double)blk[1] * xc.y;
+    sum += (double)blk[2] * xc.z;
+    sum += (double)blk[3] * xc.w;
+    xi = -1.0 * sum + xi;
+  }
+  if (UPPER) {
+    const double x0 = __shfl_sync(gmask, xi, base + 0), x1 = __shfl_sync(gmask, xi, base + 1);
+    const double x2 = __shfl_sync(gmask, xi, base + 2), x3 = __shfl_sync(gmask, xi, base + 3);
+    double y = 0.0;
+    y += (double)dg[0] * x0;
+    y += (double)dg[1] * x1;
+    y += (double)dg[2] * x2;
+    y += (double)dg[3] * x3;
+    xi = y;
+  }
+  x[4 * (size_t)d.x + r] = xi;
+}
+
 // ------------------------------------------------------------------ sync-free SpTRSV
 
 // Bounded wait for a row's completion flag (device scope, acquire).
@@ -2362,13 +2447,18 @@ void sptrsv(DevMesh &m, const double *b, double *x, int precision)
     kf_count_launch();
     return;
   }
-  if (m.trsv_mode == 4) {
+  if (m.trsv_mode == 4 || m.trsv_mode == 7) {
+    const bool four = m.trsv_mode == 7;   // four lanes per row (k_trsv_level_pdl4), else sixteen
     for (int pass = 0; pass < 2; pass++) {
       const std::vector<uint32_t> &ptr = pass == 0 ? m.lev_l_ptr : m.lev_u_ptr;
       const uint4 *desc = pass == 0 ? m.desc_l : m.desc_u;
       const void *Ap = precision == 0 ? (const void *)m.A : (const void *)m.Af;
       const void *fn;
-      if (precision == 0)
+      if (four && precision == 0)
+        fn = pass == 0 ? (const void *)k_trsv_level_pdl4<double, false> : (const void *)k_trsv_level_pdl4<double, true>;
+      else if (four)
+        fn = pass == 0 ? (const void *)k_trsv_level_pdl4<float, false> : (const void *)k_trsv_level_pdl4<float, true>;
+      else if (precision == 0)
         fn = pass == 0 ? (const void *)k_trsv_level_pdl<double, false> : (const void *)k_trsv_level_pdl<double, true>;
       else
         fn = pass == 0 ? (const void *)k_trsv_level_pdl<float, false> : (const void *)k_trsv_level_pdl<float, true>;
@@ -2378,7 +2468,7 @@ void sptrsv(DevMesh &m, const double *b, double *x, int precision)
         double *xx = x;
         void *args[] = {&s0, &s1, (void *)&desc, (void *)&m.ja, (void *)&Ap, (void *)&bb, (void *)&xx};
         cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(blocks((size_t)(s1 - s0) * 16, 256));
+        cfg.gridDim = dim3(blocks((size_t)(s1 - s0) * (four ? 4 : 16), 256));
         cfg.blockDim = dim3(256);
         cfg.stream = m.stream;
         cudaLaunchAttribute attr[1];

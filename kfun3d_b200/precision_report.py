@@ -7,7 +7,8 @@ Solves the seeded Kuhn-box mesh to a 1e-8 residual drop (at most 20 Newton
 steps, fast mode) with the plain FP64 solver -- the oracle of the other forms
 -- and with the FP32 preconditioner (FP32 Jacobian blocks, ILU(0) factors and
 triangular solves; FP64 residual, norms, CFL update, Gram-Schmidt and Givens),
-plain GMRES and FGMRES, and with the learned FGMRES when --learned.  Prints
+plain GMRES and FGMRES, and with the learned FGMRES when --learned; then the
+FP32 forms again with ILU(0) in the spatial elimination order.  Prints
 one JSON object: per form the Newton steps, GMRES iterations, device seconds,
 the max-norm relative error of the converged state and the relative error of
 each wall-force component against FP64.
@@ -53,12 +54,23 @@ def run(n, seed, bump, aoa, learned_weights=None, ts_max=20, stop_ratio=1e8):
     t, h, st = m.time_solve_flexible(**P)
     m.solve_flexible(**P)
     forms.append(("mixed_ilu_fgmres",) + finish("mixed_ilu_fgmres", t, h, st))
+    net = None
     if learned_weights:
         from . import learned
         net = learned.Network.load(learned_weights)
         t, h, st = m.time_solve_flexible(net=net, **P)
         m.solve_flexible(net=net, **P)
         forms.append(("mixed_learned_fgmres",) + finish("mixed_learned_fgmres", t, h, st))
+    # ILU(0) in the spatial elimination order
+    kf.set_ilu_order(1)
+    t, h = m.time_solve(**P)
+    m.solve(**P)
+    forms.append(("mixed_spatial_gmres",) + finish("mixed_spatial_gmres", t, h))
+    if net is not None:
+        t, h, st = m.time_solve_flexible(net=net, **P)
+        m.solve_flexible(net=net, **P)
+        forms.append(("mixed_spatial_learned_fgmres",) + finish("mixed_spatial_learned_fgmres", t, h, st))
+    kf.set_ilu_order(0)
     for name, q, f in forms:
         out[name]["state_rel_err"] = float(np.max(np.abs(q - q64)) / np.max(np.abs(q64)))
         out[name]["forces_rel_err"] = (np.abs(f - f64) / np.abs(f64)).tolist()
