@@ -153,6 +153,13 @@ int kfun3d_get_ilu_order(void);
 /* Row of every node (rank[node], N entries) in the spatial order built for
    this GEOMETRY; returns N, or -1 when it has not been built. */
 long kfun3d_ilu_rank(const GEOMETRY *g, unsigned int *rank);
+/* Host only (no GPU needed): the spatial order kfun3d_set_ilu_order(1) would
+   build for this GEOMETRY under the current environment, with `tiles` column
+   tiles (the device uses one per SM): rank[node] (N entries, may be NULL)
+   and the numbers of levels of the lower and upper triangular sweeps of the
+   renumbered pattern (may be NULL).  Returns 0, or -1 on bad arguments. */
+int kfun3d_ilu_order_plan(const GEOMETRY *g, unsigned int tiles, unsigned int *rank, unsigned int *nlev_lower,
+                          unsigned int *nlev_upper);
 /* 1: residual reconstructed without gradients (first-order flux). */
 void kfun3d_set_first_order(int on);
 /* 0 silences Kernel()'s per-step report. */

@@ -89,6 +89,8 @@ def lib():
         "kfun3d_set_ilu_order": (None, [C.c_int]),
         "kfun3d_get_ilu_order": (C.c_int, []),
         "kfun3d_ilu_rank": (C.c_long, [G, C.POINTER(C.c_uint)]),
+        "kfun3d_ilu_order_plan": (C.c_int, [G, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_uint),
+                                            C.POINTER(C.c_uint)]),
         "kfun3d_set_first_order": (None, [C.c_int]),
         "kfun3d_set_verbose": (None, [C.c_int]),
         "kfun3d_default_params": (None, [P(SolverParams)]),
@@ -328,6 +330,16 @@ class Mesh:
         if lib().kfun3d_ilu_rank(self.g, rank.ctypes.data_as(C.POINTER(C.c_uint))) < 0:
             raise RuntimeError(f"kfun3d_ilu_rank failed: {last_error()}")
         return rank.astype(np.int64)
+
+    def ilu_order_plan(self, tiles=148):
+        """Host-only preview of the spatial ILU(0) order (no GPU): (rank, levels of the
+        lower sweep, levels of the upper sweep) of the renumbered pattern."""
+        rank = np.zeros(self.view.nnodes, dtype=np.uint32)
+        nl, nu = C.c_uint(0), C.c_uint(0)
+        if lib().kfun3d_ilu_order_plan(self.g, int(tiles), rank.ctypes.data_as(C.POINTER(C.c_uint)),
+                                       C.byref(nl), C.byref(nu)) != 0:
+            raise RuntimeError(f"kfun3d_ilu_order_plan failed: {last_error()}")
+        return rank.astype(np.int64), nl.value, nu.value
 
     def time_kernel(self, which, reps=10):
         names = {"flux": 0, "timestep": 1, "fill": 2, "ilu": 3, "sptrsv": 4, "gmres_iter": 5,

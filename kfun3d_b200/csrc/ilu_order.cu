@@ -571,3 +571,26 @@ extern "C" long kfun3d_ilu_rank(const GEOMETRY *g, unsigned int *rank)
   }
   return (long)m.N;
 }
+
+extern "C" int kfun3d_ilu_order_plan(const GEOMETRY *g, unsigned int tiles, unsigned int *rank,
+                                     unsigned int *nlev_lower, unsigned int *nlev_upper)
+{
+  if (!g || !g->n || !g->e || !g->n->xyz || tiles < 1) {
+    kf_set_error(KFUN3D_ERR_ARG, "kfun3d_ilu_order_plan: bad arguments");
+    return -1;
+  }
+  const size_t N = g->n->sz, E = g->e->sz;
+  const std::vector<uint32_t> tile = partition_tiles(g->n->xyz->x0, g->n->xyz->x1, g->n->xyz->x2, N, tiles);
+  const std::vector<uint32_t> r = spatial_rank(g, N, tile);
+  if (rank) std::copy(r.begin(), r.end(), rank);
+  if (nlev_lower || nlev_upper) {
+    const unsigned int *n0 = g->e->eptr->n0, *n1 = g->e->eptr->n1;
+    std::vector<uint32_t> pn0(E), pn1(E);
+    for (size_t e = 0; e < E; e++) { pn0[e] = r[n0[e]]; pn1[e] = r[n1[e]]; }
+    HostPattern p;
+    kf_build_pattern(p, N, E, pn0.data(), pn1.data());
+    if (nlev_lower) *nlev_lower = (unsigned int)p.lev_l_ptr.size() - 1;
+    if (nlev_upper) *nlev_upper = (unsigned int)p.lev_u_ptr.size() - 1;
+  }
+  return 0;
+}

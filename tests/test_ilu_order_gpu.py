@@ -156,6 +156,59 @@ def test_renumbered_helper_with_identity_is_the_oracle(box_mesh):
     assert np.array_equal(M.sptrsv(b), R.sptrsv(b))
 
 
+def _depth(n0, n1, rank):
+    """Number of level sets of the lower triangle of the pattern renumbered by
+    `rank`: depth(i) = 1 + max depth of its lower neighbours (the definition of
+    matrix/init.cpp:194-232), restated with Python loops."""
+    N = rank.size
+    a, b = rank[n0.astype(np.int64)], rank[n1.astype(np.int64)]
+    lo, hi = np.minimum(a, b), np.maximum(a, b)
+    o = np.argsort(hi, kind="stable")
+    ptr = np.zeros(N + 1, dtype=np.int64)
+    ptr[1:] = np.cumsum(np.bincount(hi[o], minlength=N))
+    low = lo[o].tolist()
+    depth = [1] * N
+    for i in range(N):
+        if ptr[i] < ptr[i + 1]:
+            depth[i] = 1 + max(depth[j] for j in low[ptr[i]:ptr[i + 1]])
+    return max(depth)
+
+
+@pytest.mark.parametrize("perm", ["identity", "slabs", "sweep", "tiles", "morton"])
+def test_plan_on_the_host(box_mesh, perm, monkeypatch):
+    """kfun3d_ilu_order_plan (no GPU): every order is a permutation, the sweep
+    and Morton orders are the ones restated above, and the level counts of
+    both triangular sweeps are those of the renumbered pattern."""
+    if perm != "slabs":
+        monkeypatch.setenv("KFUN3D_ILU_PERM", perm)
+    m = kf.Mesh(box_mesh(11, seed=36))
+    v = m.view
+    rank, nl, nu = m.ilu_order_plan(tiles=16)
+    N = v.nnodes
+    assert np.array_equal(np.sort(rank), np.arange(N))
+    xyz = [c.copy() for c in v.xyz]
+    if perm == "identity":
+        assert np.array_equal(rank, np.arange(N))
+    if perm == "sweep":
+        assert np.array_equal(rank, sweep_rank(xyz))
+    if perm == "morton":
+        assert np.array_equal(rank, morton_rank(xyz))
+    assert nl == _depth(v.n0, v.n1, rank)
+    assert nu == _depth(v.n0, v.n1, N - 1 - rank)
+
+
+def test_plan_slab_sweeps_have_fewer_levels(box_mesh, monkeypatch):
+    m = kf.Mesh(box_mesh(20, seed=37))
+    _, nl_slabs, _ = m.ilu_order_plan()
+    monkeypatch.setenv("KFUN3D_ILU_PERM", "sweep")
+    _, nl_sweep, _ = m.ilu_order_plan()
+    monkeypatch.setenv("KFUN3D_ILU_PERM", "identity")
+    _, nl_mesh, _ = m.ilu_order_plan()
+    # a sweep orders the mesh like a lattice (about 3n levels); four slabs,
+    # each swept from both faces, cut that several times
+    assert nl_slabs < nl_sweep / 2, (nl_slabs, nl_sweep, nl_mesh)
+
+
 @pytest.mark.gpu
 def test_identity_renumbering_is_the_mesh_order(box_mesh, monkeypatch):
     """Set 1 built with the identity permutation: bit-identical factor,
