@@ -125,12 +125,21 @@ void kf_build_pattern(HostPattern &p, size_t N, size_t E, const unsigned int *n0
   for (size_t i = 0; i < N; i++) p.ia[i + 1] += p.ia[i] + 1;
   p.nnz = p.ia[N];
   p.ja.assign(p.nnz, 0);
-  std::vector<uint32_t> fillp(N);
-  for (size_t i = 0; i < N; i++) { p.ja[p.ia[i]] = (uint32_t)i; fillp[i] = p.ia[i] + 1; }
-  for (size_t e = 0; e < E; e++) {
-    p.ja[fillp[n0[e]]++] = n1[e];
-    p.ja[fillp[n1[e]]++] = n0[e];
-  }
+  // rows filled in parallel, each edge taking the next free slot of both of
+  // its rows; a row's order is undone by the sort below
+  std::vector<std::atomic<uint32_t>> fillp(N);
+  parallel_ranges(N, [&](size_t r0, size_t r1) {
+    for (size_t i = r0; i < r1; i++) {
+      p.ja[p.ia[i]] = (uint32_t)i;
+      fillp[i].store(p.ia[i] + 1, std::memory_order_relaxed);
+    }
+  });
+  parallel_ranges(E, [&](size_t e0, size_t e1) {
+    for (size_t e = e0; e < e1; e++) {
+      p.ja[fillp[n0[e]].fetch_add(1, std::memory_order_relaxed)] = n1[e];
+      p.ja[fillp[n1[e]].fetch_add(1, std::memory_order_relaxed)] = n0[e];
+    }
+  });
   p.diag.assign(N, 0);
   p.lpos.assign(N + 1, 0);
   parallel_ranges(N, [&](size_t r0, size_t r1) {
@@ -203,7 +212,7 @@ void kf_build_pattern(HostPattern &p, size_t N, size_t E, const unsigned int *n0
       }
   });
   for (size_t j = 0; j < p.nnz; j++) p.pair_ptr[j + 1] += p.pair_ptr[j];
-  p.pairs.assign(2 * (size_t)p.pair_ptr[p.nnz], 0);
+  p.pairs.resize(2 * (size_t)p.pair_ptr[p.nnz]);   // every element is written below
   parallel_ranges(N, [&](size_t r0, size_t r1) {
     for (size_t i = r0; i < r1; i++)
       for (uint32_t j = p.ia[i]; j < p.ia[i + 1]; j++) {

@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 #include "kfun3d_b200.h"
@@ -20,6 +21,16 @@ int kf_first_order();
 
 // Host-side block pattern of the edge graph (matrix/init.cpp:7-74): row i
 // holds its diagonal and one block per incident edge, columns sorted.
+// std::allocator that leaves new elements uninitialised (for arrays every
+// element of which is written right after they are sized)
+template <class T> struct uninit_alloc : std::allocator<T> {
+  template <class U> struct rebind { using other = uninit_alloc<U>; };
+  uninit_alloc() = default;
+  template <class U> uninit_alloc(const uninit_alloc<U> &) noexcept {}
+  template <class U> void construct(U *p) noexcept { ::new ((void *)p) U; }
+  template <class U, class... A> void construct(U *p, A &&...a) { ::new ((void *)p) U(static_cast<A &&>(a)...); }
+};
+
 struct HostPattern {
   size_t n = 0, nnz = 0;
   std::vector<uint32_t> ia, ja, diag;
@@ -32,7 +43,8 @@ struct HostPattern {
   // pairs [pair_ptr[j], pair_ptr[j+1]) of (L slot index or ~0 for the
   // identity, block index of U(m,k)); the last pair is the product the
   // reference adds back.
-  std::vector<uint32_t> pair_ptr, pairs;
+  std::vector<uint32_t> pair_ptr;
+  std::vector<uint32_t, uninit_alloc<uint32_t>> pairs;
 };
 
 void kf_build_pattern(HostPattern &p, size_t nnodes, size_t nedges, const unsigned int *n0,
