@@ -3,7 +3,7 @@
 * without a network the flexible solve repeats the reference's
   left-preconditioned GMRES step for step;
 * a network that makes things worse is caught by the fallback and the solve
-  still converges to the same state (the FP64 nonlinear residual is the judge);
+  still converges to the same state (the FP64 nonlinear residual decides);
 * the pair writer fills the requested slots with finite data;
 * the ablation: a network trained on the GPU by the library's own kernels,
   against the same FGMRES without it, on a held-out mesh.

@@ -83,7 +83,7 @@ def test_exact_first_order_flux(box_mesh):
 
 
 def test_exact_solve_meshA_matches_reference_history():
-    """The north-star history check: every step's residual norm, CFL, GMRES
+    """The whole-solve history check: every step's residual norm, CFL, GMRES
     count and forces equal the reference's (tolerance 1e-10 relative; exact mode
     achieves equality)."""
     gold = json.load(open(os.path.join(GOLDEN, "meshA_history.json")))["steps"]
