@@ -5,7 +5,8 @@
 
 Training set: seeded Kuhn-box meshes of n^3 nodes, bump height U(0.05, 0.15)
 and angle of attack U(0, 6) degrees, each solved from free stream by the
-ILU(0)-FGMRES solve that writes (residual, correction) pairs on the device.
+ILU(0)-FGMRES solve that writes (residual, correction) pairs on the device
+(ILU(0) in the mesh's numbering, or with --ilu-order 1 in the spatial order).
 Network and optimiser: the library's BF16 tensor-core forward/backward and
 FP32 Adam (lr 1e-3, batch 8 pairs).  Afterwards the network is compared with
 the same FGMRES without it on a held-out mesh (bump 0.12, 4.5 degrees) and a
@@ -36,11 +37,15 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--eval-n", type=int, default=40, help="held-out mesh size (0: no evaluation)")
     ap.add_argument("--precision", type=int, default=1, help="preconditioner precision of the evaluation")
+    ap.add_argument("--ilu-order", type=int, default=0, choices=[0, 1],
+                    help="ILU(0) elimination order of the pair solves and the evaluation: 0 the mesh's "
+                         "numbering (the shipped network), 1 spatial")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "weights", "mpnn_box40.npy"))
     a = ap.parse_args(argv)
 
     kf.set_mode("fast")
     kf.set_precision(0)
+    kf.set_ilu_order(a.ilu_order)
     log = lambda s: print(s, flush=True)   # noqa: E731
     rep = dict(args=vars(a))
     with tempfile.TemporaryDirectory() as work:
