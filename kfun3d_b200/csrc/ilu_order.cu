@@ -520,11 +520,14 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
 
 }  // namespace
 
+void kf_ilu_release(DevMesh &m);
+
 int kf_ilu_select(DevMesh &m, const GEOMETRY *g, int order)
 {
   order = order ? 1 : 0;
   if (order == m.ilu_active) return KFUN3D_OK;
   if (order == 1 && !m.iset[1].valid) {
+    kf_ilu_release(m);   // what an earlier attempt that ran out of memory left
     const int rc = build_spatial(m, g);
     if (rc != KFUN3D_OK) return rc;
   }
