@@ -104,6 +104,10 @@ def test_settings_roundtrip():
     assert kf.get_mode() == 1
     kf.set_mode("exact")
     assert kf.get_mode() == 0
+    kf.set_ilu_order("spatial")
+    assert kf.get_ilu_order() == 1
+    kf.set_ilu_order(0)
+    assert kf.get_ilu_order() == 0
 
 
 def test_matrix_handle_pattern_matches_reference(box_mesh):
