@@ -16,8 +16,9 @@
  * per-step history, and device-resident timing hooks.
  *
  * Failures: the reference's entry points return void and assert.  Here every
- * call records a status (kfun3d_gpu_last_status); by default a CUDA error
- * also aborts the process, as the reference's asserts do.
+ * call records a status (kfun3d_gpu_last_status); by default a CUDA error,
+ * a missing CUDA device, or a GEOMETRY set up with more than one OpenMP
+ * thread also aborts the process, as the reference's asserts do.
  */
 #ifndef KFUN3D_B200_H
 #define KFUN3D_B200_H
@@ -108,8 +109,9 @@ enum kfun3d_status {
 int kfun3d_gpu_last_status(void);
 const char *kfun3d_gpu_last_error(void);
 void kfun3d_clear_status(void);
-/* 1 (default): a CUDA error aborts the process like the reference's asserts.
-   0: the error is only recorded. */
+/* 1 (default): a CUDA error, a missing CUDA device or a GEOMETRY set up with
+   more than one OpenMP thread aborts the process like the reference's
+   asserts.  0: the error is only recorded. */
 void kfun3d_set_abort_on_error(int on);
 
 /* Angle of attack in degrees (inc/phy.h:8-9 hard-codes 3).  Free stream
@@ -242,18 +244,23 @@ void kfun3d_reset_launch_count(void);
 long kfun3d_matrix_read(const GEOMETRY *g, unsigned int *ia, unsigned int *ja, double *blocks);
 
 /* No counterpart in the reference.  Allocation-free triangular solve, for
-   callers that cannot allocate device memory: code that applies the
-   preconditioner from inside a CUDA stream capture (cudaMalloc is not allowed
-   there) or a framework that owns every device allocation.  x = (LU)^-1 b
-   with the factor of the last ComputeNumericalILU on this GEOMETRY; d_b and
-   d_x are the caller's device arrays of 4*nnodes doubles (16-byte aligned,
-   distinct).  Runs the sync-free sweep, whose per-row completion flags live
-   in a fixed device array of the library (8 MiB, held by every GPU that loads
-   the library until exit), so the call allocates nothing; at most 2,097,152
-   rows, larger matrices are rejected (KFUN3D_ERR_ARG).  The first call on a
-   device looks up that array's device address (cudaGetSymbolAddress), so make
-   it before any stream capture.  Calls share the array: calls that overlap on
-   the GPU race.  Returns KFUN3D_OK or an error code (also recorded). */
+   callers that cannot allocate device memory: a framework that owns every
+   device allocation (its own pooled allocator, or all device memory sized at
+   start-up) and forbids libraries from calling cudaMalloc afterwards.
+   x = (LU)^-1 b with the factor of the last ComputeNumericalILU on this
+   GEOMETRY, in the mesh's ILU(0) order and in the precision that is still
+   set (a changed kfun3d_set_precision or the spatial order is refused with
+   KFUN3D_ERR_ARG); d_b and d_x are the caller's device arrays of 4*nnodes
+   doubles (16-byte aligned, distinct).  Runs the sync-free sweep, whose
+   per-row completion flags live in a fixed device array of the library
+   (8 MiB, held by every GPU that loads the library until exit, cleared by
+   each call), so the call allocates nothing; at most 2,097,152 rows, larger
+   matrices are rejected (KFUN3D_ERR_ARG).  The first call on a device looks
+   up that array's device address (cudaGetSymbolAddress).  The call waits for
+   all work already queued on the device (so b may be written on any stream
+   just before), runs on the library's stream and returns once x is written.
+   Calls share the array: calls that overlap on the GPU (from several host
+   threads) race.  Returns KFUN3D_OK or an error code (also recorded). */
 int kfun3d_sptrsv_device_noalloc(const GEOMETRY *g, const double *d_b, double *d_x);
 
 /* Release the device mirror of g (also done by CXX_Matrix_Delete). */

@@ -241,6 +241,7 @@ struct DevMesh {
   double *pscr = nullptr;         // [264] scratch of the pair features
   kfun3d_mpnn_graph *mgraph = nullptr;   // the network's graph of this mesh
   bool factored = false;
+  int factor_precision = 0;       // precision of the last ILU(0) factorisation (0 FP64, 1 FP32)
   bool a_valid = false;
 };
 

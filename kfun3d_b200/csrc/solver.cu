@@ -1163,6 +1163,7 @@ extern "C" void ComputeNumericalILU(GEOMETRY *g)
   if (!m) return;
   ops().ilu(*m, kf_precision());
   m->factored = true;
+  m->factor_precision = kf_precision();
   if (!finish(*m, "ComputeNumericalILU")) return;
   if (device_status(*m) == KFUN3D_ERR_PIVOT)
     kf_set_error(KFUN3D_ERR_PIVOT, "singular or non-finite pivot block in ILU(0)");

@@ -1,14 +1,17 @@
 """The allocation-free triangular solve, checked against the existing entry point.
 
 kfun3d_sptrsv_device_noalloc exists for callers that cannot allocate device
-memory -- code driving the preconditioner from inside a CUDA stream capture,
-where cudaMalloc is not permitted, or a framework that owns every device
-allocation.  It takes the caller's device arrays and keeps its only working
-memory (per-row completion flags) in a fixed file-scope device array.  This
-test runs it twice in a row on the same factor and requires the result to
-equal ComputeSparseTriangularSolve's: exactly in exact mode, within the fast
-mode's 1e-9 solve tolerance in fast mode.  It runs last (file name) so that a
-failure here leaves every other test already run.
+memory: a framework that owns every device allocation (its own pooled
+allocator, or all device memory sized at start-up) and forbids libraries from
+calling cudaMalloc afterwards.  It takes the caller's device arrays and keeps
+its only working memory (per-row completion flags) in a fixed file-scope
+device array.  These tests run it twice in a row on the same factor, in both
+precisions of the factor, and require the result to equal
+ComputeSparseTriangularSolve's: exactly in exact mode, within the fast mode's
+1e-9 solve tolerance in fast mode.  They also check its refusals (no factor,
+misaligned pointers, the spatial ILU order, a precision changed after
+factoring, more rows than the fixed array holds).  The file runs last (file
+name) so that a failure here leaves every other test already run.
 """
 import ctypes as C
 
@@ -22,6 +25,8 @@ from oracle import port
 
 pytestmark = pytest.mark.gpu
 
+KFUN3D_ERR_ARG = 4
+
 
 def noalloc_fn():
     L = kf.lib()
@@ -31,11 +36,13 @@ def noalloc_fn():
     return f
 
 
+@pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("mode,tol", [("exact", 0.0), ("fast", 1e-9)])
-def test_noalloc_matches_existing_entry_point(box_mesh, mode, tol):
+def test_noalloc_matches_existing_entry_point(box_mesh, mode, tol, precision):
     import torch
     kf.set_mode(mode)
-    kf.set_precision(0)
+    kf.set_precision(precision)
+    kf.set_ilu_order(0)
     kf.set_aoa(3.06)
     try:
         for path in (MESH_A, box_mesh(12, seed=7)):
@@ -51,7 +58,6 @@ def test_noalloc_matches_existing_entry_point(box_mesh, mode, tol):
                 x_ref = m.sptrsv(b)
                 db = torch.from_numpy(b).to("cuda")
                 dx = torch.full_like(db, float("nan"))
-                torch.cuda.synchronize()
                 rc = f(m.g, db.data_ptr(), dx.data_ptr())
                 assert rc == 0, kf.last_error()
                 x = dx.cpu().numpy()
@@ -62,25 +68,50 @@ def test_noalloc_matches_existing_entry_point(box_mesh, mode, tol):
             m.close()
     finally:
         kf.set_mode("exact")
+        kf.set_precision(0)
         kf.set_aoa(3.0)
 
 
-def test_noalloc_rejects_bad_arguments():
+def test_noalloc_rejects_bad_arguments(box_mesh):
     import torch
     kf.set_mode("exact")
+    kf.set_precision(0)
     kf.set_abort_on_error(False)
     try:
         m = kf.Mesh(MESH_A)
         f = noalloc_fn()
         # no factor on the device yet
-        assert f(m.g, 0, 0) == 4
+        assert f(m.g, 0, 0) == KFUN3D_ERR_ARG
         assert "ComputeNumericalILU" in kf.last_error()
         m.fill()
         m.ilu()
         db = torch.zeros(m.view.dofs + 2, dtype=torch.float64, device="cuda")
         # misaligned device pointer
-        assert f(m.g, db.data_ptr() + 8, db.data_ptr()) == 4
-        kf.clear_status()
+        assert f(m.g, db.data_ptr() + 8, db.data_ptr()) == KFUN3D_ERR_ARG
+        # factor computed in FP64, FP32 now set
+        kf.set_precision(1)
+        assert f(m.g, db.data_ptr(), db.data_ptr() + 8 * 4 * 2) == KFUN3D_ERR_ARG
+        assert "precision" in kf.last_error()
+        kf.set_precision(0)
         m.close()
+        # the spatial ILU(0) order is refused
+        m = kf.Mesh(box_mesh(10, seed=2))
+        kf.set_ilu_order(1)
+        m.fill()
+        m.ilu()
+        dx = torch.zeros(m.view.dofs, dtype=torch.float64, device="cuda")
+        assert f(m.g, db.data_ptr(), dx.data_ptr()) == KFUN3D_ERR_ARG
+        assert "spatial" in kf.last_error()
+        kf.set_ilu_order(0)
+        m.close()
+        # more rows than the fixed flag array holds (129^3 = 2,146,689 > 2,097,152),
+        # refused from the host pattern alone
+        m = kf.Mesh(box_mesh(129, seed=1))
+        assert f(m.g, db.data_ptr(), dx.data_ptr()) == KFUN3D_ERR_ARG
+        assert "2,097,152" in kf.last_error()
+        m.close()
+        kf.clear_status()
     finally:
+        kf.set_ilu_order(0)
+        kf.set_precision(0)
         kf.set_abort_on_error(True)
