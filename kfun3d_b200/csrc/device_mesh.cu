@@ -38,7 +38,10 @@ void kf_set_error(int code, const char *msg)
     g_status = code;
     g_error = msg ? msg : "";
   }
-  if (code == KFUN3D_ERR_CUDA && g_abort) {
+  // a failed CUDA call, or no device at all, ends the process like the
+  // reference's asserts (unless kfun3d_set_abort_on_error(0)): the reference's
+  // void entry points have no other way to report that nothing was computed
+  if ((code == KFUN3D_ERR_CUDA || code == KFUN3D_ERR_NO_DEVICE) && g_abort) {
     fprintf(stderr, "kfun3d_b200: %s\n", msg);
     abort();
   }
@@ -330,6 +333,10 @@ DevMesh *kf_device(const GEOMETRY *g)
   }
   if (g->s && g->s->sz > 1) {
     kf_set_error(KFUN3D_ERR_ARG, "GEOMETRY built for more than one OpenMP thread: set it up with one thread");
+    if (g_abort) {
+      fprintf(stderr, "kfun3d_b200: GEOMETRY built for more than one OpenMP thread: set it up with one thread\n");
+      abort();
+    }
     return nullptr;
   }
   const HostPattern &p = h->pat;
