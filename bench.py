@@ -13,7 +13,9 @@ network as right preconditioner and its fallback).  `comparison` holds, on
 the same mesh, the plain FP64 solve (the reference's method: FP64, ILU(0) in
 the mesh's numbering), the same mixed solve without the network, the mixed
 solve in the mesh's numbering, and the wall forces' relative error against
-FP64.  The metric is seconds to the 1e-8 drop
+FP64, with the ladder between them (FP64 in the spatial order, FP32 in the
+spatial order without the network) so that the ordering, the precision and
+the network each show their own gain.  The metric is seconds to the 1e-8 drop
 (lower is better), with flux edges/s and the other kernel throughputs beside
 it.  --config 1 runs the 70^3 plain FP64 solve instead.
 
@@ -26,7 +28,12 @@ roofline the kernel family with the largest share of one GMRES iteration,
          algorithmic bytes (per-kernel formulas below) / its CUDA-event time,
          against MEASURED_PEAKS.json's HBM copy bandwidth.
 cpu_baseline / --impl reference: the reference itself (oracle/_ref, built from
-         its own sources) on all host cores, timed on a bounded sample.
+         its own sources) on all host cores, timed on a bounded sample (its
+         first Newton step(s)) and extrapolated by GMRES iterations to the
+         reference's own iteration count, taken from a full run of the
+         reference committed under tests/golden/ (make_golden.py).  The
+         reference arm never loads the CUDA library: its mesh comes from the
+         stand-alone generator program kfun3d_meshgen.
 
 Multi-GPU: replicas (one independent mesh per GPU, no collective on the data
 path); `scaling` is weak.
@@ -52,16 +59,19 @@ CONFIGS = {
             ts_max=20, stop_ratio=1e30),
     1: dict(workload="config1: 70^3 Kuhn box, second-order flux, plain FP64, solve to 1e-8 drop",
             n=70, seed=1, bump=0.1, aoa=3.06, precision=0, mode="fast", first_order=False,
-            ts_max=20, stop_ratio=1e8, ref_total_its=741),
+            ts_max=20, stop_ratio=1e8, ref_count=("box70_forces.json", 1e8)),
     2: dict(workload="config2: 70^3 Kuhn box, FP32 Jacobian/ILU(0)/SpTRSV, FP64 residual and GMRES, to 1e-8 drop",
             n=70, seed=1, bump=0.1, aoa=3.06, precision=1, mode="fast", first_order=False,
             ts_max=20, stop_ratio=1e8),
     4: dict(workload="config4: 120^3 Kuhn box (bump 0.12, AoA 4.5, held out of training), mixed precision + "
                      "spatial ILU(0) + learned FGMRES against plain FP64, to 1e-8 drop",
             n=120, seed=4, bump=0.12, aoa=4.5, precision=1, mode="fast", first_order=False,
-            ts_max=20, stop_ratio=1e8, learned=True, ilu_order=1, ref_ts=1, ref_total_its=1556),
+            ts_max=20, stop_ratio=1e8, learned=True, ilu_order=1, ref_ts=1,
+            ref_count=("box120_reference_count.json", 1e8)),
 }
 WEIGHTS = os.path.join(ROOT, "kfun3d_b200", "weights", "mpnn_box40.npy")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+MESHGEN = os.path.join(ROOT, "kfun3d_b200", "_lib", "kfun3d_meshgen")
 DEFAULT_CONFIG = 4
 
 
@@ -217,6 +227,34 @@ def host_cores():
         return os.cpu_count() or 1
 
 
+def reference_count(cfg):
+    """The reference's own GMRES iteration count (and Newton steps) to the
+    workload's drop, from a full run of oracle/_ref committed as a fixture
+    (tests/golden/make_golden.py records the command and thread count), or
+    None when the workload has none."""
+    spec = cfg.get("ref_count")
+    if not spec:
+        return None
+    path = os.path.join(GOLDEN, spec[0])
+    if not os.path.exists(path):
+        return None
+    d = json.load(open(path))
+    f0, its, steps = None, 0, 0
+    for st in d["steps"]:
+        fn = float(st["fnorm"])
+        f0 = fn if f0 is None else f0
+        its += int(st["gmres_its"])
+        steps += 1
+        if round(f0 / fn) >= spec[1]:
+            break
+    out = {"gmres_its": its, "newton_steps": steps, "threads": d.get("threads", 1),
+           "fixture": f"tests/golden/{spec[0]}"}
+    if "solve_seconds" in d and d.get("newton_steps") == steps:
+        out["full_run_seconds"] = d["solve_seconds"]
+        out["cpu"] = d.get("cpu")
+    return out
+
+
 def reference_sample(path, cfg, total_its, threads):
     """Time the reference (oracle/_ref) on a bounded sample of the solve: its
     first Newton steps (two, one at 120^3) on the same mesh and settings, at `threads` OpenMP
@@ -250,10 +288,17 @@ def run_reference_arm(args, cfg):
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libkfun3d_ref.so was not built"}))
         return
-    import kfun3d_b200 as kf
     path = mesh_path(cfg)
     threads = host_cores()
-    total_its = args.ref_total_its or cfg.get("ref_total_its", 741)
+    rc = reference_count(cfg)
+    if args.ref_total_its:
+        total_its, its_src = args.ref_total_its, "given on the command line"
+    elif rc:
+        total_its = rc["gmres_its"]
+        its_src = (f"the reference's own count at {rc['threads']} thread(s), full run in {rc['fixture']}")
+    else:
+        print(json.dumps({"impl": "reference", "unavailable": "no reference iteration count for this workload"}))
+        return
     # Warm-up: one untimed ComputeFlux pass per requested warm-up step (page-in
     # of the mesh and OpenMP thread start); each timed step is a full sample.
     if args.warmup:
@@ -270,26 +315,33 @@ def run_reference_arm(args, cfg):
     wall = time.perf_counter() - t_all
     value = statistics.mean(v["seconds"] for v in vals)
     sample = (f"first {cfg.get('ref_ts', 2)} Newton step(s) ({vals[-1]['sample_its']} GMRES iterations, "
-              f"{vals[-1]['sample_seconds']:.2f} s) of the workload, extrapolated to {total_its} iterations")
+              f"{vals[-1]['sample_seconds']:.2f} s) of the workload at {threads} threads, extrapolated to "
+              f"{total_its} GMRES iterations ({its_src})")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": cfg["workload"], "threads": threads},
             "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "reference",
-                             "sample": sample, "flux_edges_per_s": vals[-1]["flux_edges_per_s"]},
+                             "sample": sample, "flux_edges_per_s": vals[-1]["flux_edges_per_s"],
+                             "reference_gmres_its": total_its, "sample_gmres_its": vals[-1]["sample_its"],
+                             "reference_full_run": rc},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
 # ---------------------------------------------------------------- the GPU arm
 def mesh_path(cfg):
-    import kfun3d_b200 as kf
+    """The workload's mesh file, written on first use by the stand-alone
+    generator program (kfun3d_meshgen: host code only, so the reference arm
+    never loads the CUDA library)."""
     d = os.environ.get("KFUN3D_MESH_DIR", os.path.join(tempfile.gettempdir(), "kfun3d_meshes"))
     os.makedirs(d, exist_ok=True)
     p = os.path.join(d, f"box{cfg['n']}_s{cfg['seed']}_b{cfg['bump']}.msh")
     if not os.path.exists(p):
         tmp = p + f".{os.getpid()}.tmp"
-        kf.generate_mesh(tmp, cfg["n"], bump_height=cfg["bump"], seed=cfg["seed"])
+        if not os.path.exists(MESHGEN):
+            raise SystemExit(f"{MESHGEN} missing: run `make -C kfun3d_b200/csrc`")
+        subprocess.run([MESHGEN, tmp, str(cfg["n"]), repr(cfg["bump"]), str(cfg["seed"])], check=True)
         os.replace(tmp, p)
     return p
 
@@ -365,13 +417,18 @@ def run_gpu_arm(args, cfg):
     e2e_value = dist.max(statistics.mean(e2e))
 
     # the learned form against plain FP64 (the reference's method: FP64, ILU(0)
-    # in the mesh's numbering), against the same mixed-precision FGMRES without
-    # the network, and against plain GMRES in mixed precision in the mesh's
-    # numbering; one solve each
+    # in the mesh's numbering), one solve each, and the ladder between them so
+    # that each form's own gain shows: FP64 with ILU(0) in the spatial order
+    # (the ordering's gain), FP32 preconditioner in the spatial order without
+    # the network (the precision's gain), then the network (its gain); and
+    # plain GMRES in mixed precision in the mesh's numbering
     comparison = None
     if net is not None:
         f_ours = [hist[-1][k] for k in ("lift", "drag", "momn")]
         t_ilu, h_ilu, st_ilu = m.time_solve_flexible(net=None, reps=1, **params)
+        kf.set_precision(0)
+        t_sp64, h_sp64 = m.time_solve(reps=1, **params)
+        kf.set_precision(cfg["precision"])
         kf.set_ilu_order(0)
         t_mesh, h_mesh = m.time_solve(reps=1, **params)
         kf.set_precision(0)
@@ -379,13 +436,17 @@ def run_gpu_arm(args, cfg):
         kf.set_precision(cfg["precision"])
         kf.set_ilu_order(cfg.get("ilu_order", 0))
         f_plain = [h_plain[-1][k] for k in ("lift", "drag", "momn")]
+        its = lambda h: sum(x["gmres_its"] for x in h)   # noqa: E731
         comparison = {
-            "plain_fp64_s": t_plain, "plain_fp64_gmres_its": sum(h["gmres_its"] for h in h_plain),
+            "plain_fp64_s": t_plain, "plain_fp64_gmres_its": its(h_plain),
             "plain_fp64_newton_steps": len(h_plain),
             "speedup_vs_plain_fp64": t_plain / value,
-            "mixed_ilu_fgmres_s": t_ilu, "mixed_ilu_fgmres_gmres_its": st_ilu["gmres_its"],
-            "mixed_mesh_order_gmres_s": t_mesh,
-            "mixed_mesh_order_gmres_its": sum(h["gmres_its"] for h in h_mesh),
+            "fp64_spatial_gmres_s": t_sp64, "fp64_spatial_gmres_its": its(h_sp64),
+            "mixed_spatial_fgmres_no_network_s": t_ilu, "mixed_spatial_fgmres_no_network_its": st_ilu["gmres_its"],
+            "mixed_mesh_order_gmres_s": t_mesh, "mixed_mesh_order_gmres_its": its(h_mesh),
+            "gain_ordering": t_plain / t_sp64,
+            "gain_precision": t_sp64 / t_ilu,
+            "gain_network": t_ilu / value,
             "ilu_order": "spatial (slab sweeps)" if cfg.get("ilu_order", 0) else "mesh numbering",
             "learned_stats": fstats,
             "forces_rel_err_vs_fp64": max(abs(a - b) / abs(b) for a, b in zip(f_ours, f_plain)),
@@ -402,6 +463,20 @@ def run_gpu_arm(args, cfg):
     t["ilu"] = max(m.time_kernel("ilu", 3) - t["fill"], 1e-6)
     kernels = {k: {"ms": round(t[k], 5), "gbs": round(B[k] / (t[k] * 1e-3) / 1e9, 1),
                    "frac": round(B[k] / (t[k] * 1e-3) / 1e9 / peak, 4)} for k in t}
+    # the plain form's Jacobian fill, ILU(0) and triangular solves (FP64 blocks,
+    # the mesh's numbering); flux and time step are FP64 in every form
+    kernels_fp64 = None
+    if cfg["precision"] or cfg.get("ilu_order", 0):
+        kf.set_precision(0)
+        kf.set_ilu_order(0)
+        B64 = alg_bytes(N, E, Fs, Ns, Nf, nnzb, 0)
+        t64 = {k: m.time_kernel(k, 20) for k in ("fill", "sptrsv")}
+        t64["ilu"] = max(m.time_kernel("ilu", 3) - t64["fill"], 1e-6)
+        kf.set_precision(cfg["precision"])
+        kf.set_ilu_order(cfg.get("ilu_order", 0))
+        kernels_fp64 = {k: {"ms": round(t64[k], 5), "gbs": round(B64[k] / (t64[k] * 1e-3) / 1e9, 1),
+                            "frac": round(B64[k] / (t64[k] * 1e-3) / 1e9 / peak, 4)} for k in t64}
+        kernels_fp64["fill_edges_per_s"] = E / (t64["fill"] * 1e-3)
     share = {k: t[k] for k in ("flux", "sptrsv", "mgs")}
     dominant = max(share, key=share.get)
     traffic = None
@@ -418,16 +493,18 @@ def run_gpu_arm(args, cfg):
     cpu = None
     if dist.rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
         from oracle import ref
-        if ref.available():
+        rc = reference_count(cfg)
+        if ref.available() and rc:
             threads = host_cores()
             with CStdoutToStderr():
-                ref_its = cfg.get("ref_total_its", gmres_its)
-                s = reference_sample(path, cfg, ref_its, threads)
+                s = reference_sample(path, cfg, rc["gmres_its"], threads)
             cpu = {"value": s["seconds"], "unit": "s", "cores": threads, "kind": "reference",
                    "sample": (f"reference (oracle/_ref) first {cfg.get('ref_ts', 2)} Newton step(s) of this workload: "
                               f"{s['sample_its']} GMRES iterations in {s['sample_seconds']:.2f} s at "
-                              f"{threads} threads, extrapolated to the reference's own {ref_its} iterations "
-                              f"to the 1e-8 drop (FP64, ILU(0) in the mesh's numbering)"),
+                              f"{threads} threads, extrapolated to the reference's own {rc['gmres_its']} GMRES "
+                              f"iterations to the 1e-8 drop (full run at {rc['threads']} thread(s), "
+                              f"{rc['fixture']}; FP64, ILU(0) in the mesh's numbering)"),
+                   "reference_gmres_its": rc["gmres_its"], "gpu_gmres_its": gmres_its,
                    "flux_edges_per_s": s["flux_edges_per_s"]}
     if dist.rank == 0:
         line = {
@@ -444,6 +521,7 @@ def run_gpu_arm(args, cfg):
                     "d2h_bytes_per_step": 32 * N + 8 * N},
             "roofline": roofline,
             "kernels": kernels,
+            "kernels_fp64": kernels_fp64,
             "flux_edges_per_s": E / (t["flux"] * 1e-3),
             "fill_edges_per_s": E / (t["fill"] * 1e-3),
             "gmres_iterations_per_s": gmres_its / value,
@@ -483,7 +561,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-total-its", type=int, default=None,
                     help="GMRES iterations of the full solve used to extrapolate the reference sample "
-                         "(default: the plain FP64 solve's count for the workload)")
+                         "(default: the reference's own count from its full run, tests/golden/)")
     ap.add_argument("--kernel", default=None,
                     help="time one kernel family (flux, gradient, edge_flux, timestep, fill, ilu, sptrsv, mgs, "
                          "gmres_iter) instead of the solve")

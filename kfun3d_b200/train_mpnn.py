@@ -47,7 +47,10 @@ def main(argv=None):
     kf.set_precision(0)
     kf.set_ilu_order(a.ilu_order)
     log = lambda s: print(s, flush=True)   # noqa: E731
-    rep = dict(args=vars(a))
+    args = dict(vars(a))
+    # the weights' path as the package sees it (never a scratch folder of the run)
+    args["out"] = os.path.join("kfun3d_b200", "weights", os.path.basename(a.out))
+    rep = dict(args=args)
     with tempfile.TemporaryDirectory() as work:
         t0 = time.time()
         data = learned.training_set(work, n_meshes=a.meshes, n=a.n, seed=a.seed, stride=a.stride, cap=a.cap,

@@ -2,7 +2,9 @@
 
 Run in a container that has the reference sources (the path in REF below):
     make -C oracle ref port && make -C kfun3d_b200/csrc
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py                 # the fast fixtures below
+    python tests/golden/make_golden.py --configs       # box25 / box70 (about 20 min, one core)
+    python tests/golden/make_golden.py --ref-count T   # box120 count (about 30 min on T threads)
 
 Fixtures:
   uns3dA.msh            the reference's own mesh (mesh/uns3dA.msh, MIT licence),
@@ -14,6 +16,19 @@ Fixtures:
                         (oracle/_ref/libkfun3d_ref.so) on mesh A at a seeded state.
   box10_history.json    reference solve on the seeded 10^3 Kuhn-box mesh that
                         kfun3d_mesh_generate writes (AoA 3.06, 1e-8 drop).
+  box25_history.json    reference solve on the 25^3 mesh of the plain FP64
+                        CPU-runnable workload (seed 0, bump 0.1, AoA 3.06, 20
+                        Newton steps, second order: the reference has no
+                        first-order flux), one thread, every value %.17g.
+  box70_forces.json     reference solve on the 70^3 mesh (seed 1, bump 0.1, AoA
+                        3.06) at one thread, run on to a 1e-11 drop so that the
+                        forces at the 1e-8 stop and at the tighter stop are both
+                        in the history.
+  box120_reference_count.json
+                        the reference's own Newton steps, GMRES iterations and
+                        wall time to the 1e-8 drop on the 120^3 held-out mesh
+                        (seed 4, bump 0.12, AoA 4.5) at T OpenMP threads: the
+                        iteration count the CPU baseline extrapolates to.
 """
 import hashlib
 import json
@@ -110,5 +125,87 @@ def main():
     print("golden fixtures written to", GOLD)
 
 
+def _mesh(d, n, seed, bump):
+    p = os.path.join(d, f"box{n}.msh")
+    kf.generate_mesh(p, n, bump_height=bump, seed=seed)
+    with open(p, "rb") as fh:
+        return p, hashlib.sha256(fh.read()).hexdigest()
+
+
+def _steps(h):
+    return [{k: (repr(v) if isinstance(v, float) else v) for k, v in s.items()} for s in h]
+
+
+def config_fixtures():
+    """box25_history.json and box70_forces.json (one thread, the deterministic
+    reference path: src/kernel.c:47-232 through the harness's ref_solve)."""
+    import time
+    with tempfile.TemporaryDirectory() as d:
+        p, sha = _mesh(d, 25, 0, 0.1)
+        m = ref.RefMesh(p, 3.06, 1)
+        params = dict(ts_max=20, stop_ratio=1e30)
+        t0 = time.perf_counter()
+        h = m.solve(**params)
+        dt = time.perf_counter() - t0
+        m.close()
+        with open(os.path.join(GOLD, "box25_history.json"), "w") as fh:
+            json.dump(dict(source="oracle/_ref/libkfun3d_ref.so ref_solve at 1 thread, "
+                                  "kfun3d_mesh_generate(n=25, seed=0, bump_height=0.1)",
+                           mesh_sha256=sha, params=dict(aoa=3.06, **params), seconds=dt,
+                           steps=_steps(h)), fh, indent=1)
+        print("box25:", len(h), "steps", sum(s["gmres_its"] for s in h), "its", f"{dt:.1f} s", flush=True)
+        p, sha = _mesh(d, 70, 1, 0.1)
+        m = ref.RefMesh(p, 3.06, 1)
+        params = dict(ts_max=40, stop_ratio=1e11)
+        t0 = time.perf_counter()
+        h = m.solve(**params)
+        dt = time.perf_counter() - t0
+        m.close()
+        with open(os.path.join(GOLD, "box70_forces.json"), "w") as fh:
+            json.dump(dict(source="oracle/_ref/libkfun3d_ref.so ref_solve at 1 thread, "
+                                  "kfun3d_mesh_generate(n=70, seed=1, bump_height=0.1)",
+                           mesh_sha256=sha, params=dict(aoa=3.06, **params), seconds=dt,
+                           steps=_steps(h)), fh, indent=1)
+        print("box70:", len(h), "steps", sum(s["gmres_its"] for s in h), "its", f"{dt:.1f} s", flush=True)
+
+
+def reference_count(threads):
+    """box120_reference_count.json: the reference's full solve at `threads`
+    OpenMP threads (its ILU(0) is then a racing Chow-Patel sweep,
+    matrix/ilu.cpp:49-97, so the count belongs to this thread count)."""
+    import platform
+    import time
+    with tempfile.TemporaryDirectory() as d:
+        p, sha = _mesh(d, 120, 4, 0.12)
+        t0 = time.perf_counter()
+        m = ref.RefMesh(p, 4.5, threads)
+        t_setup = time.perf_counter() - t0
+        params = dict(ts_max=20, stop_ratio=1e8)
+        t0 = time.perf_counter()
+        h = m.solve(**params)
+        dt = time.perf_counter() - t0
+        m.close()
+    cpu = platform.processor() or platform.machine()
+    try:
+        with open("/proc/cpuinfo") as fh:
+            cpu = next(l.split(":", 1)[1].strip() for l in fh if l.startswith("model name"))
+    except (OSError, StopIteration):
+        pass
+    out = dict(source=f"oracle/_ref/libkfun3d_ref.so ref_solve at {threads} threads, "
+                      "kfun3d_mesh_generate(n=120, seed=4, bump_height=0.12)",
+               command=f"python tests/golden/make_golden.py --ref-count {threads}",
+               mesh_sha256=sha, params=dict(aoa=4.5, **params), threads=threads, cpu=cpu,
+               setup_seconds=t_setup, solve_seconds=dt, newton_steps=len(h),
+               gmres_its=sum(s["gmres_its"] for s in h), steps=_steps(h))
+    with open(os.path.join(GOLD, "box120_reference_count.json"), "w") as fh:
+        json.dump(out, fh, indent=1)
+    print("box120:", out["newton_steps"], "steps", out["gmres_its"], "its", f"{dt:.1f} s", flush=True)
+
+
 if __name__ == "__main__":
-    main()
+    if "--configs" in sys.argv:
+        config_fixtures()
+    elif "--ref-count" in sys.argv:
+        reference_count(int(sys.argv[sys.argv.index("--ref-count") + 1]))
+    else:
+        main()
