@@ -288,11 +288,89 @@ template <class T> static cudaError_t upload(T **dst, const T *src, size_t n)
 
 void kf_ilu_release(DevMesh &m);
 
+// ----------------------------------------------------------------- packed level schedule
+
+void kf_free_packed(PackedSweep pk[2])
+{
+  for (int s = 0; s < 2; s++) {
+    void *ptrs[] = {pk[s].row, pk[s].first, pk[s].col, pk[s].src, pk[s].chunk};
+    for (void *q : ptrs)
+      if (q) cudaFree(q);
+    pk[s] = PackedSweep{};
+  }
+}
+
+// Stream order = slot order of the level-ordered descriptors: slot s of the
+// lower sweep contributes its lower blocks [d.y, d.z) (matrix/sptrsv.cpp:173-189
+// reads them in this column order); slot s of the upper sweep its inverted
+// diagonal block and then its upper blocks [d.y, d.z) (matrix/sptrsv.cpp:191-209).
+// A level's slots are cut into chunks of at most KF_PK_ROWS rows and
+// KF_PK_BLOCKS blocks, one CTA each.
+int kf_build_packed(PackedSweep pk[2], const HostPattern &p, const std::vector<uint4> &desc_l,
+                    const std::vector<uint4> &desc_u)
+{
+  const size_t N = p.n;
+  for (int sw = 0; sw < 2; sw++) {
+    const std::vector<uint4> &d = sw == 0 ? desc_l : desc_u;
+    const std::vector<uint32_t> &lp = sw == 0 ? p.lev_l_ptr : p.lev_u_ptr;
+    std::vector<uint32_t> row(N), first(N + 1), col, src;
+    size_t nblk = 0;
+    for (size_t s = 0; s < N; s++) nblk += (d[s].z - d[s].y) + (sw == 1 ? 1u : 0u);
+    if (nblk >= 0xffffffffu) { kf_free_packed(pk); return KFUN3D_ERR_ARG; }
+    col.resize(nblk);
+    src.resize(nblk);
+    size_t k = 0;
+    for (size_t s = 0; s < N; s++) {
+      const uint4 ds = d[s];
+      row[s] = ds.x;
+      first[s] = (uint32_t)k;
+      if (ds.z - ds.y + (sw == 1 ? 1u : 0u) > KF_PK_BLOCKS) { kf_free_packed(pk); return KFUN3D_ERR_ARG; }
+      if (sw == 1) {
+        col[k] = ds.x;
+        src[k++] = p.diag[ds.x];
+      }
+      for (uint32_t j = ds.y; j < ds.z; j++) {
+        col[k] = p.ja[j];
+        src[k++] = j;
+      }
+    }
+    first[N] = (uint32_t)k;
+    std::vector<uint4> chunk;
+    std::vector<uint32_t> lev(1, 0);
+    uint32_t maxblk = 0;
+    for (size_t l = 0; l + 1 < lp.size(); l++) {
+      uint32_t s = lp[l];
+      while (s < lp[l + 1]) {
+        uint32_t e = s;
+        while (e < lp[l + 1] && e - s < KF_PK_ROWS && first[e + 1] - first[s] <= KF_PK_BLOCKS) e++;
+        chunk.push_back(make_uint4(s, e, first[s], first[e]));
+        maxblk = std::max(maxblk, first[e] - first[s]);
+        s = e;
+      }
+      lev.push_back((uint32_t)chunk.size());
+    }
+    PackedSweep &o = pk[sw];
+    o.nblk = (uint32_t)nblk;
+    o.maxblk = maxblk;
+    o.lev = lev;
+    if (upload(&o.row, row.data(), N) != cudaSuccess || upload(&o.first, first.data(), N + 1) != cudaSuccess ||
+        upload(&o.col, col.data(), nblk) != cudaSuccess || upload(&o.src, src.data(), nblk) != cudaSuccess ||
+        upload(&o.chunk, chunk.data(), chunk.size()) != cudaSuccess) {
+      cudaGetLastError();
+      kf_free_packed(pk);
+      return KFUN3D_ERR_CUDA;
+    }
+  }
+  return KFUN3D_OK;
+}
+
 static void release_device(MatrixHandle *h)
 {
   DevMesh *m = h->dev;
   if (!m) return;
   kf_ilu_release(*m);   // the spatial ILU set's arrays; the reference set's fields are back in place
+  kf_free_packed(m->iset[0].pk);
+  if (m->pk_buf) cudaFree(m->pk_buf);
   void *ptrs[] = {m->col, m->egeo, m->xyz, m->inc_ptr, m->inc_oth, m->inc_edge, m->inc_blk, m->inc_w, m->wf_nodes,
                   m->wf_n, m->s_n, m->f_n, m->bnd_of, m->bnd_node, m->bnd_ptr, m->bnd_ent, m->ia, m->ja,
                   m->diag, m->tblk, m->lpos, m->last_lower, m->lev_l, m->lev_u, m->A, m->lslot, m->dinv,
@@ -648,8 +726,18 @@ DevMesh *kf_device(const GEOMETRY *g)
     by_length(du, p.lev_u_ptr);
     KF_CUDA(upload(&m->desc_l, dl.data(), N));
     KF_CUDA(upload(&m->desc_u, du.data(), N));
-    // triangular-solve schedule (KFUN3D_SPTRSV): "pdl4" (default: one launch
-    // per level with programmatic dependent launch, 4 lanes per row), "pdl"
+    // the packed factor (room for FP64 blocks, shared by both ILU orders) and
+    // this pattern's packed level schedule
+    KF_CUDA(cudaMalloc(&m->pk_buf, 16 * (size_t)m->nnz * sizeof(double)));
+    if (kf_build_packed(m->iset[0].pk, p, dl, du) != KFUN3D_OK) {
+      kf_set_error(KFUN3D_ERR_CUDA, "device mirror: building the packed triangular-solve schedule failed");
+      return nullptr;
+    }
+    // triangular-solve schedule (KFUN3D_SPTRSV): "packed" (default: one
+    // launch per level with programmatic dependent launch, each CTA's rows
+    // one contiguous run of the packed factor staged into shared memory by a
+    // bulk copy), "pdl4" (one launch per level with programmatic dependent
+    // launch, 4 lanes per row, blocks read in the matrix's order), "pdl"
     // (the same with 16 lanes per row), "levels16" (one launch per level, 16
     // lanes per row), "persistent" / "mono" (one cooperative launch, bounded
     // grid barrier between levels), "syncfree" (per-row flags, no level
@@ -658,7 +746,7 @@ DevMesh *kf_device(const GEOMETRY *g)
     // default: one launch per level with programmatic dependent launch and
     // four lanes per row (120^3 box: 1.28 / 1.15 ms FP64 / FP32 against
     // 1.51 / 1.27 ms for the persistent sweep)
-    m->trsv_mode = 7;
+    m->trsv_mode = 8;
     if (env && strcmp(env, "pdl") == 0) m->trsv_mode = 4;
     if (env && strcmp(env, "levels16") == 0) m->trsv_mode = 2;
     if (env && strcmp(env, "persistent") == 0) m->trsv_mode = 3;
@@ -666,6 +754,7 @@ DevMesh *kf_device(const GEOMETRY *g)
     if (env && strcmp(env, "levels") == 0) m->trsv_mode = 0;
     if (env && strcmp(env, "mono") == 0) m->trsv_mode = 5;
     if (env && strcmp(env, "pdl4") == 0) m->trsv_mode = 7;
+    if (env && strcmp(env, "packed") == 0) m->trsv_mode = 8;
     std::vector<uint32_t> lp(p.lev_l_ptr);
     lp.insert(lp.end(), p.lev_u_ptr.begin(), p.lev_u_ptr.end());
     KF_CUDA(upload(&m->lev_ptr_d, lp.data(), lp.size()));
@@ -685,6 +774,8 @@ DevMesh *kf_device(const GEOMETRY *g)
     s0.nlev_l = m->nlev_l; s0.nlev_u = m->nlev_u;
     s0.desc_l = m->desc_l; s0.desc_u = m->desc_u;
     s0.trsv_mode = m->trsv_mode;
+    m->pk[0] = s0.pk[0];
+    m->pk[1] = s0.pk[1];
     s0.fill_blk = m->inc_blk; s0.fill_diag = m->diag; s0.fill_last = m->last_lower; s0.fill_lpos = m->lpos;
     s0.valid = true;
     m->fill_blk = m->inc_blk; m->fill_diag = m->diag; m->fill_last = m->last_lower; m->fill_lpos = m->lpos;

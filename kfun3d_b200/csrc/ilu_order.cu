@@ -59,6 +59,8 @@ void activate(DevMesh &m, const IluSet &s)
   m.ntiles = s.ntiles; m.tile_ptr = s.tile_ptr; m.tile_step = s.tile_step; m.tile_pub = s.tile_pub;
   m.tile_wait = s.tile_wait; m.tile_desc = s.tile_desc; m.tile_prog = s.tile_prog;
   m.tile_pack = s.tile_pack; m.tile_ndesc = s.tile_ndesc;
+  m.pk[0] = s.pk[0];
+  m.pk[1] = s.pk[1];
 }
 
 // Tiles of the tiled triangular sweep: columns along the sweep direction
@@ -443,6 +445,7 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
     by_length(du, p.lev_u_ptr);
     up(&s.desc_l, dl);
     up(&s.desc_u, du);
+    if (ok && kf_build_packed(s.pk, p, dl, du) != KFUN3D_OK) ok = false;
   }
   // the fill's view of the renumbered pattern, per node of the mesh
   {
@@ -492,11 +495,13 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
   up(&m.ilu_rank, rank);
   if (ok && cudaMalloc(&m.pb, 4 * N * sizeof(double)) != cudaSuccess) ok = false;
   if (ok && cudaMalloc(&m.px, 4 * N * sizeof(double)) != cudaSuccess) ok = false;
-  // more levels than in a random numbering: one launch per level
-  // (programmatic dependent launch, four lanes per row) by default;
-  // KFUN3D_SPTRSV picks another schedule
-  s.trsv_mode = 7;
+  // one launch per level (programmatic dependent launch, each CTA's rows one
+  // contiguous run of the packed factor) by default; KFUN3D_SPTRSV picks
+  // another schedule
+  s.trsv_mode = 8;
   const char *env = getenv("KFUN3D_SPTRSV");
+  if (env && strcmp(env, "pdl4") == 0) s.trsv_mode = 7;
+  if (env && strcmp(env, "packed") == 0) s.trsv_mode = 8;
   if (env && strcmp(env, "pdl") == 0) s.trsv_mode = 4;
   if (env && strcmp(env, "tiled") == 0) s.trsv_mode = 6;
   if (ok && s.trsv_mode == 6) {
@@ -555,6 +560,7 @@ void kf_ilu_release(DevMesh &m)
                   m.ilu_rank, m.pb, m.px};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  kf_free_packed(s.pk);
   s = IluSet{};
   m.ilu_rank = nullptr;
   m.pb = m.px = nullptr;

@@ -107,6 +107,25 @@ __device__ __forceinline__ bool kf_grid_barrier(unsigned *bar, int *err)
 constexpr uint32_t KF_TILE_STEP_ROWS = 96;   // rows of a step of the tiled sweep, at most
 constexpr uint32_t KF_TILE_REC = 624;         // bytes of a row record of the packed FP32 factor
 
+// Packed level schedule of the triangular solves (trsv_mode 8), one per
+// sweep (0 lower, 1 upper): the factor's blocks streamed in level-slot order
+// (per slot its lower blocks, or its inverted diagonal block then its upper
+// blocks, in column order), so that the rows one CTA solves in one level are
+// one contiguous run of the stream.  The blocks are copied into the stream
+// after every factorisation (k_trsv_pack, through src).
+constexpr uint32_t KF_PK_ROWS = 64;     // rows of a chunk (one CTA of 256 threads), at most
+constexpr uint32_t KF_PK_BLOCKS = 512;  // blocks of a chunk, at most (its shared-memory stage)
+struct PackedSweep {
+  uint32_t *row = nullptr;     // [N] matrix row of each slot
+  uint32_t *first = nullptr;   // [N+1] first streamed block of each slot
+  uint32_t *col = nullptr;     // [nblk] column of each streamed block
+  uint32_t *src = nullptr;     // [nblk] matrix block copied to each stream position
+  uint4 *chunk = nullptr;      // per CTA: (first slot, end slot, first block, end block)
+  std::vector<uint32_t> lev;   // first chunk of each level, nlev + 1 entries
+  uint32_t nblk = 0;           // blocks in the stream
+  uint32_t maxblk = 0;         // blocks of the largest chunk
+};
+
 struct IluSet {
   bool valid = false;
   uint32_t *ia = nullptr, *ja = nullptr, *diag = nullptr, *tblk = nullptr, *lpos = nullptr;
@@ -130,7 +149,15 @@ struct IluSet {
   unsigned *tile_prog = nullptr;   // [T] progress counters, cleared before each solve
   uint8_t *tile_pack = nullptr;    // [2N x KF_TILE_REC] FP32 factor rows in tile_desc order
   uint32_t tile_ndesc = 0;
+  PackedSweep pk[2];               // packed level schedule (trsv_mode 8)
 };
+
+// Builds the packed level schedule of one pattern from its level-slot
+// descriptors (row, first block, end block) and level offsets; KFUN3D_OK, or
+// an error code with nothing left allocated.
+int kf_build_packed(PackedSweep pk[2], const HostPattern &p, const std::vector<uint4> &desc_l,
+                    const std::vector<uint4> &desc_u);
+void kf_free_packed(PackedSweep pk[2]);
 
 // Device mirror of one GEOMETRY.  Node-indexed arrays follow the reference's
 // numbering; edge-indexed arrays its (sorted) edge order.
@@ -210,6 +237,8 @@ struct DevMesh {
   double graph_aoa = 0.0;
   bool use_graphs = true;
   unsigned mgs_grid = 0;          // cooperative grid for the Gram-Schmidt kernel
+  bool mgs_resident = true;       // Gram-Schmidt with w kept on chip (k_mgs_resident)
+  int mgs_ts = 0;                 // its double2 elements per thread in shared memory
   double *part = nullptr;         // [2][mgs_grid] block partial sums
   unsigned *bar = nullptr;        // grid-barrier words: [0..1] persistent sweep, [2..3] Gram-Schmidt,
                                   // [4] counter of the one-CTA-per-SM sweep
@@ -228,6 +257,8 @@ struct DevMesh {
   unsigned *tile_prog = nullptr;
   uint8_t *tile_pack = nullptr;
   uint32_t tile_ndesc = 0;
+  PackedSweep pk[2];              // active set's packed level schedule
+  void *pk_buf = nullptr;         // the packed factor: lower stream, then upper stream (FP64 or FP32 blocks)
   int ilu_active = 0;             // 1: the spatial set is active
   uint32_t *ilu_rank = nullptr;   // [N] row of each node in the spatial set
   double *pb = nullptr, *px = nullptr;   // [4N] right-hand side and solution, spatial numbering

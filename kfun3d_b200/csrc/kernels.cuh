@@ -370,6 +370,179 @@ __global__ void __launch_bounds__(256) k_gradient(uint32_t N, const uint32_t *__
   gz[n] = az;
 }
 
+// ------------------------------------------------------------------ least-squares weights on the device
+
+// The seven least-squares coefficients of node n (src/weights.c:237-297,
+// 173-232, 102-170 and 335-366): three passes over the node's incident edges
+// in edge order, each followed by the node's own normalisation, exactly the
+// reference's operations (its edge loops add into both end points; here each
+// node gathers its own terms in the same order).  Output per node: w00, w01,
+// w02, w11, w12, w22, w33 and a zero, as two double4.
+__global__ void __launch_bounds__(128) k_lsq_coef(uint32_t N, const uint32_t *__restrict__ ord,
+                                                  const uint32_t *__restrict__ inc_ptr,
+                                                  const uint32_t *__restrict__ inc_oth,
+                                                  const uint32_t *__restrict__ inc_edge,
+                                                  const double4 *__restrict__ xyz, double4 *__restrict__ coef)
+{
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t n = ord[p];
+  const double4 xn = xyz[n];
+  const uint32_t k0 = inc_ptr[p], k1 = inc_ptr[p + 1];
+  double w0 = 0.0, w1 = 0.0, w2 = 0.0;
+  for (uint32_t k = k0; k < k1; k++) {
+    const double4 xo = xyz[inc_oth[k]];
+    const double rx = xo.x - xn.x, ry = xo.y - xn.y, rz = xo.z - xn.z;
+    w0 += rx * rx;
+    w1 += rx * ry;
+    w2 += rx * rz;
+  }
+  w0 = sqrt(w0);
+  w1 /= w0;
+  w2 /= w0;
+  double w3 = 0.0, w4 = 0.0;
+  for (uint32_t k = k0; k < k1; k++) {
+    const double4 xo = xyz[inc_oth[k]];
+    const double d = w1 / w0;
+    if (!(inc_edge[k] >> 31)) {   // n is n0: edge vector from n to the other end
+      const double dx = xo.x - xn.x, dy = xo.y - xn.y, dz = xo.z - xn.z;
+      const double d_ = dy - dx * d;
+      w3 += d_ * d_;
+      w4 += d_ * dz;
+    } else {
+      const double dx = xn.x - xo.x, dy = xn.y - xo.y, dz = xn.z - xo.z;
+      const double d_ = -dy + dx * d;
+      w3 += d_ * d_;
+      w4 -= d_ * dz;
+    }
+  }
+  w3 = sqrt(w3);
+  w4 /= w3;
+  double w5 = 0.0;
+  for (uint32_t k = k0; k < k1; k++) {
+    const double4 xo = xyz[inc_oth[k]];
+    const double d0 = w1 / w0, d1 = w2 / w0, d2 = w4 / w3;
+    double d0_, d1_;
+    if (!(inc_edge[k] >> 31)) {
+      const double dx = xo.x - xn.x, dy = xo.y - xn.y, dz = xo.z - xn.z;
+      d0_ = dy - dx * d0;
+      d1_ = dz - dx * d1;
+    } else {
+      const double dx = xn.x - xo.x, dy = xn.y - xo.y, dz = xn.z - xo.z;
+      d0_ = -dy + dx * d0;
+      d1_ = -dz + dx * d1;
+    }
+    const double d2_ = d1_ - d2 * d0_;
+    w5 += d2_ * d2_;
+  }
+  w5 = sqrt(w5);
+  const double sw00 = w0 * w0, sw11 = w3 * w3, sw22 = w5 * w5;
+  const double w00 = 1.0 / sw00, w11 = 1.0 / sw11, w22 = 1.0 / sw22;
+  const double w01 = w1 / w0, w02 = w2 / w0, w12 = w4 / w3;
+  double m0 = w1 * w4;
+  m0 -= w2 * w3;
+  const double m1 = w0 * w3 * sw22;
+  const double w33 = m0 / m1;
+  coef[2 * (size_t)n] = make_double4(w00, w01, w02, w11);
+  coef[2 * (size_t)n + 1] = make_double4(w12, w22, w33, 0.0);
+}
+
+// The least-squares term of one incidence seen from node n (src/weights.c:
+// 9-100): (dx, dy, dz) is the edge vector from n0 to n1, c = n's coefficients
+// (w00, w01, w02, w11 | w12, w22, w33), n0side = n is the edge's n0.
+__device__ __forceinline__ void lsq_term(bool n0side, double dx, double dy, double dz, const double4 ca,
+                                         const double4 cb, double &tx, double &ty, double &tz)
+{
+  double c0, c1;
+  if (n0side) {
+    c0 = -dx * ca.y + dy;
+    c1 = -dx * ca.z + dz;
+  } else {
+    c0 = dx * ca.y - dy;
+    c1 = dx * ca.z - dz;
+  }
+  c1 = -cb.x * c0 + c1;
+  tx = ca.w * ca.y * c0;
+  tx = (n0side ? dx : -dx) * ca.x - tx;
+  tx += cb.z * c1;
+  ty = cb.x * cb.y * c1;
+  ty = ca.w * c0 - ty;
+  tz = cb.y * c1;
+}
+
+// Counts the incidences whose term, recomputed from the coefficients, differs
+// in any bit from the stored one (inc_w): zero means the gradient may compute
+// its terms on the fly.
+__global__ void __launch_bounds__(128) k_lsq_check(uint32_t N, const uint32_t *__restrict__ ord,
+                                                   const uint32_t *__restrict__ inc_ptr,
+                                                   const uint32_t *__restrict__ inc_oth,
+                                                   const uint32_t *__restrict__ inc_edge,
+                                                   const double *__restrict__ inc_w, uint32_t wstride,
+                                                   const double4 *__restrict__ xyz,
+                                                   const double4 *__restrict__ coef, unsigned *bad)
+{
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t n = ord[p];
+  const double4 xn = xyz[n], ca = coef[2 * (size_t)n], cb = coef[2 * (size_t)n + 1];
+  unsigned nbad = 0;
+  for (uint32_t k = inc_ptr[p]; k < inc_ptr[p + 1]; k++) {
+    const double4 xo = xyz[inc_oth[k]];
+    const bool n0side = !(inc_edge[k] >> 31);
+    const double dx = n0side ? xo.x - xn.x : xn.x - xo.x;
+    const double dy = n0side ? xo.y - xn.y : xn.y - xo.y;
+    const double dz = n0side ? xo.z - xn.z : xn.z - xo.z;
+    double tx, ty, tz;
+    lsq_term(n0side, dx, dy, dz, ca, cb, tx, ty, tz);
+    if (__double_as_longlong(tx) != __double_as_longlong(inc_w[k]) ||
+        __double_as_longlong(ty) != __double_as_longlong(inc_w[wstride + k]) ||
+        __double_as_longlong(tz) != __double_as_longlong(inc_w[2 * (size_t)wstride + k]))
+      nbad++;
+  }
+  if (nbad) atomicAdd(bad, nbad);
+}
+
+// k_gradient with the least-squares terms computed from the node's seven
+// coefficients and the edge vector instead of read per incidence (4 bytes
+// per incidence from memory instead of 28; the end points' coordinates are
+// gathered like their states).  ROLE_BY_INDEX: every edge has n0 < n1, so n
+// is an edge's n0 exactly when the other end has the larger index.
+template <bool ROLE_BY_INDEX>
+__global__ void __launch_bounds__(256) k_gradient_otf(uint32_t N, const uint32_t *__restrict__ ord,
+                                                      const uint32_t *__restrict__ inc_ptr,
+                                                      const uint32_t *__restrict__ inc_oth,
+                                                      const uint32_t *__restrict__ inc_edge,
+                                                      const double4 *__restrict__ xyz,
+                                                      const double4 *__restrict__ coef,
+                                                      const double4 *__restrict__ q, double4 *__restrict__ gx,
+                                                      double4 *__restrict__ gy, double4 *__restrict__ gz)
+{
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t n = ord[p];
+  const double4 qn = q[n], xn = xyz[n], ca = coef[2 * (size_t)n], cb = coef[2 * (size_t)n + 1];
+  double4 ax = make_double4(0, 0, 0, 0), ay = ax, az = ax;
+  const uint32_t k1 = inc_ptr[p + 1];
+  for (uint32_t k = inc_ptr[p]; k < k1; k++) {
+    const uint32_t o = inc_oth[k];
+    const bool n0side = ROLE_BY_INDEX ? o > n : !(inc_edge[k] >> 31);
+    const double4 qo = q[o], xo = xyz[o];
+    const double dx = n0side ? xo.x - xn.x : xn.x - xo.x;
+    const double dy = n0side ? xo.y - xn.y : xn.y - xo.y;
+    const double dz = n0side ? xo.z - xn.z : xn.z - xo.z;
+    double wx, wy, wz;
+    lsq_term(n0side, dx, dy, dz, ca, cb, wx, wy, wz);
+    double dq;
+    dq = qo.x - qn.x; ax.x += wx * dq; ay.x += wy * dq; az.x += wz * dq;
+    dq = qo.y - qn.y; ax.y += wx * dq; ay.y += wy * dq; az.y += wz * dq;
+    dq = qo.z - qn.z; ax.z += wx * dq; ay.z += wy * dq; az.z += wz * dq;
+    dq = qo.w - qn.w; ax.w += wx * dq; ay.w += wy * dq; az.w += wz * dq;
+  }
+  gx[n] = ax;
+  gy[n] = ay;
+  gz[n] = az;
+}
+
 // ------------------------------------------------------------------ residual
 
 // src/flux.c:151-465 as a gather: node n recomputes the flux of each incident
@@ -1677,6 +1850,126 @@ __global__ void __launch_bounds__(256) k_trsv_level_pdl4(uint32_t s0, uint32_t s
   x[4 * (size_t)d.x + r] = xi;
 }
 
+// ------------------------------------------------------------------ packed level schedule
+
+// Copies the factor's blocks into the packed stream of one sweep: stream
+// position k takes matrix block src[k] (16-byte words, one per thread).
+template <typename T>
+__global__ void __launch_bounds__(256) k_trsv_pack(uint32_t nblk, const uint32_t *__restrict__ src,
+                                                   const T *__restrict__ A, T *__restrict__ P)
+{
+  constexpr uint32_t V = 16 * sizeof(T) / 16;   // 16-byte words per block
+  const size_t gid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (gid >= (size_t)nblk * V) return;
+  const uint32_t k = (uint32_t)(gid / V), w = (uint32_t)(gid % V);
+  const uint4 v = __ldcs(reinterpret_cast<const uint4 *>(A + 16 * (size_t)__ldg(src + k)) + w);
+  reinterpret_cast<uint4 *>(P + 16 * (size_t)k)[w] = v;
+}
+
+// Row r (0..3) of a 4x4 block in shared memory, widened to double.
+__device__ __forceinline__ void block_row(const float *a, double &a0, double &a1, double &a2, double &a3)
+{
+  const float4 v = *reinterpret_cast<const float4 *>(a);
+  a0 = v.x; a1 = v.y; a2 = v.z; a3 = v.w;
+}
+__device__ __forceinline__ void block_row(const double *a, double &a0, double &a1, double &a2, double &a3)
+{
+  const double2 u = reinterpret_cast<const double2 *>(a)[0], v = reinterpret_cast<const double2 *>(a)[1];
+  a0 = u.x; a1 = u.y; a2 = v.x; a3 = v.y;
+}
+
+// One level of the packed schedule (matrix/sptrsv.cpp:173-209), one CTA per
+// chunk (up to 64 rows of the level, four lanes per row, lane r = component
+// r).  Before the previous level has finished (griddepcontrol.wait) the CTA
+// stages its chunk of the packed factor -- one contiguous run -- into shared
+// memory with a single bulk copy, and loads the chunk's columns, rows and
+// (lower sweep) right-hand side; after it, it gathers the final x of the
+// columns (four at a time) and subtracts the block products in column order,
+// each product summed from zero in component order as the reference does.
+// The upper sweep then applies the inverted diagonal block (the first block
+// of the row's run).  The chunk's blocks in shared memory: 16 T each, then
+// their columns.
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(256, 4) k_trsv_packed(uint32_t c0, const uint4 *__restrict__ chunk,
+                                                        const uint32_t *__restrict__ prow,
+                                                        const uint32_t *__restrict__ pfirst,
+                                                        const uint32_t *__restrict__ pcol, const T *__restrict__ pk,
+                                                        const double *__restrict__ b, double *x, int *err)
+{
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t mbar;
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  const uint4 ch = chunk[c0 + blockIdx.x];
+  const uint32_t nblk = ch.w - ch.z;
+  T *sa = reinterpret_cast<T *>(smem);
+  uint32_t *sc = reinterpret_cast<uint32_t *>(smem + (size_t)nblk * 16 * sizeof(T));
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar, 1);
+    mbar_expect_tx(&mbar, nblk * 16u * (unsigned)sizeof(T));
+    if (nblk) bulk_g2s(sa, pk + 16 * (size_t)ch.z, nblk * 16u * (unsigned)sizeof(T), &mbar);
+  }
+  for (uint32_t k = threadIdx.x; k < nblk; k += blockDim.x) sc[k] = __ldg(pcol + ch.z + k);
+  const uint32_t s = ch.x + (threadIdx.x >> 2);
+  const int r = threadIdx.x & 3, base = (threadIdx.x & 31) & ~3;
+  const bool active = s < ch.y;
+  uint32_t row = 0, k0 = 0, k1 = 0;
+  double xi = 0.0;
+  if (active) {
+    row = __ldg(prow + s);
+    k0 = __ldg(pfirst + s) - ch.z;
+    k1 = __ldg(pfirst + s + 1) - ch.z;
+    if (!UPPER) xi = b[4 * (size_t)row + r];
+  }
+  __syncthreads();   // the columns and the barrier's initialisation, for every thread
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (!mbar_wait(&mbar, 0, err)) return;
+  if (!active) return;
+  uint32_t k = k0;
+  if (UPPER) {
+    xi = __ldcg(x + 4 * (size_t)row + r);
+    k = k0 + 1;
+  }
+  const double2 *x2 = reinterpret_cast<const double2 *>(x);
+  for (; k < k1; k += 4) {
+    double2 lo[4], hi[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      if (k + c < k1) {
+        const size_t col = sc[k + c];
+        lo[c] = __ldcg(x2 + 2 * col);
+        hi[c] = __ldcg(x2 + 2 * col + 1);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      if (k + c < k1) {
+        double a0, a1, a2, a3;
+        block_row(sa + 16 * (size_t)(k + c) + 4 * r, a0, a1, a2, a3);
+        double sum = 0.0;
+        sum += a0 * lo[c].x;
+        sum += a1 * lo[c].y;
+        sum += a2 * hi[c].x;
+        sum += a3 * hi[c].y;
+        xi = -1.0 * sum + xi;
+      }
+    }
+  }
+  if (UPPER) {
+    const unsigned gmask = 0xfu << base;
+    const double x0 = __shfl_sync(gmask, xi, base + 0), x1 = __shfl_sync(gmask, xi, base + 1);
+    const double x2v = __shfl_sync(gmask, xi, base + 2), x3 = __shfl_sync(gmask, xi, base + 3);
+    double a0, a1, a2, a3;
+    block_row(sa + 16 * (size_t)k0 + 4 * r, a0, a1, a2, a3);
+    double y = 0.0;
+    y += a0 * x0;
+    y += a1 * x1;
+    y += a2 * x2v;
+    y += a3 * x3;
+    xi = y;
+  }
+  x[4 * (size_t)row + r] = xi;
+}
+
 // ------------------------------------------------------------------ sync-free SpTRSV
 
 // Bounded wait for a row's completion flag (device scope, acquire).
@@ -2353,6 +2646,8 @@ void fill(DevMesh &m, const double *q, double u, double v, int precision)
   }
 }
 
+static void packed_setup();
+
 void ilu(DevMesh &m, int precision)
 {
   int *status = m.status;
@@ -2384,10 +2679,86 @@ void ilu(DevMesh &m, int precision)
                                                                             m.tile_pack);
     kf_count_launch();
   }
+  if (m.trsv_mode == 8 && m.pk[0].chunk) {
+    packed_setup();
+    for (int pass = 0; pass < 2; pass++) {
+      const uint32_t nb = m.pk[pass].nblk, off = pass == 0 ? 0u : m.pk[0].nblk;
+      if (precision == 0)
+        k_trsv_pack<double><<<blocks((size_t)nb * 8, 256), 256, 0, m.stream>>>(
+            nb, m.pk[pass].src, m.A, reinterpret_cast<double *>(m.pk_buf) + 16 * (size_t)off);
+      else
+        k_trsv_pack<float><<<blocks((size_t)nb * 4, 256), 256, 0, m.stream>>>(
+            nb, m.pk[pass].src, m.Af, reinterpret_cast<float *>(m.pk_buf) + 16 * (size_t)off);
+      kf_count_launch();
+    }
+  }
+}
+
+// Dynamic shared memory of k_trsv_packed for a chunk of `blocks` blocks.
+template <typename T> static size_t packed_smem(uint32_t blocks)
+{
+  return (size_t)blocks * (16 * sizeof(T) + 4);
+}
+
+// The kernels' shared-memory limit, raised once to the largest chunk the
+// schedule allows (before any stream capture: ilu() calls it).
+static void packed_setup()
+{
+  static bool done = false;
+  if (done) return;
+  const int f32 = (int)packed_smem<float>(KF_PK_BLOCKS), f64 = (int)packed_smem<double>(KF_PK_BLOCKS);
+  cudaFuncSetAttribute((const void *)k_trsv_packed<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f32);
+  cudaFuncSetAttribute((const void *)k_trsv_packed<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f32);
+  cudaFuncSetAttribute((const void *)k_trsv_packed<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f64);
+  cudaFuncSetAttribute((const void *)k_trsv_packed<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f64);
+  done = true;
+}
+
+// Both sweeps of the packed schedule: one launch per level, chained by
+// programmatic dependent launch (the first level of the lower sweep waits for
+// the right-hand side normally).
+template <typename T> static void sptrsv_packed(DevMesh &m, const double *b, double *x)
+{
+  packed_setup();
+  int *err = m.status + 1;
+  const T *base = reinterpret_cast<const T *>(m.pk_buf);
+  for (int pass = 0; pass < 2; pass++) {
+    const PackedSweep &pk = m.pk[pass];
+    const T *P = pass == 0 ? base : base + 16 * (size_t)m.pk[0].nblk;
+    const void *fn = pass == 0 ? (const void *)k_trsv_packed<T, false> : (const void *)k_trsv_packed<T, true>;
+    const size_t smem = packed_smem<T>(pk.maxblk);
+    for (size_t l = 0; l + 1 < pk.lev.size(); l++) {
+      uint32_t c0 = pk.lev[l];
+      const uint32_t nc = pk.lev[l + 1] - c0;
+      if (nc == 0) continue;
+      const double *bb = b;
+      double *xx = x;
+      void *args[] = {&c0, (void *)&pk.chunk, (void *)&pk.row, (void *)&pk.first, (void *)&pk.col, (void *)&P,
+                      (void *)&bb, (void *)&xx, (void *)&err};
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(nc);
+      cfg.blockDim = dim3(256);
+      cfg.dynamicSmemBytes = smem;
+      cfg.stream = m.stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[0].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = (pass == 0 && l == 0) ? 0 : 1;
+      const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
+      if (e != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e));
+      kf_count_launch();
+    }
+  }
 }
 
 void sptrsv(DevMesh &m, const double *b, double *x, int precision)
 {
+  if (m.trsv_mode == 8 && m.pk[0].chunk) {
+    if (precision == 0) sptrsv_packed<double>(m, b, x);
+    else sptrsv_packed<float>(m, b, x);
+    return;
+  }
   if (m.trsv_mode == 6 && m.ntiles && precision == 1 && m.tile_pack) {
     cudaMemsetAsync(m.tile_prog, 0, m.ntiles * sizeof(unsigned), m.stream);
     const double *bb = b;

@@ -200,8 +200,8 @@ def test_blas_entry_points():
     assert np.array_equal(z, x * (1.0 / nrm))
 
 
-@pytest.mark.parametrize("schedule", ["levels", "syncfree", "levels16", "persistent", "pdl", "pdl4", "mono", "mono:8", "mono:4",
-                                      "mono:16:1", "mono:8:3"])
+@pytest.mark.parametrize("schedule", ["packed", "levels", "syncfree", "levels16", "persistent", "pdl", "pdl4", "mono",
+                                      "mono:8", "mono:4", "mono:16:1", "mono:8:3"])
 def test_exact_sptrsv_every_schedule(box_mesh, schedule, monkeypatch):
     """Every triangular-solve schedule (chosen when the device mirror is built;
     for the persistent sweep also lanes per row and CTAs per SM) gives the

@@ -303,8 +303,8 @@ def test_spatial_factor_is_the_renumbered_reference_factor(box_mesh, prec, perm,
 @pytest.mark.parametrize("perm", ["slabs", "tiles"])
 @pytest.mark.parametrize("n", [13, 30])
 def test_spatial_sweep_every_schedule(box_mesh, n, perm, monkeypatch):
-    """One launch per level with four lanes per row (default for the spatial
-    order) and with sixteen, the tiled sweep
+    """The packed level launches (default for the spatial order), one launch
+    per level with four lanes per row and with sixteen, the tiled sweep
     (with 0, 2 and 7 steps of pipeline slack where the order allows it),
     the persistent sweep, plain level launches and the sync-free sweep give
     bit-identical triangular solves on the spatial factor (exact mode)."""
@@ -313,9 +313,9 @@ def test_spatial_sweep_every_schedule(box_mesh, n, perm, monkeypatch):
         monkeypatch.setenv("KFUN3D_ILU_PERM", perm)
     path = box_mesh(n, seed=35)
     out = {}
-    for sched in ["pdl4", "pdl", "tiled", "tiled:0", "tiled:7", "mono", "levels16", "syncfree"]:
+    for sched in ["packed", "pdl4", "pdl", "tiled", "tiled:0", "tiled:7", "mono", "levels16", "syncfree"]:
         monkeypatch.delenv("KFUN3D_TILE_SLACK", raising=False)
-        if sched == "pdl4":
+        if sched == "packed":
             monkeypatch.delenv("KFUN3D_SPTRSV", raising=False)
         else:
             monkeypatch.setenv("KFUN3D_SPTRSV", sched.split(":")[0])
@@ -335,7 +335,7 @@ def test_spatial_sweep_every_schedule(box_mesh, n, perm, monkeypatch):
             assert kf.last_status() == 0, (sched, prec)
         m.close()
     for (sched, prec), x in out.items():
-        assert np.array_equal(x, out["pdl4", prec]), (sched, prec)
+        assert np.array_equal(x, out["packed", prec]), (sched, prec)
 
 
 @pytest.mark.gpu
