@@ -92,3 +92,25 @@ def test_generator_is_reproducible_and_oracle_matches_box10(box_mesh):
         assert digest(r) == kd["r"]
     finally:
         kf.set_aoa(3.0)
+
+
+def test_generator_writes_the_config_fixture_meshes_and_oracle_matches_box25(box_mesh):
+    """The 25^3 (seed 0) and 70^3 (seed 1) meshes of the config fixtures are
+    what the generator writes today; the oracle repeats the reference's 25^3
+    history (first 8 Newton steps, bit for bit)."""
+    for name, n, seed in (("box25_history.json", 25, 0), ("box70_forces.json", 70, 1)):
+        path = os.path.join(GOLDEN, name)
+        if not os.path.exists(path):
+            continue
+        gold = json.load(open(path))
+        with open(box_mesh(n, seed=seed, bump=0.1), "rb") as fh:
+            assert hashlib.sha256(fh.read()).hexdigest() == gold["mesh_sha256"], name
+    gold = load("box25_history.json")
+    kf.set_aoa(3.06)
+    try:
+        m = kf.Mesh(box_mesh(25, seed=0, bump=0.1))
+        q = m.view.q.copy()
+        hist = port.solve(m.g, 3.06, q, ts_max=8, stop_ratio=1e30)
+        check_history(hist, gold["steps"][:8])
+    finally:
+        kf.set_aoa(3.0)
