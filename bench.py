@@ -536,6 +536,33 @@ def run_gpu_arm(args, cfg):
     dist.close()
 
 
+def run_network_probe(args, cfg, kf, m):
+    """--kernel mpnn_apply: one application of the shipped network on the
+    workload's mesh (k_mlp_fwd), `reps` times; --kernel mpnn_train: pairs from
+    one solve on the mesh, then `reps` Adam steps of the library's training
+    loop (k_mlp_fwd, k_mlp_bwd, k_adam), batch 8."""
+    from kfun3d_b200 import learned
+    if args.kernel == "mpnn_apply":
+        net = learned.Network.load(WEIGHTS)
+        ms = m.time_learned_apply(net, args.reps)
+        net.close()
+        return {"kernel": args.kernel, "config": cfg["workload"], "ms": ms}
+    import time
+    x0, tgt, st = m.collect_pairs(stride=2, cap=16, ts_max=cfg["ts_max"], stop_ratio=cfg["stop_ratio"])
+    g = learned.Graph(m)
+    net = learned.Network(seed=0)
+    data = [learned.Sample(m, g, x0, tgt, cfg["aoa"], cfg["bump"], st)]
+    cuda_sync()
+    t0 = time.perf_counter()
+    losses = learned.train(net, data, args.reps, batch=8)
+    cuda_sync()
+    ms = (time.perf_counter() - t0) / args.reps * 1e3
+    net.close()
+    g.close()
+    return {"kernel": args.kernel, "config": cfg["workload"], "ms": ms, "pairs": int(x0.shape[0]),
+            "loss_first": losses[0], "loss_last": losses[-1]}
+
+
 def run_kernel_probe(args, cfg):
     """--kernel NAME: time one kernel family `reps` times on the workload's mesh
     and print {"kernel", "ms", "gbs"} -- the command the profiles use to
@@ -543,6 +570,10 @@ def run_kernel_probe(args, cfg):
     import kfun3d_b200 as kf
     configure(kf, cfg)
     m = kf.Mesh(mesh_path(cfg))
+    if args.kernel in ("mpnn_apply", "mpnn_train"):
+        print(json.dumps(run_network_probe(args, cfg, kf, m)))
+        m.close()
+        return
     v = m.view
     B = alg_bytes(v.nnodes, v.nedges, v.nfaces, v.ns, v.nf, v.nnodes + 2 * v.nedges, cfg["precision"])
     ms = m.time_kernel(args.kernel, args.reps)
@@ -564,8 +595,10 @@ def main():
                          "(default: the reference's own count from its full run, tests/golden/)")
     ap.add_argument("--kernel", default=None,
                     help="time one kernel family (flux, gradient, edge_flux, timestep, fill, ilu, sptrsv, mgs, "
-                         "gmres_iter) instead of the solve")
+                         "gmres_iter, mpnn_apply, mpnn_train) instead of the solve")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--n", type=int, default=None,
+                    help="with --kernel: mesh of n^3 nodes instead of the workload's (same seed and bump)")
     ap.add_argument("--precision", type=int, default=None, choices=[0, 1],
                     help="override the workload's preconditioner precision (with --kernel)")
     ap.add_argument("--ilu-order", type=int, default=None, choices=[0, 1],
@@ -576,6 +609,9 @@ def main():
         cfg["precision"] = args.precision
     if args.ilu_order is not None:
         cfg["ilu_order"] = args.ilu_order
+    if args.n is not None and args.kernel:
+        cfg["n"] = args.n
+        cfg["workload"] += f" (kernel probe on the {args.n}^3 mesh)"
     if args.kernel:
         run_kernel_probe(args, cfg)
     elif args.impl == "reference":

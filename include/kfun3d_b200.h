@@ -266,6 +266,17 @@ int kfun3d_sptrsv_device_noalloc(const GEOMETRY *g, const double *d_b, double *d
 /* Release the device mirror of g (also done by CXX_Matrix_Delete). */
 void kfun3d_device_release(GEOMETRY *g);
 
+/* Which device paths g's mirror uses (for tests and reports; builds the
+   mirror on first use): key "sptrsv_schedule" -> the triangular-solve
+   schedule of the active ILU(0) order (8 packed level launches, 7 four-lane
+   level launches, ...), "lsq_terms_match" -> 1 when the least-squares
+   terms recomputed on the device from per-node coefficients made there equal
+   the GEOMETRY's stored terms bit for bit, "visit_order_copies" -> 1 when
+   the residual passes work on copies of the node data in their spatial visit
+   order, "mgs_resident" -> 1 when Gram-Schmidt keeps the vector on chip.
+   -1 for an unknown key or on error. */
+long kfun3d_device_query(const GEOMETRY *g, const char *key);
+
 /* ---------------------------------------------------------------------
  * Part 3: the learned right preconditioner (no reference counterpart).
  *

@@ -103,6 +103,7 @@ def lib():
         "kfun3d_launch_count": (C.c_ulonglong, []),
         "kfun3d_reset_launch_count": (None, []),
         "kfun3d_device_release": (None, [G]),
+        "kfun3d_device_query": (C.c_long, [G, C.c_char_p]),
         "kfun3d_matrix_read": (C.c_long, [G, P(C.c_uint), P(C.c_uint), D]),
         "kfun3d_time_solve": (C.c_double, [G, P(SolverParams), C.c_int, P(Step), C.c_int, P(C.c_int)]),
         # learned preconditioner (include/kfun3d_b200.h, part 3)
@@ -340,6 +341,14 @@ class Mesh:
                                        C.byref(nl), C.byref(nu)) != 0:
             raise RuntimeError(f"kfun3d_ilu_order_plan failed: {last_error()}")
         return rank.astype(np.int64), nl.value, nu.value
+
+    def query(self, key):
+        """Device path in use (kfun3d_device_query): "sptrsv_schedule", "lsq_terms_match",
+        "visit_order_copies", "mgs_resident"."""
+        v = lib().kfun3d_device_query(self.g, key.encode())
+        if v < 0:
+            raise RuntimeError(f"kfun3d_device_query({key}) failed: {last_error()}")
+        return int(v)
 
     def time_kernel(self, which, reps=10):
         names = {"flux": 0, "timestep": 1, "fill": 2, "ilu": 3, "sptrsv": 4, "gmres_iter": 5,

@@ -293,7 +293,7 @@ void kf_ilu_release(DevMesh &m);
 void kf_free_packed(PackedSweep pk[2])
 {
   for (int s = 0; s < 2; s++) {
-    void *ptrs[] = {pk[s].row, pk[s].first, pk[s].col, pk[s].src, pk[s].chunk};
+    void *ptrs[] = {pk[s].row, pk[s].first, pk[s].col, pk[s].src, pk[s].chunk[0], pk[s].chunk[1]};
     for (void *q : ptrs)
       if (q) cudaFree(q);
     pk[s] = PackedSweep{};
@@ -304,8 +304,9 @@ void kf_free_packed(PackedSweep pk[2])
 // lower sweep contributes its lower blocks [d.y, d.z) (matrix/sptrsv.cpp:173-189
 // reads them in this column order); slot s of the upper sweep its inverted
 // diagonal block and then its upper blocks [d.y, d.z) (matrix/sptrsv.cpp:191-209).
-// A level's slots are cut into chunks of at most KF_PK_ROWS rows and
-// KF_PK_BLOCKS blocks, one CTA each.
+// Each level's slots are cut into chunks, one CTA each, twice: at most 32 rows
+// and 256 blocks, and at most 64 rows and 512 blocks.  KFUN3D_ERR_ARG (and
+// nothing allocated) when a row has more than KF_PK_ROW_MAX blocks.
 int kf_build_packed(PackedSweep pk[2], const HostPattern &p, const std::vector<uint4> &desc_l,
                     const std::vector<uint4> &desc_u)
 {
@@ -315,7 +316,11 @@ int kf_build_packed(PackedSweep pk[2], const HostPattern &p, const std::vector<u
     const std::vector<uint32_t> &lp = sw == 0 ? p.lev_l_ptr : p.lev_u_ptr;
     std::vector<uint32_t> row(N), first(N + 1), col, src;
     size_t nblk = 0;
-    for (size_t s = 0; s < N; s++) nblk += (d[s].z - d[s].y) + (sw == 1 ? 1u : 0u);
+    for (size_t s = 0; s < N; s++) {
+      const size_t len = (d[s].z - d[s].y) + (sw == 1 ? 1u : 0u);
+      if (len > KF_PK_ROW_MAX) { kf_free_packed(pk); return KFUN3D_ERR_ARG; }
+      nblk += len;
+    }
     if (nblk >= 0xffffffffu) { kf_free_packed(pk); return KFUN3D_ERR_ARG; }
     col.resize(nblk);
     src.resize(nblk);
@@ -324,7 +329,6 @@ int kf_build_packed(PackedSweep pk[2], const HostPattern &p, const std::vector<u
       const uint4 ds = d[s];
       row[s] = ds.x;
       first[s] = (uint32_t)k;
-      if (ds.z - ds.y + (sw == 1 ? 1u : 0u) > KF_PK_BLOCKS) { kf_free_packed(pk); return KFUN3D_ERR_ARG; }
       if (sw == 1) {
         col[k] = ds.x;
         src[k++] = p.diag[ds.x];
@@ -335,27 +339,31 @@ int kf_build_packed(PackedSweep pk[2], const HostPattern &p, const std::vector<u
       }
     }
     first[N] = (uint32_t)k;
-    std::vector<uint4> chunk;
-    std::vector<uint32_t> lev(1, 0);
-    uint32_t maxblk = 0;
-    for (size_t l = 0; l + 1 < lp.size(); l++) {
-      uint32_t s = lp[l];
-      while (s < lp[l + 1]) {
-        uint32_t e = s;
-        while (e < lp[l + 1] && e - s < KF_PK_ROWS && first[e + 1] - first[s] <= KF_PK_BLOCKS) e++;
-        chunk.push_back(make_uint4(s, e, first[s], first[e]));
-        maxblk = std::max(maxblk, first[e] - first[s]);
-        s = e;
-      }
-      lev.push_back((uint32_t)chunk.size());
-    }
     PackedSweep &o = pk[sw];
     o.nblk = (uint32_t)nblk;
-    o.maxblk = maxblk;
-    o.lev = lev;
-    if (upload(&o.row, row.data(), N) != cudaSuccess || upload(&o.first, first.data(), N + 1) != cudaSuccess ||
-        upload(&o.col, col.data(), nblk) != cudaSuccess || upload(&o.src, src.data(), nblk) != cudaSuccess ||
-        upload(&o.chunk, chunk.data(), chunk.size()) != cudaSuccess) {
+    bool ok = upload(&o.row, row.data(), N) == cudaSuccess && upload(&o.first, first.data(), N + 1) == cudaSuccess &&
+              upload(&o.col, col.data(), nblk) == cudaSuccess && upload(&o.src, src.data(), nblk) == cudaSuccess;
+    for (int cut = 0; cut < 2 && ok; cut++) {
+      const uint32_t rows = cut == 0 ? 32u : 64u, budget = 8u * rows;
+      std::vector<uint4> chunk;
+      std::vector<uint32_t> lev(1, 0);
+      uint32_t maxblk = 0;
+      for (size_t l = 0; l + 1 < lp.size(); l++) {
+        uint32_t s = lp[l];
+        while (s < lp[l + 1]) {
+          uint32_t e = s + 1;   // a chunk holds at least one row, however long
+          while (e < lp[l + 1] && e - s < rows && first[e + 1] - first[s] <= budget) e++;
+          chunk.push_back(make_uint4(s, e, first[s], first[e]));
+          maxblk = std::max(maxblk, first[e] - first[s]);
+          s = e;
+        }
+        lev.push_back((uint32_t)chunk.size());
+      }
+      o.lev[cut] = lev;
+      o.maxblk[cut] = maxblk;
+      ok = upload(&o.chunk[cut], chunk.data(), chunk.size()) == cudaSuccess;
+    }
+    if (!ok) {
       cudaGetLastError();
       kf_free_packed(pk);
       return KFUN3D_ERR_CUDA;
@@ -375,7 +383,8 @@ static void release_device(MatrixHandle *h)
                   m->wf_n, m->s_n, m->f_n, m->bnd_of, m->bnd_node, m->bnd_ptr, m->bnd_ent, m->ia, m->ja,
                   m->diag, m->tblk, m->lpos, m->last_lower, m->lev_l, m->lev_u, m->A, m->lslot, m->dinv,
                   m->Af, m->dinvf, m->q, m->r, m->gx, m->gy, m->gz, m->cdt, m->w, m->t, m->x, m->rhs, m->V,
-                  m->red, m->scal, m->forces, m->dscr, m->status, m->flags, m->ticket, m->part, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->n0s, m->pair_ptr, m->pairs, m->lev_ptr_d, m->bar, m->Z, m->qold, m->fy, m->fx, m->pscr, m->ord, m->rowof, m->egeo_s};
+                  m->red, m->scal, m->forces, m->dscr, m->status, m->flags, m->ticket, m->part, m->lsq_coef,
+                  m->qv, m->xyzv, m->gxv, m->gyv, m->gzv, m->inc_othv, m->n0v, m->n1v, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->eseg, m->n0s, m->pair_ptr, m->pairs, m->lev_ptr_d, m->bar, m->Z, m->qold, m->fy, m->fx, m->pscr, m->ord, m->rowof, m->egeo_s};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (m->h_scal) cudaFreeHost(m->h_scal);
@@ -387,6 +396,17 @@ static void release_device(MatrixHandle *h)
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
   h->dev = nullptr;
+}
+
+extern "C" long kfun3d_device_query(const GEOMETRY *g, const char *key)
+{
+  DevMesh *m = key ? kf_device(g) : nullptr;
+  if (!m) return -1;
+  if (strcmp(key, "sptrsv_schedule") == 0) return m->trsv_mode;
+  if (strcmp(key, "lsq_terms_match") == 0) return m->lsq_match ? 1 : 0;
+  if (strcmp(key, "visit_order_copies") == 0) return m->visit ? 1 : 0;
+  if (strcmp(key, "mgs_resident") == 0) return m->mgs_resident ? 1 : 0;
+  return -1;
 }
 
 extern "C" void kfun3d_device_release(GEOMETRY *g)
@@ -594,6 +614,34 @@ DevMesh *kf_device(const GEOMETRY *g)
       KF_CUDA(upload(&m->in1_ptr, iptr.data(), N + 1));
       KF_CUDA(upload(&m->in1_edge, iedge.data(), E));
       KF_CUDA(cudaMalloc(&m->eres, std::max<size_t>(E, 1) * sizeof(double4)));
+      // fast mode sums each node's n0 side in the edge pass (KFUN3D_RESIDUAL_SEG=0: not)
+      const char *senv = getenv("KFUN3D_RESIDUAL_SEG");
+      if (!(senv && strcmp(senv, "0") == 0)) KF_CUDA(cudaMalloc(&m->eseg, std::max<size_t>(E, 1) * sizeof(double4)));
+      // visit-order copies for the residual passes when the visit order is
+      // not the mesh's own (KFUN3D_VISIT_COPIES=0: not): the edges' end
+      // points and each incidence's other end as visit positions, the
+      // coordinates in visit order, room for the state and the gradients
+      const char *venv = getenv("KFUN3D_VISIT_COPIES");
+      m->visit = m->spatial_order && !(venv && strcmp(venv, "0") == 0);
+      if (m->visit) {
+        std::vector<uint32_t> rowv(N), othv(2 * (size_t)E), e0v(E), e1v(E);
+        std::vector<double4> xv(N);
+        for (uint32_t p2 = 0; p2 < N; p2++) {
+          rowv[ord[p2]] = p2;
+          const uint32_t nd = ord[p2];
+          xv[p2] = make_double4(g->n->xyz->x0[nd], g->n->xyz->x1[nd], g->n->xyz->x2[nd], 0.0);
+        }
+        std::vector<uint32_t> othm(2 * (size_t)E);
+        KF_CUDA(cudaMemcpy(othm.data(), m->inc_oth, 2 * (size_t)E * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < 2 * (size_t)E; k++) othv[k] = rowv[othm[k]];
+        for (uint32_t e = 0; e < E; e++) { e0v[e] = rowv[n0s[e]]; e1v[e] = rowv[n1s[e]]; }
+        KF_CUDA(upload(&m->inc_othv, othv.data(), othv.size()));
+        KF_CUDA(upload(&m->n0v, e0v.data(), E));
+        KF_CUDA(upload(&m->n1v, e1v.data(), E));
+        KF_CUDA(upload(&m->xyzv, xv.data(), N));
+        double4 **vv[] = {&m->qv, &m->gxv, &m->gyv, &m->gzv};
+        for (double4 **v : vv) KF_CUDA(cudaMalloc(v, (size_t)N * sizeof(double4)));
+      }
     }
   }
   // wall faces (colour order) with normals -(1/6) a x b (src/flux.c:485-508)
@@ -729,32 +777,40 @@ DevMesh *kf_device(const GEOMETRY *g)
     // the packed factor (room for FP64 blocks, shared by both ILU orders) and
     // this pattern's packed level schedule
     KF_CUDA(cudaMalloc(&m->pk_buf, 16 * (size_t)m->nnz * sizeof(double)));
-    if (kf_build_packed(m->iset[0].pk, p, dl, du) != KFUN3D_OK) {
+    const int pkrc = kf_build_packed(m->iset[0].pk, p, dl, du);   // ERR_ARG: rows too long, no packed schedule
+    if (pkrc == KFUN3D_ERR_CUDA) {
       kf_set_error(KFUN3D_ERR_CUDA, "device mirror: building the packed triangular-solve schedule failed");
       return nullptr;
+    }
+    // chunk cut per factor precision (KFUN3D_PK_ROWS="<fp64 rows>,<fp32 rows>", 32 or 64 each)
+    const char *fenv = getenv("KFUN3D_PK_FP64");
+    m->pk_fp64 = fenv && strcmp(fenv, "1") == 0;
+    const char *renv = getenv("KFUN3D_PK_ROWS");
+    if (renv) {
+      int r64 = 0, r32 = 0;
+      if (sscanf(renv, "%d,%d", &r64, &r32) == 2) {
+        m->pk_cut[0] = r64 == 32 ? 0 : 1;
+        m->pk_cut[1] = r32 == 32 ? 0 : 1;
+      }
     }
     // triangular-solve schedule (KFUN3D_SPTRSV): "packed" (default: one
     // launch per level with programmatic dependent launch, each CTA's rows
     // one contiguous run of the packed factor staged into shared memory by a
     // bulk copy), "pdl4" (one launch per level with programmatic dependent
     // launch, 4 lanes per row, blocks read in the matrix's order), "pdl"
-    // (the same with 16 lanes per row), "levels16" (one launch per level, 16
-    // lanes per row), "persistent" / "mono" (one cooperative launch, bounded
-    // grid barrier between levels), "syncfree" (per-row flags, no level
-    // barriers) or "levels" (one launch per level, 4 lanes per row)
+    // (the same with 16 lanes per row), "persistent" / "mono" (one
+    // cooperative launch, bounded grid barrier between levels), "syncfree"
+    // (per-row flags, no level barriers; the allocation-free entry point's
+    // sweep) or "levels" (one plain launch per level, 4 lanes per row)
     const char *env = getenv("KFUN3D_SPTRSV");
-    // default: one launch per level with programmatic dependent launch and
-    // four lanes per row (120^3 box: 1.28 / 1.15 ms FP64 / FP32 against
-    // 1.51 / 1.27 ms for the persistent sweep)
-    m->trsv_mode = 8;
+    m->trsv_mode = m->iset[0].pk[0].chunk[0] ? 8 : 7;
     if (env && strcmp(env, "pdl") == 0) m->trsv_mode = 4;
-    if (env && strcmp(env, "levels16") == 0) m->trsv_mode = 2;
     if (env && strcmp(env, "persistent") == 0) m->trsv_mode = 3;
     if (env && strcmp(env, "syncfree") == 0) m->trsv_mode = 1;
     if (env && strcmp(env, "levels") == 0) m->trsv_mode = 0;
     if (env && strcmp(env, "mono") == 0) m->trsv_mode = 5;
     if (env && strcmp(env, "pdl4") == 0) m->trsv_mode = 7;
-    if (env && strcmp(env, "packed") == 0) m->trsv_mode = 8;
+    if (env && strcmp(env, "packed") == 0 && m->iset[0].pk[0].chunk[0]) m->trsv_mode = 8;
     std::vector<uint32_t> lp(p.lev_l_ptr);
     lp.insert(lp.end(), p.lev_u_ptr.begin(), p.lev_u_ptr.end());
     KF_CUDA(upload(&m->lev_ptr_d, lp.data(), lp.size()));
@@ -779,6 +835,12 @@ DevMesh *kf_device(const GEOMETRY *g)
     s0.fill_blk = m->inc_blk; s0.fill_diag = m->diag; s0.fill_last = m->last_lower; s0.fill_lpos = m->lpos;
     s0.valid = true;
     m->fill_blk = m->inc_blk; m->fill_diag = m->diag; m->fill_last = m->last_lower; m->fill_lpos = m->lpos;
+  }
+  // least-squares coefficients on the device; the gradient's terms on the fly
+  // when they reproduce the GEOMETRY's stored ones bit for bit
+  if (kf_exact::lsq_setup(*m) != KFUN3D_OK) {
+    kf_set_error(KFUN3D_ERR_CUDA, "device mirror: least-squares coefficients failed");
+    return nullptr;
   }
   KF_CUDA(cudaDeviceSynchronize());
   return m;

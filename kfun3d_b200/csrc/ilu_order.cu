@@ -56,15 +56,12 @@ void activate(DevMesh &m, const IluSet &s)
   m.trsv_mode = s.trsv_mode;
   m.syncfree = s.trsv_mode == 1;
   m.fill_blk = s.fill_blk; m.fill_diag = s.fill_diag; m.fill_last = s.fill_last; m.fill_lpos = s.fill_lpos;
-  m.ntiles = s.ntiles; m.tile_ptr = s.tile_ptr; m.tile_step = s.tile_step; m.tile_pub = s.tile_pub;
-  m.tile_wait = s.tile_wait; m.tile_desc = s.tile_desc; m.tile_prog = s.tile_prog;
-  m.tile_pack = s.tile_pack; m.tile_ndesc = s.tile_ndesc;
   m.pk[0] = s.pk[0];
   m.pk[1] = s.pk[1];
 }
 
-// Tiles of the tiled triangular sweep: columns along the sweep direction
-// (1,1,1), cut in the plane across it (u = x - y, w = x + y - 2z) into
+// Tiles of the tile-major order (KFUN3D_ILU_PERM=tiles): columns along the
+// sweep direction (1,1,1), cut in the plane across it (u = x - y, w = x + y - 2z) into
 // floor(sqrt(T)) strips by u, each strip into cells by w, with equal shares
 // of the cross-section rather than of the nodes: a node weighs 1 / (the
 // extent in s = x + y + z of the nodes that project near it, on a 64 x 64
@@ -171,8 +168,7 @@ std::vector<uint32_t> partition_tiles(const double *X, const double *Y, const do
 //     and 1.3 ms in the mesh's random numbering;
 //   KFUN3D_ILU_PERM=tiles: tile by tile (ids as above), ascending s within a
 //     tile: between tiles the edges point from the lower tile id to the
-//     higher, so the tiled sweep's CTAs depend on their neighbours one way
-//     only and run as a pipeline;
+//     higher (an order whose tiles depend on their neighbours one way only);
 //   KFUN3D_ILU_PERM=sweep: ascending s over the whole mesh (level sets: about
 //     3n on an n^3 Kuhn box, against about 9n for the Morton order of the
 //     jittered coordinates);
@@ -243,152 +239,6 @@ std::vector<uint32_t> spatial_rank(const GEOMETRY *g, size_t N, const std::vecto
   return rank;
 }
 
-// Host form of the tiled sweep: per tile its rows of each sweep grouped by
-// level (a step, at most KF_TILE_STEP_ROWS rows; longest rows first; desc.w
-// = 1 in the upper sweep), and before each step the progress it
-// needs from other tiles -- for every row of the step and every column row
-// j held by another tile t', progress[t'] >= (level of j) + 1 in the lower
-// sweep, nlev_l + (backward level of j) + 1 in the upper sweep -- keeping
-// only requirements that earlier steps of the tile did not already cover.
-// A tile publishes level + 1 (lower) or nlev_l + level + 1 (upper) after a
-// step that another tile waits for (flagged by bit 31 of pub).  Every
-// requirement names a strictly earlier level, so with all tiles resident the
-// sweep cannot deadlock.
-//
-// When every wait of the lower sweep points to a lower tile id and every
-// wait of the upper sweep to a higher one (the tile-major numbering), the
-// tiles form a pipeline and a requirement may ask for `slack` more steps of
-// the other tile than the rows need (capped at its last step of the sweep):
-// the downstream tile then trails far enough behind that it rarely finds a
-// requirement unmet, without any wait cycle.
-struct TileHost {
-  std::vector<uint32_t> ptr, pub;
-  std::vector<uint4> step, desc;
-  std::vector<uint2> wait;
-  std::vector<uint2> raw;            // requirements before slack and filtering
-  std::vector<uint32_t> raw_ptr;     // per step into raw
-};
-
-TileHost build_tiles(const HostPattern &p, const std::vector<uint32_t> &rank, const std::vector<uint32_t> &tile,
-                     uint32_t T, size_t N, uint32_t slack)
-{
-  std::vector<uint32_t> rt(N), ll(N), ul(N);
-  for (size_t i = 0; i < N; i++) rt[rank[i]] = tile[i];
-  const uint32_t nl = (uint32_t)p.lev_l_ptr.size() - 1, nu = (uint32_t)p.lev_u_ptr.size() - 1;
-  for (uint32_t l = 0; l < nl; l++)
-    for (uint32_t q = p.lev_l_ptr[l]; q < p.lev_l_ptr[l + 1]; q++) ll[p.lev_l[q]] = l;
-  for (uint32_t l = 0; l < nu; l++)
-    for (uint32_t q = p.lev_u_ptr[l]; q < p.lev_u_ptr[l + 1]; q++) ul[p.lev_u[q]] = l;
-  std::vector<uint32_t> tcnt(T + 1, 0), trow(N);
-  for (size_t i = 0; i < N; i++) tcnt[rt[i] + 1]++;
-  for (uint32_t t = 0; t < T; t++) tcnt[t + 1] += tcnt[t];
-  {
-    std::vector<uint32_t> fillp(tcnt.begin(), tcnt.end() - 1);
-    for (size_t i = 0; i < N; i++) trow[fillp[rt[i]]++] = (uint32_t)i;
-  }
-  std::vector<TileHost> part(T);
-  std::vector<char> two_way(T, 0);
-  auto for_tiles = [T](auto &&fn) {
-    const unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    std::vector<std::thread> th;
-    for (unsigned k = 0; k < nth; k++) {
-      const size_t a = (size_t)T * k / nth, b = (size_t)T * (k + 1) / nth;
-      if (a < b) th.emplace_back([&fn, a, b] { for (size_t t = a; t < b; t++) fn(t); });
-    }
-    for (auto &x : th) x.join();
-  };
-  // 1. steps, row descriptors and the raw requirements
-  for_tiles([&](size_t t) {
-    TileHost &h = part[t];
-    for (int upper = 0; upper < 2; upper++) {
-      h.ptr.push_back((uint32_t)h.step.size());
-      std::vector<uint32_t> rows(trow.begin() + tcnt[t], trow.begin() + tcnt[t + 1]);
-      auto len = [&](uint32_t i) { return upper ? p.ia[i + 1] - p.diag[i] - 1 : p.diag[i] - p.ia[i]; };
-      auto lev = [&](uint32_t i) { return upper ? ul[i] : ll[i]; };
-      std::stable_sort(rows.begin(), rows.end(), [&](uint32_t a, uint32_t b) {
-        return lev(a) != lev(b) ? lev(a) < lev(b) : len(a) > len(b);
-      });
-      for (size_t q0 = 0; q0 < rows.size();) {
-        size_t qe = q0;
-        const uint32_t L = lev(rows[q0]);
-        while (qe < rows.size() && lev(rows[qe]) == L) qe++;
-        // a level of more than KF_TILE_STEP_ROWS rows takes several steps;
-        // only the last one completes the level
-        const size_t q1 = std::min(qe, q0 + KF_TILE_STEP_ROWS);
-        uint4 st = make_uint4((uint32_t)h.desc.size(), 0, 0, 0);
-        h.raw_ptr.push_back((uint32_t)h.raw.size());
-        const size_t r0 = h.raw.size();
-        for (size_t q = q0; q < q1; q++) {
-          const uint32_t i = rows[q];
-          const uint32_t jb = upper ? p.diag[i] + 1 : p.ia[i], je = upper ? p.ia[i + 1] : p.diag[i];
-          h.desc.push_back(make_uint4(i, jb, je, (uint32_t)upper));
-          for (uint32_t j = jb; j < je; j++) {
-            const uint32_t c = p.ja[j], tc = rt[c];
-            if (tc == t) continue;
-            if (upper ? tc < t : tc > t) two_way[t] = 1;
-            const uint32_t v = upper ? nl + ul[c] + 1 : ll[c] + 1;
-            auto it = std::find_if(h.raw.begin() + r0, h.raw.end(), [&](const uint2 &x) { return x.x == tc; });
-            if (it == h.raw.end()) h.raw.push_back(make_uint2(tc, v));
-            else it->y = std::max(it->y, v);
-          }
-        }
-        st.y = (uint32_t)h.desc.size();
-        h.step.push_back(st);
-        if (q1 == qe) h.pub.push_back(upper ? nl + L + 1 : L + 1);
-        else h.pub.push_back(h.pub.empty() ? 0u : h.pub.back());
-        q0 = q1;
-      }
-    }
-    h.ptr.push_back((uint32_t)h.step.size());
-    h.raw_ptr.push_back((uint32_t)h.raw.size());
-  });
-  if (std::find(two_way.begin(), two_way.end(), 1) != two_way.end()) slack = 0;
-  // 2. slack, then only the requirements earlier steps do not cover
-  for_tiles([&](size_t t) {
-    TileHost &h = part[t];
-    std::vector<std::pair<uint32_t, uint32_t>> have;
-    for (uint32_t k = 0; k < (uint32_t)h.step.size(); k++) {
-      const int upper = k >= h.ptr[1];
-      h.step[k].z = (uint32_t)h.wait.size();
-      for (uint32_t q = h.raw_ptr[k]; q < h.raw_ptr[k + 1]; q++) {
-        uint2 nd = h.raw[q];
-        if (slack) {
-          const TileHost &o = part[nd.x];
-          auto b = o.pub.begin() + o.ptr[upper], e = o.pub.begin() + o.ptr[upper + 1];
-          const uint32_t target = std::min(nd.y + slack, *(e - 1));
-          nd.y = *std::lower_bound(b, e, target);
-        }
-        auto it = std::find_if(have.begin(), have.end(), [&](const auto &x) { return x.first == nd.x; });
-        if (it != have.end() && it->second >= nd.y) continue;
-        if (it == have.end()) have.push_back({nd.x, nd.y});
-        else it->second = nd.y;
-        h.wait.push_back(nd);
-      }
-      h.step[k].w = (uint32_t)h.wait.size();
-    }
-  });
-  // 3. one array of each, steps' offsets rebased
-  TileHost out;
-  for (uint32_t t = 0; t < T; t++) {
-    const TileHost &h = part[t];
-    const uint32_t s0 = (uint32_t)out.step.size(), d0 = (uint32_t)out.desc.size(), w0 = (uint32_t)out.wait.size();
-    out.ptr.push_back(s0 + h.ptr[0]);
-    out.ptr.push_back(s0 + h.ptr[1]);
-    for (const uint4 &st : h.step) out.step.push_back(make_uint4(st.x + d0, st.y + d0, st.z + w0, st.w + w0));
-    out.pub.insert(out.pub.end(), h.pub.begin(), h.pub.end());
-    out.desc.insert(out.desc.end(), h.desc.begin(), h.desc.end());
-    out.wait.insert(out.wait.end(), h.wait.begin(), h.wait.end());
-  }
-  out.ptr.push_back((uint32_t)out.step.size());
-  // a step's completion is published only when another tile waits for it
-  std::vector<std::vector<uint32_t>> needed(T);
-  for (const uint2 &w : out.wait) needed[w.x].push_back(w.y);
-  for (auto &v : needed) std::sort(v.begin(), v.end());
-  for (uint32_t t = 0; t < T; t++)
-    for (uint32_t k = out.ptr[2 * t]; k < out.ptr[2 * t + 2]; k++)
-      if (std::binary_search(needed[t].begin(), needed[t].end(), out.pub[k])) out.pub[k] |= 0x80000000u;
-  return out;
-}
 
 int build_spatial(DevMesh &m, const GEOMETRY *g)
 {
@@ -445,7 +295,7 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
     by_length(du, p.lev_u_ptr);
     up(&s.desc_l, dl);
     up(&s.desc_u, du);
-    if (ok && kf_build_packed(s.pk, p, dl, du) != KFUN3D_OK) ok = false;
+    if (ok && kf_build_packed(s.pk, p, dl, du) == KFUN3D_ERR_CUDA) ok = false;
   }
   // the fill's view of the renumbered pattern, per node of the mesh
   {
@@ -478,42 +328,18 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
     up(&s.fill_last, fl);
     up(&s.fill_lpos, fp);
   }
-  {
-    uint32_t slack = 2;
-    const char *senv = getenv("KFUN3D_TILE_SLACK");   // steps of slack in the pipeline (0-64)
-    if (senv && atoi(senv) >= 0 && atoi(senv) <= 64) slack = (uint32_t)atoi(senv);
-    const TileHost th = build_tiles(p, rank, tile, T, N, slack);
-    s.ntiles = T;
-    up(&s.tile_ptr, th.ptr);
-    up(&s.tile_step, th.step);
-    up(&s.tile_pub, th.pub);
-    up(&s.tile_wait, th.wait);
-    up(&s.tile_desc, th.desc);
-    if (ok && cudaMalloc(&s.tile_prog, T * sizeof(unsigned)) != cudaSuccess) ok = false;
-    s.tile_ndesc = (uint32_t)th.desc.size();
-  }
   up(&m.ilu_rank, rank);
   if (ok && cudaMalloc(&m.pb, 4 * N * sizeof(double)) != cudaSuccess) ok = false;
   if (ok && cudaMalloc(&m.px, 4 * N * sizeof(double)) != cudaSuccess) ok = false;
   // one launch per level (programmatic dependent launch, each CTA's rows one
   // contiguous run of the packed factor) by default; KFUN3D_SPTRSV picks
   // another schedule
-  s.trsv_mode = 8;
+  s.trsv_mode = s.pk[0].chunk[0] ? 8 : 7;
   const char *env = getenv("KFUN3D_SPTRSV");
   if (env && strcmp(env, "pdl4") == 0) s.trsv_mode = 7;
-  if (env && strcmp(env, "packed") == 0) s.trsv_mode = 8;
+  if (env && strcmp(env, "packed") == 0 && s.pk[0].chunk[0]) s.trsv_mode = 8;
   if (env && strcmp(env, "pdl") == 0) s.trsv_mode = 4;
-  if (env && strcmp(env, "tiled") == 0) s.trsv_mode = 6;
-  if (ok && s.trsv_mode == 6) {
-    // the packed FP32 factor of the tiled sweep (without room for it the
-    // FP32 solves take the unpacked one)
-    if (cudaMalloc(&s.tile_pack, (size_t)s.tile_ndesc * KF_TILE_REC) != cudaSuccess) {
-      cudaGetLastError();
-      s.tile_pack = nullptr;
-    }
-  }
   if (env && strcmp(env, "mono") == 0) s.trsv_mode = 5;
-  if (env && strcmp(env, "levels16") == 0) s.trsv_mode = 2;
   if (env && strcmp(env, "syncfree") == 0) s.trsv_mode = 1;
   if (!ok) {
     kf_set_error(KFUN3D_ERR_CUDA, "spatial ILU(0) order: out of device memory");
@@ -556,7 +382,6 @@ void kf_ilu_release(DevMesh &m)
   IluSet &s = m.iset[1];
   void *ptrs[] = {s.ia, s.ja, s.diag, s.tblk, s.lpos, s.last_lower, s.pair_ptr, s.pairs, s.lev_l, s.lev_u,
                   s.lev_ptr_d, s.desc_l, s.desc_u, s.fill_blk, s.fill_diag, s.fill_last, s.fill_lpos,
-                  s.tile_ptr, s.tile_step, s.tile_pub, s.tile_wait, s.tile_desc, s.tile_prog, s.tile_pack,
                   m.ilu_rank, m.pb, m.px};
   for (void *p : ptrs)
     if (p) cudaFree(p);

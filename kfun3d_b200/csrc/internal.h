@@ -102,10 +102,7 @@ __device__ __forceinline__ bool kf_grid_barrier(unsigned *bar, int *err)
 // The matrix pattern the Jacobian fill, ILU(0) and the triangular solves use:
 // the reference's numbering (set 0), or its rows and columns renumbered in a
 // spatial order (set 1, kfun3d_set_ilu_order).  fill_* are indexed by node in
-// the mesh's numbering and point into the set's pattern.  tile_*: the tiled
-// triangular sweep of set 1 (one CTA per tile, trsv_mode 6).
-constexpr uint32_t KF_TILE_STEP_ROWS = 96;   // rows of a step of the tiled sweep, at most
-constexpr uint32_t KF_TILE_REC = 624;         // bytes of a row record of the packed FP32 factor
+// the mesh's numbering and point into the set's pattern.
 
 // Packed level schedule of the triangular solves (trsv_mode 8), one per
 // sweep (0 lower, 1 upper): the factor's blocks streamed in level-slot order
@@ -113,17 +110,19 @@ constexpr uint32_t KF_TILE_REC = 624;         // bytes of a row record of the pa
 // blocks, in column order), so that the rows one CTA solves in one level are
 // one contiguous run of the stream.  The blocks are copied into the stream
 // after every factorisation (k_trsv_pack, through src).
-constexpr uint32_t KF_PK_ROWS = 64;     // rows of a chunk (one CTA of 256 threads), at most
-constexpr uint32_t KF_PK_BLOCKS = 512;  // blocks of a chunk, at most (its shared-memory stage)
+constexpr uint32_t KF_PK_ROW_MAX = 1536;   // blocks of one row, at most (larger: no packed schedule)
 struct PackedSweep {
   uint32_t *row = nullptr;     // [N] matrix row of each slot
   uint32_t *first = nullptr;   // [N+1] first streamed block of each slot
   uint32_t *col = nullptr;     // [nblk] column of each streamed block
   uint32_t *src = nullptr;     // [nblk] matrix block copied to each stream position
-  uint4 *chunk = nullptr;      // per CTA: (first slot, end slot, first block, end block)
-  std::vector<uint32_t> lev;   // first chunk of each level, nlev + 1 entries
-  uint32_t nblk = 0;           // blocks in the stream
-  uint32_t maxblk = 0;         // blocks of the largest chunk
+  // two cuts of the levels into chunks, [0] of at most 32 rows and 256 blocks
+  // (one CTA of 128 threads), [1] of at most 64 rows and 512 blocks (256
+  // threads); a row longer than the budget is a chunk of its own
+  uint4 *chunk[2] = {nullptr, nullptr};   // per CTA: (first slot, end slot, first block, end block)
+  std::vector<uint32_t> lev[2];           // first chunk of each level, nlev + 1 entries
+  uint32_t maxblk[2] = {0, 0};            // blocks of the largest chunk
+  uint32_t nblk = 0;                      // blocks in the stream
 };
 
 struct IluSet {
@@ -140,15 +139,6 @@ struct IluSet {
   uint32_t *fill_diag = nullptr;   // [N] diagonal block of each node
   uint32_t *fill_last = nullptr;   // [N] the node's row's last-touched lower block (or ~0)
   uint32_t *fill_lpos = nullptr;   // [N] the node's row's first persistent L slot
-  uint32_t ntiles = 0;
-  uint32_t *tile_ptr = nullptr;    // [2T+1] tile t: lower steps [2t, 2t+1), upper steps [2t+1, 2t+2)
-  uint4 *tile_step = nullptr;      // per step: rows [x, y) of tile_desc, waits [z, w)
-  uint32_t *tile_pub = nullptr;    // per step: progress the tile publishes after it
-  uint2 *tile_wait = nullptr;      // (tile, progress it must have reached)
-  uint4 *tile_desc = nullptr;      // [2N] row descriptors (row, first block, end block), by tile and step
-  unsigned *tile_prog = nullptr;   // [T] progress counters, cleared before each solve
-  uint8_t *tile_pack = nullptr;    // [2N x KF_TILE_REC] FP32 factor rows in tile_desc order
-  uint32_t tile_ndesc = 0;
   PackedSweep pk[2];               // packed level schedule (trsv_mode 8)
 };
 
@@ -178,6 +168,15 @@ struct DevMesh {
   double *inc_w = nullptr;        // [3][wstride] least-squares terms seen from the node
   uint32_t wstride = 0;           // 2E rounded up to a multiple of 4 (16-byte aligned rows)
   unsigned grad_smem = 0;         // dynamic shared memory of k_gradient_tma (0: not used)
+  double4 *lsq_coef = nullptr;    // [2N] least-squares coefficients per node, computed on the device
+  bool lsq_match = false;         // the terms recomputed from lsq_coef equal the stored ones bit for bit
+  int grad_lanes = 1;             // lanes per node of the gradient in the mesh's order (1 or 4)
+  // visit-order copies for the residual passes on large meshes (spatial_order
+  // and two_pass): state, coordinates, gradients, the other end of each
+  // incidence and the end points of each stored edge as visit positions
+  bool visit = false;
+  double4 *qv = nullptr, *xyzv = nullptr, *gxv = nullptr, *gyv = nullptr, *gzv = nullptr;
+  uint32_t *inc_othv = nullptr, *n0v = nullptr, *n1v = nullptr;
   // two-pass residual (every edge has n0 < n1); edge arrays in storage
   // order: grouped by n0 in node-visit order (ord), each group in edge order
   bool two_pass = false;
@@ -188,6 +187,7 @@ struct DevMesh {
   uint32_t *in1_ptr = nullptr;    // [N+1] edges with n1 = ord[p], in edge order
   uint32_t *in1_edge = nullptr;   // [E] their storage positions
   double4 *eres = nullptr;        // [E] edge fluxes, storage order
+  double4 *eseg = nullptr;        // [E] fast mode: n0-run sums of a warp's edges at the runs' first positions
   uint32_t *wf_nodes = nullptr;   // [3F] wall faces in colour order
   double *wf_n = nullptr;         // [3F] wall-face normals -(1/6) a x b
   uint32_t *col = nullptr;        // [ncol+1] wall-face colour offsets
@@ -222,10 +222,11 @@ struct DevMesh {
   int *status = nullptr;          // device status words: [0] pivot failure, [1] wait timeout
   // sync-free triangular solves
   bool syncfree = true;
-  int trsv_mode = 4;               // 0 levels (4 lanes/row), 1 sync-free, 2 levels (16 lanes/row),
-                                   // 3 one persistent launch, grid barrier between levels,
-                                   // 4 levels with programmatic dependent launch,
-                                   // 5 one persistent launch, 1-3 CTAs per SM, counter barrier
+  int trsv_mode = 8;               // 0 levels (4 lanes/row), 1 sync-free, 3 one persistent launch,
+                                   // grid barrier between levels, 4 levels with programmatic
+                                   // dependent launch (16 lanes/row), 5 one persistent launch,
+                                   // 1-3 CTAs per SM, counter barrier, 7 the same with 4 lanes/row,
+                                   // 8 packed level launches (default)
   unsigned trsv_grid = 0;          // persistent grid (whole blocks resident on every SM)
   uint32_t *flags = nullptr;       // [N] per-row completion epoch
   unsigned long long *ticket = nullptr;   // unused (kept zero)
@@ -250,14 +251,9 @@ struct DevMesh {
   double *h_scal = nullptr;       // pinned host mirror of scal
   // ILU(0) ordering: the active set's fields are copied into the fields above
   IluSet iset[2];
-  uint32_t ntiles = 0;            // active set's tiled sweep (trsv_mode 6)
-  uint32_t *tile_ptr = nullptr, *tile_pub = nullptr;
-  uint4 *tile_step = nullptr, *tile_desc = nullptr;
-  uint2 *tile_wait = nullptr;
-  unsigned *tile_prog = nullptr;
-  uint8_t *tile_pack = nullptr;
-  uint32_t tile_ndesc = 0;
   PackedSweep pk[2];              // active set's packed level schedule
+  int pk_cut[2] = {0, 0};         // chunk cut used with FP64 / FP32 factors (0: 32 rows, 1: 64 rows)
+  bool pk_fp64 = false;           // FP64 factors also take the packed schedule (KFUN3D_PK_FP64=1)
   void *pk_buf = nullptr;         // the packed factor: lower stream, then upper stream (FP64 or FP32 blocks)
   int ilu_active = 0;             // 1: the spatial set is active
   uint32_t *ilu_rank = nullptr;   // [N] row of each node in the spatial set
@@ -295,6 +291,8 @@ void kfun3d_reset_launch_count_by(unsigned long long n);   // undo counts taken 
   void ilu(DevMesh &m, int precision);                                                  \
   void sptrsv(DevMesh &m, const double *b, double *x, int precision);                   \
   void sptrsv_flags(DevMesh &m, const double *b, double *x, int precision, uint32_t *flags); \
+  int lsq_setup(DevMesh &m);                                                            \
+  void gradient_to_mesh_order(DevMesh &m);                                              \
   void jv_combine(DevMesh &m, double *y, const double *r, const double *w,              \
                   const double *q, const double *scal, int ia);                          \
   }

@@ -502,45 +502,56 @@ __global__ void __launch_bounds__(128) k_lsq_check(uint32_t N, const uint32_t *_
   if (nbad) atomicAdd(bad, nbad);
 }
 
-// k_gradient with the least-squares terms computed from the node's seven
-// coefficients and the edge vector instead of read per incidence (4 bytes
-// per incidence from memory instead of 28; the end points' coordinates are
-// gathered like their states).  ROLE_BY_INDEX: every edge has n0 < n1, so n
-// is an edge's n0 exactly when the other end has the larger index.
-template <bool ROLE_BY_INDEX>
-__global__ void __launch_bounds__(256) k_gradient_otf(uint32_t N, const uint32_t *__restrict__ ord,
+// The gradient with four lanes per node, lane r owning state component r:
+// each lane sums its component's three gradient entries over the node's
+// incident edges in edge order (the same additions as one thread doing all
+// four components, so the same result).  A quad of lanes reads one 32-byte
+// state record per edge and shares the index and term loads; a lane keeps 3
+// accumulators instead of 12, so four times as many nodes are in flight.
+// ord == nullptr: node data in visit order (row p of the incidence is node p
+// of q and of the outputs).
+__global__ void __launch_bounds__(256, 4) k_gradient4(uint32_t N, const uint32_t *__restrict__ ord,
                                                       const uint32_t *__restrict__ inc_ptr,
                                                       const uint32_t *__restrict__ inc_oth,
-                                                      const uint32_t *__restrict__ inc_edge,
-                                                      const double4 *__restrict__ xyz,
-                                                      const double4 *__restrict__ coef,
-                                                      const double4 *__restrict__ q, double4 *__restrict__ gx,
-                                                      double4 *__restrict__ gy, double4 *__restrict__ gz)
+                                                      const double *__restrict__ inc_w, uint32_t ninc,
+                                                      const double *__restrict__ q, double *__restrict__ gx,
+                                                      double *__restrict__ gy, double *__restrict__ gz)
 {
-  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t p = gid >> 2, r = gid & 3;
   if (p >= N) return;
-  const uint32_t n = ord[p];
-  const double4 qn = q[n], xn = xyz[n], ca = coef[2 * (size_t)n], cb = coef[2 * (size_t)n + 1];
-  double4 ax = make_double4(0, 0, 0, 0), ay = ax, az = ax;
+  const uint32_t n = ord ? ord[p] : p;
+  const double qn = q[4 * (size_t)n + r];
+  double ax = 0.0, ay = 0.0, az = 0.0;
   const uint32_t k1 = inc_ptr[p + 1];
   for (uint32_t k = inc_ptr[p]; k < k1; k++) {
-    const uint32_t o = inc_oth[k];
-    const bool n0side = ROLE_BY_INDEX ? o > n : !(inc_edge[k] >> 31);
-    const double4 qo = q[o], xo = xyz[o];
-    const double dx = n0side ? xo.x - xn.x : xn.x - xo.x;
-    const double dy = n0side ? xo.y - xn.y : xn.y - xo.y;
-    const double dz = n0side ? xo.z - xn.z : xn.z - xo.z;
-    double wx, wy, wz;
-    lsq_term(n0side, dx, dy, dz, ca, cb, wx, wy, wz);
-    double dq;
-    dq = qo.x - qn.x; ax.x += wx * dq; ay.x += wy * dq; az.x += wz * dq;
-    dq = qo.y - qn.y; ax.y += wx * dq; ay.y += wy * dq; az.y += wz * dq;
-    dq = qo.z - qn.z; ax.z += wx * dq; ay.z += wy * dq; az.z += wz * dq;
-    dq = qo.w - qn.w; ax.w += wx * dq; ay.w += wy * dq; az.w += wz * dq;
+    const double dq = q[4 * (size_t)inc_oth[k] + r] - qn;
+    ax += inc_w[k] * dq;
+    ay += inc_w[ninc + k] * dq;
+    az += inc_w[2 * (size_t)ninc + k] * dq;
   }
-  gx[n] = ax;
-  gy[n] = ay;
-  gz[n] = az;
+  gx[4 * (size_t)n + r] = ax;
+  gy[4 * (size_t)n + r] = ay;
+  gz[4 * (size_t)n + r] = az;
+}
+
+// Node data in the visit order of the node-centric passes: dst[p] =
+// src[ord[p]] (gather) and back (scatter).  On large meshes the residual
+// passes work on visit-ordered copies of the state, coordinates and
+// gradients, so that a node's neighbours -- close to it in space, hence in
+// the Morton visit order -- are close to it in memory too.
+__global__ void __launch_bounds__(256) k_visit_gather(uint32_t N, const uint32_t *__restrict__ ord,
+                                                      const double4 *__restrict__ src, double4 *__restrict__ dst)
+{
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < N) dst[p] = src[ord[p]];
+}
+
+__global__ void __launch_bounds__(256) k_visit_scatter(uint32_t N, const uint32_t *__restrict__ ord,
+                                                       const double4 *__restrict__ src, double4 *__restrict__ dst)
+{
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < N) dst[ord[p]] = src[p];
 }
 
 // ------------------------------------------------------------------ residual
@@ -646,6 +657,87 @@ __global__ void __launch_bounds__(256) k_flux_nodes(uint32_t N, const uint32_t *
   for (uint32_t k = in1_ptr[p]; k < k1; k++) acc = sub4(acc, res[in1_edge[k]]);
   const uint32_t e1 = eoff[p + 1];
   for (uint32_t e = eoff[p]; e < e1; e++) acc = add4(acc, res[e]);
+  r[n] = acc;
+}
+
+// Fast-mode form of the two-pass residual with the n0 side summed in the
+// edge pass: a warp's 32 consecutive stored edges hold runs of equal n0 (the
+// storage is grouped by n0), so a segmented suffix sum over the warp (five
+// fixed shuffle steps) leaves each run's total in its first lane, which
+// writes it to seg[its storage position].  Every edge's flux still goes to
+// res for the n1 side.  The node pass then reads a node's n0 side as the
+// partial sums at the start of its group and at every warp boundary inside it
+// (one or two, instead of all of its edges' fluxes).  The sums are taken in
+// another order than the reference's, so exact mode keeps k_flux_edges.
+template <bool FIRST_ORDER>
+__global__ void __launch_bounds__(128) k_flux_edges_seg(uint32_t E, const uint32_t *__restrict__ n0,
+                                                        const uint32_t *__restrict__ n1,
+                                                        const double4 *__restrict__ egeo,
+                                                        const double4 *__restrict__ xyz,
+                                                        const double4 *__restrict__ q,
+                                                        const double4 *__restrict__ gx,
+                                                        const double4 *__restrict__ gy,
+                                                        const double4 *__restrict__ gz, double4 *__restrict__ res,
+                                                        double4 *__restrict__ seg)
+{
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  double4 f = make_double4(0, 0, 0, 0);
+  uint32_t a = 0xffffffffu;
+  if (e < E) {
+    a = n0[e];
+    const uint32_t o = n1[e];
+    const double4 geo = egeo[e];
+    const double4 qa = q[a], xa = xyz[a], qb = q[o], xb = xyz[o];
+    const double xm = 0.5 * (xa.x + xb.x), ym = 0.5 * (xa.y + xb.y), zm = 0.5 * (xa.z + xb.z);
+    double4 sL, sR;
+    if (FIRST_ORDER) {
+      const double4 z = make_double4(0, 0, 0, 0);
+      sL = recon(qa, z, z, z, xm - xa.x, ym - xa.y, zm - xa.z);
+      sR = recon(qb, z, z, z, xm - xb.x, ym - xb.y, zm - xb.z);
+    } else {
+      sL = recon(qa, gx[a], gy[a], gz[a], xm - xa.x, ym - xa.y, zm - xa.z);
+      sR = recon(qb, gx[o], gy[o], gz[o], xm - xb.x, ym - xb.y, zm - xb.z);
+    }
+    f = edge_flux(geo, sL, sR);
+    res[e] = f;
+  }
+  // segmented suffix sum over runs of equal n0 (runs are contiguous)
+  double4 acc = f;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t ao = __shfl_down_sync(0xffffffffu, a, off);
+    const double vx = __shfl_down_sync(0xffffffffu, acc.x, off), vy = __shfl_down_sync(0xffffffffu, acc.y, off);
+    const double vz = __shfl_down_sync(0xffffffffu, acc.z, off), vw = __shfl_down_sync(0xffffffffu, acc.w, off);
+    if (lane + off < 32 && ao == a) {
+      acc.x += vx;
+      acc.y += vy;
+      acc.z += vz;
+      acc.w += vw;
+    }
+  }
+  const uint32_t ap = __shfl_up_sync(0xffffffffu, a, 1);
+  if (e < E && (lane == 0 || ap != a)) seg[e] = acc;
+}
+
+__global__ void __launch_bounds__(256) k_flux_nodes_seg(uint32_t N, const uint32_t *__restrict__ ord,
+                                                        const uint32_t *__restrict__ in1_ptr,
+                                                        const uint32_t *__restrict__ in1_edge,
+                                                        const uint32_t *__restrict__ eoff,
+                                                        const double4 *__restrict__ res,
+                                                        const double4 *__restrict__ seg, double4 *__restrict__ r)
+{
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t n = ord[p];
+  double4 acc = make_double4(0, 0, 0, 0);
+  const uint32_t k1 = in1_ptr[p + 1];
+  for (uint32_t k = in1_ptr[p]; k < k1; k++) acc = sub4(acc, res[in1_edge[k]]);
+  const uint32_t e0 = eoff[p], e1 = eoff[p + 1];
+  if (e0 < e1) {
+    acc = add4(acc, seg[e0]);
+    for (uint32_t h = (e0 | 31u) + 1; h < e1; h += 32) acc = add4(acc, seg[h]);
+  }
   r[n] = acc;
 }
 
@@ -1422,68 +1514,10 @@ __global__ void __launch_bounds__(128) k_trsv_upper(uint32_t nrows, const uint32
   x[4 * (size_t)i + rr] = t;
 }
 
-// Level-synchronous sweep, one launch per level: 16 lanes per row
-// (lane = 4*block + component); every load of a row (its blocks, their
-// columns, and the already final x of those columns) is issued at once, then
-// the products are subtracted in column order exactly as in
-// matrix/sptrsv.cpp:173-209.  desc holds (row, first block, end block) in
-// level order; rows [s0, s1) are this level.
-template <typename T, bool UPPER>
-__global__ void __launch_bounds__(256) k_trsv_level16(uint32_t s0, uint32_t s1, const uint4 *__restrict__ desc,
-                                                      const uint32_t *__restrict__ ja, const T *__restrict__ A,
-                                                      const double *__restrict__ b, double *__restrict__ x)
-{
-  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t slot = s0 + (gid >> 4);
-  const int lane = threadIdx.x & 31, half = lane >> 4, l16 = lane & 15, jj = l16 >> 2, r = l16 & 3;
-  const unsigned hmask = 0xffffu << (16 * half);
-  if (slot >= s1) return;
-  const uint4 d = desc[slot];
-  const uint32_t i = d.x, jb = d.y, je = d.z;
-  double xi = UPPER ? x[4 * (size_t)i + r] : b[4 * (size_t)i + r];
-  for (uint32_t c0 = jb; c0 < je; c0 += 16) {
-    double t[4];
-#pragma unroll
-    for (int p = 0; p < 4; p++) {
-      const uint32_t j = c0 + 4 * p + jj;
-      t[p] = 0.0;
-      if (j < je) {
-        const uint32_t col = ja[j];
-        const T *blk = A + 16 * (size_t)j + 4 * r;
-        const double4 xc = reinterpret_cast<const double4 *>(x)[col];
-        double s = 0.0;
-        s += (double)blk[0] * xc.x;
-        s += (double)blk[1] * xc.y;
-        s += (double)blk[2] * xc.z;
-        s += (double)blk[3] * xc.w;
-        t[p] = s;
-      }
-    }
-    const uint32_t cnt = (je - c0) < 16u ? (je - c0) : 16u;
-#pragma unroll
-    for (int p = 0; p < 4; p++)
-      for (uint32_t q = 0; q < 4; q++) {
-        if (4 * p + q >= cnt) break;
-        xi = -1.0 * __shfl_sync(hmask, t[p], 16 * half + 4 * q + r) + xi;
-      }
-  }
-  if (UPPER) {
-    const int b4 = 16 * half;
-    const double x0 = __shfl_sync(hmask, xi, b4 + 0), x1 = __shfl_sync(hmask, xi, b4 + 1);
-    const double x2 = __shfl_sync(hmask, xi, b4 + 2), x3 = __shfl_sync(hmask, xi, b4 + 3);
-    const T *dg = A + 16 * (size_t)(jb - 1) + 4 * r;
-    double y = 0.0;
-    y += (double)dg[0] * x0;
-    y += (double)dg[1] * x1;
-    y += (double)dg[2] * x2;
-    y += (double)dg[3] * x3;
-    xi = y;
-  }
-  if (l16 < 4) x[4 * (size_t)i + r] = xi;
-}
-
-// One row of a triangular sweep (the body of k_trsv_level16) for a 16-lane
-// group.
+// One row of a triangular sweep for a 16-lane group (lane = 4*block +
+// component): every load of the row (its blocks, their columns, and the
+// already final x of those columns) is issued at once, then the products are
+// subtracted in column order exactly as in matrix/sptrsv.cpp:173-209.
 template <typename T, bool UPPER>
 __device__ __forceinline__ void trsv_row16(const uint4 d, const uint32_t *__restrict__ ja, const T *__restrict__ A,
                                            const double *__restrict__ b, double *x, int half, int jj, int r,
@@ -1535,7 +1569,7 @@ __device__ __forceinline__ void trsv_row16(const uint4 d, const uint32_t *__rest
 
 // One row of a triangular sweep for a group of G lanes (G = 8 or 16): lane
 // (jj, r) takes blocks c0 + (G/4) p + jj, row r of each; the partial products
-// are subtracted in column order, so the arithmetic is k_trsv_level16's.
+// are subtracted in column order, so the arithmetic is trsv_row16's.
 template <typename T, bool UPPER, int G>
 __device__ __forceinline__ void trsv_row_g(const uint4 d, const uint32_t *__restrict__ ja, const T *__restrict__ A,
                                            const double *__restrict__ b, double *x, int base, int gl,
@@ -1588,7 +1622,7 @@ __device__ __forceinline__ void trsv_row_g(const uint4 d, const uint32_t *__rest
 
 // Both sweeps in one cooperative launch: the rows of each level are spread
 // over every half-warp of the grid, and a grid barrier (kf_grid_barrier,
-// bounded) separates consecutive levels.  Arithmetic as in k_trsv_level16.
+// bounded) separates consecutive levels.  Arithmetic as in trsv_row16.
 template <typename T>
 __global__ void __launch_bounds__(256, 4) k_trsv_persistent(const uint32_t *__restrict__ lev_l, uint32_t nl,
                                                             const uint32_t *__restrict__ lev_u, uint32_t nu,
@@ -1648,7 +1682,7 @@ __device__ __forceinline__ bool kf_mono_barrier(unsigned *cnt, unsigned target, 
 }
 
 // Both sweeps in one cooperative launch of MINB 512-thread CTAs per SM;
-// levels separated by kf_mono_barrier.  Arithmetic as in k_trsv_level16.
+// levels separated by kf_mono_barrier.  Arithmetic as in trsv_row16.
 template <typename T, int MINB, int G>
 __global__ void __launch_bounds__(512, MINB) k_trsv_persistent_mono(const uint32_t *__restrict__ lev_l, uint32_t nl,
                                                                  const uint32_t *__restrict__ lev_u, uint32_t nu,
@@ -1684,7 +1718,7 @@ __global__ void __launch_bounds__(512, MINB) k_trsv_persistent_mono(const uint32
 // its row descriptor, the columns and the factor blocks (final since the
 // factorisation, which completed before this solve began) -- and only then
 // waits for the previous level's grid (griddepcontrol.wait) before reading x.
-// Arithmetic as in k_trsv_level16.  Rows with more than 16 blocks take a second
+// Arithmetic as in trsv_row16.  Rows with more than 16 blocks take a second
 // pass after the wait.
 template <typename T, bool UPPER>
 __global__ void __launch_bounds__(256) k_trsv_level_pdl(uint32_t s0, uint32_t s1, const uint4 *__restrict__ desc,
@@ -1768,7 +1802,7 @@ __global__ void __launch_bounds__(256) k_trsv_level_pdl(uint32_t s0, uint32_t s1
 // One launch per level with programmatic dependent launch, four lanes per
 // row: lane r keeps component r and subtracts the row's block products one
 // block at a time (each summed from zero, in block order: the arithmetic of
-// k_trsv_level16), so there is no reduction across lanes and a level needs a
+// trsv_row16), so there is no reduction across lanes and a level needs a
 // quarter of the threads of k_trsv_level_pdl.  Before waiting for the
 // previous level (griddepcontrol.wait) a row loads everything that does not
 // depend on x: its descriptor, the columns and rows of its first 8 blocks,
@@ -1879,7 +1913,7 @@ __device__ __forceinline__ void block_row(const double *a, double &a0, double &a
 }
 
 // One level of the packed schedule (matrix/sptrsv.cpp:173-209), one CTA per
-// chunk (up to 64 rows of the level, four lanes per row, lane r = component
+// chunk (up to ROWS rows of the level, four lanes per row, lane r = component
 // r).  Before the previous level has finished (griddepcontrol.wait) the CTA
 // stages its chunk of the packed factor -- one contiguous run -- into shared
 // memory with a single bulk copy, and loads the chunk's columns, rows and
@@ -1889,8 +1923,8 @@ __device__ __forceinline__ void block_row(const double *a, double &a0, double &a
 // The upper sweep then applies the inverted diagonal block (the first block
 // of the row's run).  The chunk's blocks in shared memory: 16 T each, then
 // their columns.
-template <typename T, bool UPPER>
-__global__ void __launch_bounds__(256, 4) k_trsv_packed(uint32_t c0, const uint4 *__restrict__ chunk,
+template <typename T, bool UPPER, int ROWS>
+__global__ void __launch_bounds__(4 * ROWS, 256 / ROWS) k_trsv_packed(uint32_t c0, const uint4 *__restrict__ chunk,
                                                         const uint32_t *__restrict__ prow,
                                                         const uint32_t *__restrict__ pfirst,
                                                         const uint32_t *__restrict__ pcol, const T *__restrict__ pk,
@@ -2085,450 +2119,6 @@ __global__ void __launch_bounds__(256, 4) k_trsv_syncfree(uint32_t N, const uint
   }
 }
 
-// The tiled sweep of the spatial ILU(0) order: both triangular sweeps in one
-// cooperative launch of one 512-thread CTA per tile (rows of a tile: a column
-// of the mesh along the sweep direction).  Warps 0-14 work the tile's steps
-// in order -- the rows of one level that it holds, G lanes per row and up to
-// P rows per group, arithmetic as in k_trsv_level16 -- separated by a
-// barrier of those warps only.  Warp 15 talks to the other tiles: it checks,
-// steps ahead, that the tiles a step reads from have reached the progress
-// computed on the host (acquire) and posts the last step cleared in shared
-// memory; and it follows the count of completed steps and stores the tile's
-// progress (release) when a step another tile waits for (bit 31 of pub) is
-// complete.  The compute warps thus see neither polls of other tiles nor
-// fences.  Everything that does not depend on x -- step records three steps
-// ahead, row descriptors two, columns, first blocks, diagonal blocks and
-// right-hand sides one -- is loaded before it is needed.  With every tile
-// resident and every requirement naming a strictly earlier level, the sweep
-// cannot deadlock.  Waits are bounded: one that runs out records an error in
-// *err and the tile stops; the others give up at their next look at *err.
-constexpr uint32_t KF_TILE_IDLE_LIMIT = 1u << 26;   // polls without news before a wait is declared failed
-
-__device__ __forceinline__ uint32_t ld_acquire_cta_shared(const uint32_t *p)
-{
-  uint32_t v;
-  asm volatile("ld.acquire.cta.shared.u32 %0, [%1];" : "=r"(v) : "r"((uint32_t)__cvta_generic_to_shared(p)) : "memory");
-  return v;
-}
-
-__device__ __forceinline__ void st_release_cta_shared(uint32_t *p, uint32_t v)
-{
-  asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"((uint32_t)__cvta_generic_to_shared(p)), "r"(v) : "memory");
-}
-
-__device__ __forceinline__ void prefetch_l1(const void *p)
-{
-  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-}
-
-template <typename T, int G, int P>
-__global__ void __launch_bounds__(512, 1) k_trsv_tiled(const uint32_t *__restrict__ tptr,
-                                                       const uint4 *__restrict__ steps,
-                                                       const uint32_t *__restrict__ pub,
-                                                       const uint2 *__restrict__ waits,
-                                                       const uint4 *__restrict__ tdesc,
-                                                       const uint32_t *__restrict__ ja, const T *__restrict__ A,
-                                                       const double *__restrict__ b, double *x, uint32_t *prog,
-                                                       int *err)
-{
-  constexpr int S = G / 4;
-  constexpr int NCW = 15;                       // compute warps
-  constexpr uint32_t NCT = NCW * 32;
-  __shared__ int fail_s;
-  __shared__ uint32_t done_s;                   // steps completed
-  __shared__ uint32_t ready_s;                  // steps whose requirements are met
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t t = blockIdx.x;
-  const uint32_t k0 = tptr[2 * t], k1 = tptr[2 * t + 1], k2 = tptr[2 * t + 2];
-  if (threadIdx.x == 0) { fail_s = 0; done_s = k0; ready_s = k0; }
-  __syncthreads();
-  if (warp == NCW) {
-    // the tile's link to the others
-    uint32_t published = k0, ready = k0, idle = 0;
-    while (published < k2) {
-      bool news = false;
-      const uint32_t done = __shfl_sync(0xffffffffu, ld_acquire_cta_shared(&done_s), 0);
-      if (done > published) {
-        if (lane == 0)
-          for (uint32_t kk = done; kk-- > published;) {
-            const uint32_t pv = pub[kk];
-            if (pv >> 31) { st_release(prog + t, pv & 0x7fffffffu); break; }
-          }
-        published = done;
-        news = true;
-      }
-      if (ready < k2 && ready < done + 3) {
-        const uint4 sr = steps[ready];
-        bool ok = true;
-        for (uint32_t w = sr.z + lane; w < sr.w; w += 32) {
-          const uint2 wt = waits[w];
-          if (ld_acquire(prog + wt.x) < wt.y) ok = false;
-        }
-        if (__all_sync(0xffffffffu, ok)) {
-          ready++;
-          if (lane == 0) st_release_cta_shared(&ready_s, ready);
-          news = true;
-        }
-      }
-      if (news) {
-        idle = 0;
-      } else if (++idle > KF_TILE_IDLE_LIMIT) {
-        if (lane == 0) { atomicExch(err, 1); fail_s = 1; }
-        break;
-      } else if ((idle & 255) == 0 && (*(volatile int *)&fail_s || *(volatile int *)err)) {
-        if (lane == 0) fail_s = 1;
-        break;
-      }
-    }
-    return;
-  }
-  const int gl = lane & (G - 1), base = lane - gl, jj = gl >> 2, r = gl & 3;
-  const unsigned gmask = ((1u << G) - 1u) << base;
-  const uint32_t R = NCT / G, h = threadIdx.x / G;
-  // into L1 ahead of use: the row descriptors of step k, and through them
-  // each row's columns, blocks (from the diagonal block on in the upper
-  // sweep) and right-hand side
-  auto prefetch_desc = [&](uint32_t k) {
-    if (k >= k2) return;
-    const uint4 rec = steps[k];
-    const char *p0 = reinterpret_cast<const char *>(tdesc + rec.x), *p1 = reinterpret_cast<const char *>(tdesc + rec.y);
-    for (const char *q = p0 + 128 * threadIdx.x; q < p1; q += 128 * NCT) prefetch_l1(q);
-    if (threadIdx.x == 0) prefetch_l1(steps + k + 8);
-  };
-  auto prefetch_rows = [&](uint32_t k) {
-    if (k >= k2) return;
-    const uint4 rec = steps[k];
-    const bool up = k >= k1;
-    for (uint32_t sl = rec.x + h; sl < rec.y; sl += R) {
-      const uint4 dd = tdesc[sl];
-      const uint32_t j0 = up ? dd.y - 1 : dd.y;
-      const char *p0 = reinterpret_cast<const char *>(A + 16 * (size_t)j0);
-      const char *p1 = reinterpret_cast<const char *>(A + 16 * (size_t)dd.z);
-      const char *q = p0 + 128 * gl;
-      if (q < p1) prefetch_l1(q);
-      if (gl == 0) prefetch_l1(ja + dd.y);
-      if (gl == 1 && !up) prefetch_l1(b + 4 * (size_t)dd.x);
-    }
-  };
-  prefetch_desc(k0);
-  prefetch_desc(k0 + 1);
-  prefetch_desc(k0 + 2);
-  prefetch_rows(k0);
-  prefetch_rows(k0 + 1);
-  for (uint32_t k = k0; k < k2; k++) {
-    if (threadIdx.x == 0) {
-      uint32_t spins = 0;
-      while (ld_acquire_cta_shared(&ready_s) <= k) {
-        if (*(volatile int *)&fail_s) break;
-        if (++spins > KF_TILE_IDLE_LIMIT) { atomicExch(err, 1); fail_s = 1; break; }
-      }
-    }
-    asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
-    if (*(volatile int *)&fail_s) return;
-    const uint4 cur = steps[k];
-    const bool upper = k >= k1;
-    // up to P rows per group: every load first, then the arithmetic of trsv_row_g
-    uint4 d[P];
-    uint32_t col[P][4];
-    T a[P][4][4], dg[P][4];
-    double xi[P];
-#pragma unroll
-    for (int q = 0; q < P; q++) {
-      const uint32_t sl = cur.x + h + R * q;
-      d[q] = make_uint4(0, 0, 0, 0);
-      if (sl < cur.y) { d[q] = tdesc[sl]; d[q].w = 1; }
-    }
-#pragma unroll
-    for (int q = 0; q < P; q++) {
-      xi[q] = 0.0;
-#pragma unroll
-      for (int p = 0; p < 4; p++) {
-        col[q][p] = 0xffffffffu;
-        const uint32_t j = d[q].y + S * p + jj;
-        if (d[q].w && j < d[q].z) {
-          col[q][p] = ja[j];
-          const T *blk = A + 16 * (size_t)j + 4 * r;
-#pragma unroll
-          for (int c = 0; c < 4; c++) a[q][p][c] = blk[c];
-        }
-      }
-      if (d[q].w) {
-        if (upper) {
-          const T *blk = A + 16 * (size_t)(d[q].y - 1) + 4 * r;
-#pragma unroll
-          for (int c = 0; c < 4; c++) dg[q][c] = blk[c];
-          xi[q] = __ldcg(x + 4 * (size_t)d[q].x + r);
-        } else {
-          xi[q] = b[4 * (size_t)d[q].x + r];
-        }
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < P; q++) {
-      if (!d[q].w) continue;
-      const uint32_t jb = d[q].y, je = d[q].z;
-      for (uint32_t c0 = jb; c0 < je; c0 += 4 * S) {
-        double tp[4];
-#pragma unroll
-        for (int p = 0; p < 4; p++) {
-          const uint32_t j = c0 + S * p + jj;
-          tp[p] = 0.0;
-          if (j < je) {
-            uint32_t cc = col[q][p];
-            double a0 = (double)a[q][p][0], a1 = (double)a[q][p][1], a2 = (double)a[q][p][2], a3 = (double)a[q][p][3];
-            if (c0 != jb) {
-              cc = ja[j];
-              const T *blk = A + 16 * (size_t)j + 4 * r;
-              a0 = (double)blk[0]; a1 = (double)blk[1]; a2 = (double)blk[2]; a3 = (double)blk[3];
-            }
-            const double2 x01 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)cc);
-            const double2 x23 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)cc + 1);
-            double sum = 0.0;
-            sum += a0 * x01.x;
-            sum += a1 * x01.y;
-            sum += a2 * x23.x;
-            sum += a3 * x23.y;
-            tp[p] = sum;
-          }
-        }
-        const uint32_t cnt = (je - c0) < (uint32_t)(4 * S) ? (je - c0) : (uint32_t)(4 * S);
-#pragma unroll
-        for (int p = 0; p < 4; p++)
-          for (int qq = 0; qq < S; qq++) {
-            if ((uint32_t)(S * p + qq) >= cnt) break;
-            xi[q] = -1.0 * __shfl_sync(gmask, tp[p], base + 4 * qq + r) + xi[q];
-          }
-      }
-      if (upper) {
-        const double x0 = __shfl_sync(gmask, xi[q], base + 0), x1 = __shfl_sync(gmask, xi[q], base + 1);
-        const double x2 = __shfl_sync(gmask, xi[q], base + 2), x3 = __shfl_sync(gmask, xi[q], base + 3);
-        double y = 0.0;
-        y += (double)dg[q][0] * x0;
-        y += (double)dg[q][1] * x1;
-        y += (double)dg[q][2] * x2;
-        y += (double)dg[q][3] * x3;
-        xi[q] = y;
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < P; q++)
-      if (d[q].w && gl < 4) __stcg(x + 4 * (size_t)d[q].x + r, xi[q]);
-    // rows beyond those
-    if (upper)
-      for (uint32_t s = cur.x + h + R * P; s < cur.y; s += R) trsv_row_g<T, true, G>(tdesc[s], ja, A, b, x, base, gl, gmask);
-    else
-      for (uint32_t s = cur.x + h + R * P; s < cur.y; s += R) trsv_row_g<T, false, G>(tdesc[s], ja, A, b, x, base, gl, gmask);
-    prefetch_desc(k + 3);
-    prefetch_rows(k + 2);
-    asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
-    if (threadIdx.x == 0) st_release_cta_shared(&done_s, k + 1);
-  }
-}
-
-// The FP32 factor rows of the tiled sweep packed in step order, one
-// KF_TILE_REC-byte record per row of tile_desc (a warp per record, 16 bytes
-// a lane): the row, its block count in the record (at most 8), first and end
-// block (uint32 x 4); the columns of its first 8 blocks (uint32 x 8); those
-// blocks (float x 16 each); and in the upper sweep the inverted diagonal
-// block (float x 16).  Rewritten after every FP32 factorisation.
-__global__ void k_tile_pack(uint32_t ndesc, const uint4 *__restrict__ tdesc, const uint32_t *__restrict__ ja,
-                            const float *__restrict__ Af, uint8_t *__restrict__ pack)
-{
-  const uint32_t slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (slot >= ndesc) return;
-  const uint4 d = tdesc[slot];
-  const uint32_t jb = d.y, je = d.z, nb = je - jb < 8 ? je - jb : 8;
-  uint4 *dst = reinterpret_cast<uint4 *>(pack + (size_t)slot * KF_TILE_REC);
-  for (uint32_t c = lane; c < KF_TILE_REC / 16; c += 32) {
-    uint4 v = make_uint4(0, 0, 0, 0);
-    if (c == 0) {
-      v = make_uint4(d.x, nb, jb, je);
-    } else if (c < 3) {
-      uint32_t w[4];
-      for (int e = 0; e < 4; e++) {
-        const uint32_t k = 4 * (c - 1) + e;
-        w[e] = k < nb ? ja[jb + k] : 0u;
-      }
-      v = make_uint4(w[0], w[1], w[2], w[3]);
-    } else if (c < 35) {
-      const uint32_t k = (c - 3) >> 2, quarter = (c - 3) & 3;
-      if (k < nb) v = *reinterpret_cast<const uint4 *>(Af + 16 * (size_t)(jb + k) + 4 * quarter);
-    } else if (d.w) {
-      v = *reinterpret_cast<const uint4 *>(Af + 16 * (size_t)(jb - 1) + 4 * (c - 35));
-    }
-    dst[c] = v;
-  }
-}
-
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
-{
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)), "l"(gmem)
-               : "memory");
-}
-
-// The tiled sweep on the packed FP32 factor: the schedule of k_trsv_tiled
-// (same steps, requirements and link warp), but every step's row records
-// arrive in shared memory by asynchronous copies issued two steps ahead (a
-// ring of three stages; issued after the step's own x reads), so a row
-// waits on nothing but its x reads.  Four lanes per row, lane r keeping
-// component r: each block's product is summed from zero and subtracted in
-// block order (the arithmetic of k_trsv_level16) with no reduction across
-// lanes.  Rows with more than 8 blocks take the rest from ja / Af.
-template <int G>
-__global__ void __launch_bounds__(512, 1) k_trsv_tiled_packed(const uint32_t *__restrict__ tptr,
-                                                              const uint4 *__restrict__ steps,
-                                                              const uint32_t *__restrict__ pub,
-                                                              const uint2 *__restrict__ waits,
-                                                              const uint8_t *__restrict__ pack,
-                                                              const uint32_t *__restrict__ ja,
-                                                              const float *__restrict__ Af,
-                                                              const double *__restrict__ b, double *x,
-                                                              uint32_t *prog, int *err)
-{
-  constexpr int S = G / 4;
-  constexpr int NCW = 15;
-  constexpr uint32_t NCT = NCW * 32;
-  constexpr uint32_t NST = 3, STAGE = KF_TILE_STEP_ROWS * KF_TILE_REC;
-  extern __shared__ __align__(16) uint8_t ring[];
-  __shared__ int fail_s;
-  __shared__ uint32_t done_s, ready_s;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t t = blockIdx.x;
-  const uint32_t k0 = tptr[2 * t], k1 = tptr[2 * t + 1], k2 = tptr[2 * t + 2];
-  if (threadIdx.x == 0) { fail_s = 0; done_s = k0; ready_s = k0; }
-  __syncthreads();
-  if (warp == NCW) {
-    uint32_t published = k0, ready = k0, idle = 0;
-    while (published < k2) {
-      bool news = false;
-      const uint32_t done = __shfl_sync(0xffffffffu, ld_acquire_cta_shared(&done_s), 0);
-      if (done > published) {
-        if (lane == 0)
-          for (uint32_t kk = done; kk-- > published;) {
-            const uint32_t pv = pub[kk];
-            if (pv >> 31) { st_release(prog + t, pv & 0x7fffffffu); break; }
-          }
-        published = done;
-        news = true;
-      }
-      if (ready < k2 && ready < done + 3) {
-        const uint4 sr = steps[ready];
-        bool ok = true;
-        for (uint32_t w = sr.z + lane; w < sr.w; w += 32) {
-          const uint2 wt = waits[w];
-          if (ld_acquire(prog + wt.x) < wt.y) ok = false;
-        }
-        if (__all_sync(0xffffffffu, ok)) {
-          ready++;
-          if (lane == 0) st_release_cta_shared(&ready_s, ready);
-          news = true;
-        }
-      }
-      if (news) {
-        idle = 0;
-      } else if (++idle > KF_TILE_IDLE_LIMIT) {
-        if (lane == 0) { atomicExch(err, 1); fail_s = 1; }
-        break;
-      } else if ((idle & 255) == 0 && (*(volatile int *)&fail_s || *(volatile int *)err)) {
-        if (lane == 0) fail_s = 1;
-        break;
-      }
-    }
-    return;
-  }
-  // four lanes per row, lane r = component r: each lane subtracts the row's
-  // block products one block at a time, so no reduction across lanes
-  const int r = lane & 3, base = lane & ~3;
-  const unsigned gmask = 0xfu << base;
-  const uint32_t R = NCT / 4, h = threadIdx.x >> 2;
-  static_assert(KF_TILE_STEP_ROWS <= NCT / 4, "one pass of rows per step");
-  auto issue = [&](uint32_t k) {
-    if (k < k2) {
-      const uint4 rec = steps[k];
-      const uint8_t *src = pack + (size_t)rec.x * KF_TILE_REC;
-      const uint32_t bytes = (rec.y - rec.x) * KF_TILE_REC;
-      uint8_t *dst = ring + (k % NST) * STAGE;
-      for (uint32_t off = threadIdx.x * 16; off < bytes; off += NCT * 16) cp_async16(dst + off, src + off);
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  };
-  issue(k0);
-  issue(k0 + 1);
-  uint4 cur = k0 < k2 ? steps[k0] : make_uint4(0, 0, 0, 0);
-  for (uint32_t k = k0; k < k2; k++) {
-    if (threadIdx.x == 0) {
-      uint32_t spins = 0;
-      while (ld_acquire_cta_shared(&ready_s) <= k) {
-        if (*(volatile int *)&fail_s) break;
-        if (++spins > KF_TILE_IDLE_LIMIT) { atomicExch(err, 1); fail_s = 1; break; }
-      }
-    }
-    asm volatile("cp.async.wait_group 1;" ::: "memory");
-    asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
-    if (*(volatile int *)&fail_s) {
-      asm volatile("cp.async.wait_all;" ::: "memory");
-      return;
-    }
-    const bool upper = k >= k1;
-    const uint8_t *stage = ring + (k % NST) * STAGE;
-    const uint32_t nrows = cur.y - cur.x;
-    uint32_t row_i = 0;
-    double xi = 0.0;
-    if (h < nrows) {
-      const uint8_t *rec = stage + h * KF_TILE_REC;
-      const uint4 hd = *reinterpret_cast<const uint4 *>(rec);
-      const uint32_t *cols = reinterpret_cast<const uint32_t *>(rec + 16);
-      const float *blks = reinterpret_cast<const float *>(rec + 48);
-      const uint32_t i = hd.x, nb = hd.y, jb = hd.z, je = hd.w;
-      row_i = i;
-      xi = upper ? __ldcg(x + 4 * (size_t)i + r) : b[4 * (size_t)i + r];
-#pragma unroll 4
-      for (uint32_t c = 0; c < nb; c++) {
-        const double2 x01 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)cols[c]);
-        const double2 x23 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)cols[c] + 1);
-        const float4 av = *reinterpret_cast<const float4 *>(blks + 16 * c + 4 * r);
-        double sum = 0.0;
-        sum += (double)av.x * x01.x;
-        sum += (double)av.y * x01.y;
-        sum += (double)av.z * x23.x;
-        sum += (double)av.w * x23.y;
-        xi = -1.0 * sum + xi;
-      }
-      for (uint32_t j = jb + nb; j < je; j++) {
-        const uint32_t cc = ja[j];
-        const double2 x01 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)cc);
-        const double2 x23 = __ldcg(reinterpret_cast<const double2 *>(x) + 2 * (size_t)cc + 1);
-        const float *blk = Af + 16 * (size_t)j + 4 * r;
-        double sum = 0.0;
-        sum += (double)blk[0] * x01.x;
-        sum += (double)blk[1] * x01.y;
-        sum += (double)blk[2] * x23.x;
-        sum += (double)blk[3] * x23.y;
-        xi = -1.0 * sum + xi;
-      }
-      if (upper) {
-        const float4 dv = *reinterpret_cast<const float4 *>(rec + 560 + 16 * r);
-        const double x0 = __shfl_sync(gmask, xi, base + 0), x1 = __shfl_sync(gmask, xi, base + 1);
-        const double x2 = __shfl_sync(gmask, xi, base + 2), x3 = __shfl_sync(gmask, xi, base + 3);
-        double y = 0.0;
-        y += (double)dv.x * x0;
-        y += (double)dv.y * x1;
-        y += (double)dv.z * x2;
-        y += (double)dv.w * x3;
-        xi = y;
-      }
-      __stcg(x + 4 * (size_t)i + r, xi);
-    }
-    (void)row_i;
-    // the copies two steps ahead go out after this step's x reads
-    issue(k + 2);
-    if (k + 1 < k2) cur = steps[k + 1];
-    asm volatile("bar.sync 1, %0;" ::"r"(NCT) : "memory");
-    if (threadIdx.x == 0) st_release_cta_shared(&done_s, k + 1);
-  }
-  asm volatile("cp.async.wait_all;" ::: "memory");
-}
-
 // ------------------------------------------------------------------ J.v
 
 // src/kernel.c:35-44: y = (y - r + cdt (w - q)) * a, a = |x| / h from the
@@ -2557,8 +2147,61 @@ __global__ void k_jv_combine(uint32_t N, double *__restrict__ y, const double *_
 
 inline unsigned blocks(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
+// The least-squares coefficients of every node on the device (k_lsq_coef),
+// and whether the terms recomputed from them equal the GEOMETRY's stored
+// terms bit for bit (k_lsq_check).
+int lsq_setup(DevMesh &m)
+{
+  if (!m.lsq_coef && cudaMalloc(&m.lsq_coef, 2 * (size_t)m.N * sizeof(double4)) != cudaSuccess) {
+    cudaGetLastError();
+    m.lsq_coef = nullptr;
+    return KFUN3D_ERR_CUDA;
+  }
+  unsigned *bad = reinterpret_cast<unsigned *>(m.status + 2);
+  if (cudaMemsetAsync(bad, 0, sizeof(unsigned), m.stream) != cudaSuccess) return KFUN3D_ERR_CUDA;
+  k_lsq_coef<<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.ord, m.inc_ptr, m.inc_oth, m.inc_edge,
+                                                     (const double4 *)m.xyz, m.lsq_coef);
+  k_lsq_check<<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.ord, m.inc_ptr, m.inc_oth, m.inc_edge, m.inc_w,
+                                                      m.wstride, (const double4 *)m.xyz, m.lsq_coef, bad);
+  kf_count_launch(2);
+  unsigned nbad = 1;
+  if (cudaMemcpyAsync(&nbad, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, m.stream) != cudaSuccess ||
+      cudaStreamSynchronize(m.stream) != cudaSuccess || cudaMemsetAsync(bad, 0, sizeof(unsigned), m.stream) != cudaSuccess)
+    return KFUN3D_ERR_CUDA;
+  m.lsq_match = nbad == 0;
+  return KFUN3D_OK;
+}
+
+// The state's visit-order copy (when the residual passes use one).
+static void visit_state(DevMesh &m, const double *q)
+{
+  if (!m.visit) return;
+  k_visit_gather<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, (const double4 *)q, m.qv);
+  kf_count_launch();
+}
+
+// Gradients of q (src/flux.c:60-145) into gx/gy/gz, or into their visit-order
+// copies (m.visit; the residual reads those).  Kernel (KFUN3D_GRADIENT):
+// four lanes per node (default on large meshes), one thread per node with
+// the incidence staged into shared memory by bulk copies (default in the
+// mesh's own order), "plain" one thread per node.
 void gradient(DevMesh &m, const double *q)
 {
+  if (m.visit) {
+    visit_state(m, q);
+    k_gradient4<<<blocks(4 * (size_t)m.N, 256), 256, 0, m.stream>>>(m.N, nullptr, m.inc_ptr, m.inc_othv, m.inc_w,
+                                                                     m.wstride, (const double *)m.qv,
+                                                                     (double *)m.gxv, (double *)m.gyv,
+                                                                     (double *)m.gzv);
+    kf_count_launch();
+    return;
+  }
+  if (m.grad_lanes == 4) {
+    k_gradient4<<<blocks(4 * (size_t)m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.inc_ptr, m.inc_oth, m.inc_w,
+                                                                     m.wstride, q, m.gx, m.gy, m.gz);
+    kf_count_launch();
+    return;
+  }
   if (m.grad_smem) {
     static bool attr_set = false;
     if (!attr_set) {
@@ -2576,20 +2219,54 @@ void gradient(DevMesh &m, const double *q)
   kf_count_launch();
 }
 
+// The gradients in the mesh's numbering (after gradient() wrote visit-order
+// copies), for callers that read them back.
+void gradient_to_mesh_order(DevMesh &m)
+{
+  if (!m.visit) return;
+  const unsigned nb = blocks(m.N, 256);
+  k_visit_scatter<<<nb, 256, 0, m.stream>>>(m.N, m.ord, m.gxv, (double4 *)m.gx);
+  k_visit_scatter<<<nb, 256, 0, m.stream>>>(m.N, m.ord, m.gyv, (double4 *)m.gy);
+  k_visit_scatter<<<nb, 256, 0, m.stream>>>(m.N, m.ord, m.gzv, (double4 *)m.gz);
+  kf_count_launch(3);
+}
+
+// Residual of q into r.  With visit-order copies (m.visit) the edge pass
+// reads the state, coordinates and gradients from them: the copy of q made
+// by gradient() for the second-order flux, made here for the first order.
 void residual(DevMesh &m, const double *q, double *r, int first_order, double u, double v)
 {
   if (m.two_pass) {
-    const double4 *G[3] = {(const double4 *)m.gx, (const double4 *)m.gy, (const double4 *)m.gz};
-    if (first_order)
-      k_flux_edges<true><<<blocks(m.E, 128), 128, 0, m.stream>>>(m.E, m.n0s, m.n1, m.egeo_s, m.xyz,
-                                                                  (const double4 *)q, nullptr, nullptr, nullptr,
-                                                                  m.eres);
-    else
-      k_flux_edges<false><<<blocks(m.E, 128), 128, 0, m.stream>>>(m.E, m.n0s, m.n1, m.egeo_s, m.xyz,
-                                                                   (const double4 *)q, G[0], G[1], G[2], m.eres);
-    k_flux_nodes<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.in1_ptr, m.in1_edge, m.eoff, m.eres,
-                                                         (double4 *)r);
-    kf_count_launch(2);
+    if (first_order) visit_state(m, q);
+    const double4 *G[3] = {m.visit ? m.gxv : (const double4 *)m.gx, m.visit ? m.gyv : (const double4 *)m.gy,
+                           m.visit ? m.gzv : (const double4 *)m.gz};
+    const double4 *Q = m.visit ? m.qv : (const double4 *)q;
+    const double4 *X = m.visit ? m.xyzv : m.xyz;
+    const uint32_t *E0 = m.visit ? m.n0v : m.n0s, *E1 = m.visit ? m.n1v : m.n1;
+#if KF_FAST
+    if (m.eseg) {
+      if (first_order)
+        k_flux_edges_seg<true><<<blocks(m.E, 128), 128, 0, m.stream>>>(m.E, E0, E1, m.egeo_s, X, Q, nullptr, nullptr,
+                                                                        nullptr, m.eres, m.eseg);
+      else
+        k_flux_edges_seg<false><<<blocks(m.E, 128), 128, 0, m.stream>>>(m.E, E0, E1, m.egeo_s, X, Q, G[0], G[1], G[2],
+                                                                         m.eres, m.eseg);
+      k_flux_nodes_seg<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.in1_ptr, m.in1_edge, m.eoff, m.eres,
+                                                               m.eseg, (double4 *)r);
+      kf_count_launch(2);
+    } else
+#endif
+    {
+      if (first_order)
+        k_flux_edges<true><<<blocks(m.E, 128), 128, 0, m.stream>>>(m.E, E0, E1, m.egeo_s, X, Q, nullptr, nullptr,
+                                                                    nullptr, m.eres);
+      else
+        k_flux_edges<false><<<blocks(m.E, 128), 128, 0, m.stream>>>(m.E, E0, E1, m.egeo_s, X, Q, G[0], G[1], G[2],
+                                                                     m.eres);
+      k_flux_nodes<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.in1_ptr, m.in1_edge, m.eoff, m.eres,
+                                                           (double4 *)r);
+      kf_count_launch(2);
+    }
   } else if (first_order)
     k_residual<true><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.ord, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo, m.xyz,
                                                             (const double4 *)q, nullptr, nullptr, nullptr,
@@ -2674,12 +2351,7 @@ void ilu(DevMesh &m, int precision)
   else
     k_ilu_finish_f32<<<blocks((size_t)m.N * 16, 256), 256, 0, m.stream>>>(m.N, m.diag, m.dinvf, m.Af);
   kf_count_launch();
-  if (precision == 1 && m.tile_pack) {
-    k_tile_pack<<<blocks((size_t)m.tile_ndesc * 32, 256), 256, 0, m.stream>>>(m.tile_ndesc, m.tile_desc, m.ja, m.Af,
-                                                                            m.tile_pack);
-    kf_count_launch();
-  }
-  if (m.trsv_mode == 8 && m.pk[0].chunk) {
+  if (m.trsv_mode == 8 && m.pk[0].chunk[0] && (precision == 1 || m.pk_fp64)) {
     packed_setup();
     for (int pass = 0; pass < 2; pass++) {
       const uint32_t nb = m.pk[pass].nblk, off = pass == 0 ? 0u : m.pk[0].nblk;
@@ -2701,43 +2373,50 @@ template <typename T> static size_t packed_smem(uint32_t blocks)
 }
 
 // The kernels' shared-memory limit, raised once to the largest chunk the
-// schedule allows (before any stream capture: ilu() calls it).
+// schedule allows (a single row of KF_PK_ROW_MAX blocks).
 static void packed_setup()
 {
   static bool done = false;
   if (done) return;
-  const int f32 = (int)packed_smem<float>(KF_PK_BLOCKS), f64 = (int)packed_smem<double>(KF_PK_BLOCKS);
-  cudaFuncSetAttribute((const void *)k_trsv_packed<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f32);
-  cudaFuncSetAttribute((const void *)k_trsv_packed<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f32);
-  cudaFuncSetAttribute((const void *)k_trsv_packed<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f64);
-  cudaFuncSetAttribute((const void *)k_trsv_packed<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f64);
+  const int f32 = (int)packed_smem<float>(KF_PK_ROW_MAX), f64 = (int)packed_smem<double>(KF_PK_ROW_MAX);
+  const void *fns32[] = {(const void *)k_trsv_packed<float, false, 32>, (const void *)k_trsv_packed<float, true, 32>,
+                         (const void *)k_trsv_packed<float, false, 64>, (const void *)k_trsv_packed<float, true, 64>};
+  const void *fns64[] = {(const void *)k_trsv_packed<double, false, 32>, (const void *)k_trsv_packed<double, true, 32>,
+                         (const void *)k_trsv_packed<double, false, 64>, (const void *)k_trsv_packed<double, true, 64>};
+  for (const void *f : fns32) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, f32);
+  for (const void *f : fns64) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, f64);
   done = true;
 }
 
 // Both sweeps of the packed schedule: one launch per level, chained by
 // programmatic dependent launch (the first level of the lower sweep waits for
-// the right-hand side normally).
+// the right-hand side normally).  The chunk cut (32 or 64 rows a CTA) is the
+// one chosen for the factor's precision.
 template <typename T> static void sptrsv_packed(DevMesh &m, const double *b, double *x)
 {
   packed_setup();
   int *err = m.status + 1;
   const T *base = reinterpret_cast<const T *>(m.pk_buf);
+  const int cut = m.pk_cut[sizeof(T) == 8 ? 0 : 1];
   for (int pass = 0; pass < 2; pass++) {
     const PackedSweep &pk = m.pk[pass];
     const T *P = pass == 0 ? base : base + 16 * (size_t)m.pk[0].nblk;
-    const void *fn = pass == 0 ? (const void *)k_trsv_packed<T, false> : (const void *)k_trsv_packed<T, true>;
-    const size_t smem = packed_smem<T>(pk.maxblk);
-    for (size_t l = 0; l + 1 < pk.lev.size(); l++) {
-      uint32_t c0 = pk.lev[l];
-      const uint32_t nc = pk.lev[l + 1] - c0;
+    const void *fn = cut == 0 ? (pass == 0 ? (const void *)k_trsv_packed<T, false, 32> : (const void *)k_trsv_packed<T, true, 32>)
+                              : (pass == 0 ? (const void *)k_trsv_packed<T, false, 64> : (const void *)k_trsv_packed<T, true, 64>);
+    const size_t smem = packed_smem<T>(pk.maxblk[cut]);
+    const uint4 *chunk = pk.chunk[cut];
+    const std::vector<uint32_t> &lev = pk.lev[cut];
+    for (size_t l = 0; l + 1 < lev.size(); l++) {
+      uint32_t c0 = lev[l];
+      const uint32_t nc = lev[l + 1] - c0;
       if (nc == 0) continue;
       const double *bb = b;
       double *xx = x;
-      void *args[] = {&c0, (void *)&pk.chunk, (void *)&pk.row, (void *)&pk.first, (void *)&pk.col, (void *)&P,
+      void *args[] = {&c0, (void *)&chunk, (void *)&pk.row, (void *)&pk.first, (void *)&pk.col, (void *)&P,
                       (void *)&bb, (void *)&xx, (void *)&err};
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3(nc);
-      cfg.blockDim = dim3(256);
+      cfg.blockDim = dim3(cut == 0 ? 128 : 256);
       cfg.dynamicSmemBytes = smem;
       cfg.stream = m.stream;
       cudaLaunchAttribute attr[1];
@@ -2754,72 +2433,16 @@ template <typename T> static void sptrsv_packed(DevMesh &m, const double *b, dou
 
 void sptrsv(DevMesh &m, const double *b, double *x, int precision)
 {
-  if (m.trsv_mode == 8 && m.pk[0].chunk) {
+  // the packed schedule serves FP32 factors; FP64 factors take the four-lane
+  // level launches unless m.pk_fp64 (measured faster at 120^3 in both orders)
+  const int mode = (m.trsv_mode == 8 && precision == 0 && !m.pk_fp64) ? 7 : m.trsv_mode;
+  if (mode == 8 && m.pk[0].chunk[0]) {
     if (precision == 0) sptrsv_packed<double>(m, b, x);
     else sptrsv_packed<float>(m, b, x);
     return;
   }
-  if (m.trsv_mode == 6 && m.ntiles && precision == 1 && m.tile_pack) {
-    cudaMemsetAsync(m.tile_prog, 0, m.ntiles * sizeof(unsigned), m.stream);
-    const double *bb = b;
-    int *err = m.status + 1;
-    void *args[] = {(void *)&m.tile_ptr, (void *)&m.tile_step, (void *)&m.tile_pub, (void *)&m.tile_wait,
-                    (void *)&m.tile_pack, (void *)&m.ja, (void *)&m.Af, (void *)&bb, (void *)&x,
-                    (void *)&m.tile_prog, (void *)&err};
-    const void *fn = (const void *)k_trsv_tiled_packed<8>;
-    const size_t smem = 3 * (size_t)KF_TILE_STEP_ROWS * KF_TILE_REC;
-    static bool attr_set = false;
-    if (!attr_set) {
-      cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      attr_set = true;
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(m.ntiles);
-    cfg.blockDim = dim3(512);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = m.stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
-    if (e != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e));
-    kf_count_launch();
-    return;
-  }
-  if (m.trsv_mode == 6 && m.ntiles) {
-    cudaMemsetAsync(m.tile_prog, 0, m.ntiles * sizeof(unsigned), m.stream);
-    const double *bb = b;
-    int *err = m.status + 1;
-    const void *Ap = precision == 0 ? (const void *)m.A : (const void *)m.Af;
-    void *args[] = {(void *)&m.tile_ptr, (void *)&m.tile_step, (void *)&m.tile_pub, (void *)&m.tile_wait,
-                    (void *)&m.tile_desc, (void *)&m.ja, (void *)&Ap, (void *)&bb, (void *)&x,
-                    (void *)&m.tile_prog, (void *)&err};
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(m.ntiles);
-    cfg.blockDim = dim3(512);
-    cfg.stream = m.stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeCooperative;
-    attr[0].val.cooperative = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    const void *fn = precision == 0 ? (const void *)k_trsv_tiled<double, 8, 1> : (const void *)k_trsv_tiled<float, 8, 2>;
-    static bool carveout = false;   // no shared memory to speak of: all of it as L1 for the prefetched rows
-    if (!carveout) {
-      cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-      const void *other = precision == 0 ? (const void *)k_trsv_tiled<float, 8, 2> : (const void *)k_trsv_tiled<double, 8, 1>;
-      cudaFuncSetAttribute(other, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-      carveout = true;
-    }
-    const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
-    if (e != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e));
-    kf_count_launch();
-    return;
-  }
-  if (m.trsv_mode == 4 || m.trsv_mode == 7) {
-    const bool four = m.trsv_mode == 7;   // four lanes per row (k_trsv_level_pdl4), else sixteen
+  if (mode == 4 || mode == 7) {
+    const bool four = mode == 7;   // four lanes per row (k_trsv_level_pdl4), else sixteen
     for (int pass = 0; pass < 2; pass++) {
       const std::vector<uint32_t> &ptr = pass == 0 ? m.lev_l_ptr : m.lev_u_ptr;
       const uint4 *desc = pass == 0 ? m.desc_l : m.desc_u;
@@ -2916,25 +2539,6 @@ void sptrsv(DevMesh &m, const double *b, double *x, int precision)
     const cudaError_t e = cudaLaunchKernelExC(&cfg, fn, args);
     if (e != cudaSuccess) kf_set_error(KFUN3D_ERR_CUDA, cudaGetErrorString(e));
     kf_count_launch();
-    return;
-  }
-  if (m.trsv_mode == 2) {
-    for (int pass = 0; pass < 2; pass++) {
-      const std::vector<uint32_t> &ptr = pass == 0 ? m.lev_l_ptr : m.lev_u_ptr;
-      const uint4 *desc = pass == 0 ? m.desc_l : m.desc_u;
-      for (size_t l = 0; l + 1 < ptr.size(); l++) {
-        const uint32_t s0 = ptr[l], s1 = ptr[l + 1];
-        const unsigned nb = blocks((size_t)(s1 - s0) * 16, 256);
-        if (precision == 0) {
-          if (pass == 0) k_trsv_level16<double, false><<<nb, 256, 0, m.stream>>>(s0, s1, desc, m.ja, m.A, b, x);
-          else k_trsv_level16<double, true><<<nb, 256, 0, m.stream>>>(s0, s1, desc, m.ja, m.A, b, x);
-        } else {
-          if (pass == 0) k_trsv_level16<float, false><<<nb, 256, 0, m.stream>>>(s0, s1, desc, m.ja, m.Af, b, x);
-          else k_trsv_level16<float, true><<<nb, 256, 0, m.stream>>>(s0, s1, desc, m.ja, m.Af, b, x);
-        }
-        kf_count_launch();
-      }
-    }
     return;
   }
   if (m.syncfree) {

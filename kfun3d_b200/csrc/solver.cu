@@ -209,6 +209,146 @@ __global__ void __launch_bounds__(256, 3) k_mgs_coop(size_t n, double *__restric
   }
 }
 
+// The same modified Gram-Schmidt with the vector being orthogonalised, w,
+// resident on chip for the whole launch: each thread keeps its first
+// KF_MGS_REG double2 elements of w in registers and the next `ts` in shared
+// memory (the rest, on meshes too large for that, stays in global memory).
+// A sweep then reads only the previous basis vector (just read by the sweep
+// before, so mostly an L2 hit) and the current one from memory, instead of
+// reading and writing w as well.  One CTA of 512 threads per SM; element i of
+// thread g (grid-wide) is g + t * stride for t = 0, 1, ...  The arithmetic is
+// k_mgs_coop's: per thread the same fma chain in the same element order,
+// block sums and the fixed-order grid total unchanged in form.
+constexpr int KF_MGS_REG = 16;    // double2 elements per thread in registers
+constexpr int KF_MGS_BATCH = 4;   // elements whose loads are in flight together
+
+__global__ void __launch_bounds__(512, 1) k_mgs_resident(size_t n, double *__restrict__ V, int k,
+                                                         double *__restrict__ h, double *__restrict__ part,
+                                                         unsigned *bar, int *err, int ts)
+{
+  extern __shared__ double2 wsm[];   // [ts][blockDim.x]
+  __shared__ double sm[40];
+  const int G = gridDim.x;
+  const size_t n2 = n / 2;
+  double2 *w = reinterpret_cast<double2 *>(V + (size_t)(k + 1) * n);
+  const size_t stride = (size_t)G * blockDim.x;
+  const size_t i0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t tcache = (size_t)KF_MGS_REG + (size_t)ts;   // elements t below this are on chip
+  double2 wr[KF_MGS_REG];
+#pragma unroll
+  for (int t = 0; t < KF_MGS_REG; t++) {
+    const size_t i = i0 + (size_t)t * stride;
+    wr[t] = i < n2 ? w[i] : make_double2(0.0, 0.0);
+  }
+  for (int t = 0; t < ts; t++) {
+    const size_t i = i0 + (size_t)(KF_MGS_REG + t) * stride;
+    wsm[(size_t)t * blockDim.x + threadIdx.x] = i < n2 ? w[i] : make_double2(0.0, 0.0);
+  }
+  double hprev = 0.0;
+  for (int v = 0; v <= k + 1; v++) {
+    const double2 *prev = v > 0 ? reinterpret_cast<const double2 *>(V + (size_t)(v - 1) * n) : nullptr;
+    const double2 *cur = v <= k ? reinterpret_cast<const double2 *>(V + (size_t)v * n) : nullptr;
+    double s = 0.0;
+    // elements in batches of KF_MGS_BATCH: all their loads are issued before
+    // any is used, so a thread keeps that many pairs of loads in flight
+    double2 pv[KF_MGS_BATCH], cv[KF_MGS_BATCH];
+    auto load = [&](int u, size_t i) {
+      if (prev) pv[u] = prev[i];
+      if (cur) cv[u] = cur[i];
+    };
+    auto step = [&](double2 &a, int u) {
+      if (prev) {
+        a.x = fma(-hprev, pv[u].x, a.x);
+        a.y = fma(-hprev, pv[u].y, a.y);
+      }
+      if (cur) {
+        s = fma(a.x, cv[u].x, s);
+        s = fma(a.y, cv[u].y, s);
+      } else {
+        s = fma(a.x, a.x, s);
+        s = fma(a.y, a.y, s);
+      }
+    };
+#pragma unroll
+    for (int t0 = 0; t0 < KF_MGS_REG; t0 += KF_MGS_BATCH) {
+#pragma unroll
+      for (int u = 0; u < KF_MGS_BATCH; u++) {
+        const size_t i = i0 + (size_t)(t0 + u) * stride;
+        if (i < n2) load(u, i);
+      }
+#pragma unroll
+      for (int u = 0; u < KF_MGS_BATCH; u++) {
+        const size_t i = i0 + (size_t)(t0 + u) * stride;
+        if (i < n2) step(wr[t0 + u], u);
+      }
+    }
+    for (int t0 = 0; t0 < ts; t0 += KF_MGS_BATCH) {
+#pragma unroll
+      for (int u = 0; u < KF_MGS_BATCH; u++) {
+        const size_t i = i0 + (size_t)(KF_MGS_REG + t0 + u) * stride;
+        if (t0 + u < ts && i < n2) load(u, i);
+      }
+#pragma unroll
+      for (int u = 0; u < KF_MGS_BATCH; u++) {
+        const size_t i = i0 + (size_t)(KF_MGS_REG + t0 + u) * stride;
+        if (t0 + u < ts && i < n2) {
+          double2 a = wsm[(size_t)(t0 + u) * blockDim.x + threadIdx.x];
+          step(a, u);
+          wsm[(size_t)(t0 + u) * blockDim.x + threadIdx.x] = a;
+        }
+      }
+    }
+    for (size_t i0g = i0 + tcache * stride; i0g < n2; i0g += KF_MGS_BATCH * stride) {
+#pragma unroll
+      for (int u = 0; u < KF_MGS_BATCH; u++) {
+        const size_t i = i0g + (size_t)u * stride;
+        if (i < n2) load(u, i);
+      }
+#pragma unroll
+      for (int u = 0; u < KF_MGS_BATCH; u++) {
+        const size_t i = i0g + (size_t)u * stride;
+        if (i < n2) {
+          double2 a = w[i];
+          step(a, u);
+          if (prev) w[i] = a;
+        }
+      }
+    }
+    double *pb = part + (v & 1) * G;
+    const double bs = block_sum(s, sm);
+    if (threadIdx.x == 0) pb[blockIdx.x] = bs;
+    __threadfence();
+    if (!kf_grid_barrier(bar, err)) return;
+    const double tot = grid_total(pb, G, sm);
+    if (v <= k) {
+      hprev = tot;
+      if (blockIdx.x == 0 && threadIdx.x == 0) h[v] = tot;
+    } else {
+      const double nrm = sqrt(tot);
+      if (blockIdx.x == 0 && threadIdx.x == 0) h[k + 1] = nrm;
+      const double sc = 1.0 / nrm;
+#pragma unroll
+      for (int t = 0; t < KF_MGS_REG; t++) {
+        const size_t i = i0 + (size_t)t * stride;
+        if (i < n2) w[i] = make_double2(wr[t].x * sc, wr[t].y * sc);
+      }
+      for (int t = 0; t < ts; t++) {
+        const size_t i = i0 + (size_t)(KF_MGS_REG + t) * stride;
+        if (i < n2) {
+          const double2 a = wsm[(size_t)t * blockDim.x + threadIdx.x];
+          w[i] = make_double2(a.x * sc, a.y * sc);
+        }
+      }
+      for (size_t i = i0 + tcache * stride; i < n2; i += stride) {
+        double2 a = w[i];
+        a.x *= sc;
+        a.y *= sc;
+        w[i] = a;
+      }
+    }
+  }
+}
+
 // y = (mult * coef[0]) * x + y with the coefficient on the device
 __global__ void k_axpy_dev(size_t n, const double *__restrict__ coef, double mult, const double *__restrict__ x,
                            double *__restrict__ y, int fast)
@@ -458,13 +598,28 @@ void dev_normalize(DevMesh &m, double *x, double *nrm, bool fast)
   kf_count_launch();
 }
 
+// Gram-Schmidt kernel: k_mgs_resident (default, w kept on chip) or
+// k_mgs_coop (KFUN3D_MGS=coop); grid and shared memory fixed per mesh.
 void mgs_coop_prepare(DevMesh &m)
 {
   if (!m.mgs_grid) {
-    int nsm = 0, per = 0;
+    int nsm = 0, per = 0, smax = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m.device));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mgs_coop, 256, 0));
-    m.mgs_grid = (unsigned)nsm * (unsigned)std::min(std::max(per, 1), 3);
+    const char *env = getenv("KFUN3D_MGS");
+    m.mgs_resident = !(env && strcmp(env, "coop") == 0);
+    if (m.mgs_resident) {
+      CK(cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, m.device));
+      const size_t n2 = 2 * (size_t)m.N, stride = (size_t)nsm * 512;
+      const size_t per_thread = (n2 + stride - 1) / stride;
+      const size_t room = (size_t)std::max(smax - 1024, 0) / (512 * sizeof(double2));
+      m.mgs_ts = (int)std::min(room, per_thread > (size_t)KF_MGS_REG ? per_thread - KF_MGS_REG : (size_t)0);
+      CK(cudaFuncSetAttribute((const void *)k_mgs_resident, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(m.mgs_ts * 512 * sizeof(double2))));
+      m.mgs_grid = (unsigned)nsm;
+    } else {
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mgs_coop, 256, 0));
+      m.mgs_grid = (unsigned)nsm * (unsigned)std::min(std::max(per, 1), 3);
+    }
     CK(cudaMalloc(&m.part, 2 * m.mgs_grid * sizeof(double)));
   }
 }
@@ -476,17 +631,19 @@ void mgs_coop(DevMesh &m, int k)
   double *V = m.V, *h = m.scal, *part = m.part;
   unsigned *bar = m.bar + 2;
   int *err = m.status + 1;
-  void *args[] = {&n, &V, &k, &h, &part, &bar, &err};
+  int ts = m.mgs_ts;
+  void *args[] = {&n, &V, &k, &h, &part, &bar, &err, &ts};
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(m.mgs_grid);
-  cfg.blockDim = dim3(256);
+  cfg.blockDim = dim3(m.mgs_resident ? 512 : 256);
+  cfg.dynamicSmemBytes = m.mgs_resident ? (size_t)m.mgs_ts * 512 * sizeof(double2) : 0;
   cfg.stream = m.stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  CK(cudaLaunchKernelExC(&cfg, (const void *)k_mgs_coop, args));
+  CK(cudaLaunchKernelExC(&cfg, m.mgs_resident ? (const void *)k_mgs_resident : (const void *)k_mgs_coop, args));
   kf_count_launch();
 }
 
@@ -1126,6 +1283,10 @@ extern "C" void ComputeFlux(const GEOMETRY *g, const double *q, GRADIENT *grad, 
     CK(cudaMemsetAsync(m->gz, 0, n * sizeof(double), m->stream));
   }
   dev_residual(*m, o, m->w, m->t);
+  if (!kf_first_order()) {
+    if (o.fast) kf_fast::gradient_to_mesh_order(*m);
+    else kf_exact::gradient_to_mesh_order(*m);
+  }
   d2h(*m, grad->x0, m->gx, n);
   d2h(*m, grad->x1, m->gy, n);
   d2h(*m, grad->x2, m->gz, n);

@@ -46,6 +46,10 @@ def test_exact_kernels_bit_identical(box_mesh):
     for path, aoa, seed in meshes(box_mesh):
         kf.set_aoa(aoa)
         m = kf.Mesh(path)
+        # the least-squares terms recomputed on the device from per-node
+        # coefficients made there equal the stored (reference) ones bit for bit
+        assert m.query("lsq_terms_match") == 1, path
+        assert m.query("sptrsv_schedule") == 8, path
         v = m.view
         q = seeded_state(v.q.copy(), seed)
         (g1, r1) = m.flux(q)
@@ -200,7 +204,7 @@ def test_blas_entry_points():
     assert np.array_equal(z, x * (1.0 / nrm))
 
 
-@pytest.mark.parametrize("schedule", ["packed", "levels", "syncfree", "levels16", "persistent", "pdl", "pdl4", "mono",
+@pytest.mark.parametrize("schedule", ["packed", "packed:32", "levels", "syncfree", "persistent", "pdl", "pdl4", "mono",
                                       "mono:8", "mono:4", "mono:16:1", "mono:8:3"])
 def test_exact_sptrsv_every_schedule(box_mesh, schedule, monkeypatch):
     """Every triangular-solve schedule (chosen when the device mirror is built;
@@ -208,7 +212,12 @@ def test_exact_sptrsv_every_schedule(box_mesh, schedule, monkeypatch):
     oracle's solve bit for bit in exact mode, FP64 and FP32."""
     parts = schedule.split(":")
     monkeypatch.setenv("KFUN3D_SPTRSV", parts[0])
-    if len(parts) > 1:
+    if parts[0] == "packed":
+        # chunks of 64 rows (256 threads) or 32 rows (128 threads) a CTA; FP64
+        # factors through the packed kernels too (by default they take pdl4)
+        monkeypatch.setenv("KFUN3D_PK_ROWS", f"{parts[1]},{parts[1]}" if len(parts) > 1 else "64,64")
+        monkeypatch.setenv("KFUN3D_PK_FP64", "1")
+    elif len(parts) > 1:
         monkeypatch.setenv("KFUN3D_SPTRSV_LANES", parts[1])
     if len(parts) > 2:
         monkeypatch.setenv("KFUN3D_SPTRSV_CTAS", parts[2])

@@ -303,24 +303,26 @@ def test_spatial_factor_is_the_renumbered_reference_factor(box_mesh, prec, perm,
 @pytest.mark.parametrize("perm", ["slabs", "tiles"])
 @pytest.mark.parametrize("n", [13, 30])
 def test_spatial_sweep_every_schedule(box_mesh, n, perm, monkeypatch):
-    """The packed level launches (default for the spatial order), one launch
-    per level with four lanes per row and with sixteen, the tiled sweep
-    (with 0, 2 and 7 steps of pipeline slack where the order allows it),
-    the persistent sweep, plain level launches and the sync-free sweep give
-    bit-identical triangular solves on the spatial factor (exact mode)."""
+    """The packed level launches (default for the spatial order; chunks of 64
+    and of 32 rows), one launch per level with four lanes per row and with
+    sixteen, the persistent sweep and the sync-free sweep give bit-identical
+    triangular solves on the spatial factor (exact mode)."""
     kf.set_mode("exact")
     if perm != "slabs":
         monkeypatch.setenv("KFUN3D_ILU_PERM", perm)
     path = box_mesh(n, seed=35)
     out = {}
-    for sched in ["packed", "pdl4", "pdl", "tiled", "tiled:0", "tiled:7", "mono", "levels16", "syncfree"]:
-        monkeypatch.delenv("KFUN3D_TILE_SLACK", raising=False)
+    monkeypatch.setenv("KFUN3D_PK_FP64", "1")   # FP64 factors through the packed kernels too
+    for sched in ["packed", "packed:32", "pdl4", "pdl", "mono", "syncfree"]:
+        monkeypatch.delenv("KFUN3D_PK_ROWS", raising=False)
         if sched == "packed":
             monkeypatch.delenv("KFUN3D_SPTRSV", raising=False)
         else:
             monkeypatch.setenv("KFUN3D_SPTRSV", sched.split(":")[0])
             if ":" in sched:
-                monkeypatch.setenv("KFUN3D_TILE_SLACK", sched.split(":")[1])
+                monkeypatch.setenv("KFUN3D_PK_ROWS", "32,32")
+            else:
+                monkeypatch.setenv("KFUN3D_PK_ROWS", "64,64")
         kf.set_ilu_order(0)
         m = kf.Mesh(path)
         q = seeded_state(m.view.q.copy(), 35)
