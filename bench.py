@@ -100,7 +100,10 @@ def alg_bytes(N, E, Fs, Ns, Nf, nnzb, prec, j=15):
     b["fill"] = (296 * E + 168 * N if not prec else 168 * E + 104 * N) + 28 * (Ns + Nf)
     b["ilu"] = nnzb * (32 * w + 4) + 8 * (N + 1)
     b["sptrsv"] = nnzb * (16 * w + 4) + 8 * (N + 1) + 96 * N
-    b["mgs"] = (5 * (j + 1) + 3) * 32 * N                             # j+1 dot/axpy pairs + normalise
+    # Gram-Schmidt at Arnoldi index j: the j+1 basis vectors read once, the new
+    # vector read and written once (the kernel keeps it on chip; classical MGS
+    # would move (5(j+1)+3)*32N re-reading and re-writing it per projection)
+    b["mgs"] = (j + 3) * 32 * N
     b["gmres_iter"] = b["flux"] + 296 * N + b["sptrsv"] + b["mgs"]
     return b
 

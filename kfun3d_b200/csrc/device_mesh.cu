@@ -384,7 +384,7 @@ static void release_device(MatrixHandle *h)
                   m->diag, m->tblk, m->lpos, m->last_lower, m->lev_l, m->lev_u, m->A, m->lslot, m->dinv,
                   m->Af, m->dinvf, m->q, m->r, m->gx, m->gy, m->gz, m->cdt, m->w, m->t, m->x, m->rhs, m->V,
                   m->red, m->scal, m->forces, m->dscr, m->status, m->flags, m->ticket, m->part, m->lsq_coef,
-                  m->qv, m->xyzv, m->gxv, m->gyv, m->gzv, m->inc_othv, m->n0v, m->n1v, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->eseg, m->n0s, m->pair_ptr, m->pairs, m->lev_ptr_d, m->bar, m->Z, m->qold, m->fy, m->fx, m->pscr, m->ord, m->rowof, m->egeo_s};
+                  m->qv, m->xyzv, m->gxv, m->gyv, m->gzv, m->inc_othv, m->n0v, m->n1v, m->inc_geo, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->n0s, m->pair_ptr, m->pairs, m->lev_ptr_d, m->bar, m->Z, m->qold, m->fy, m->fx, m->pscr, m->ord, m->rowof, m->egeo_s};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (m->h_scal) cudaFreeHost(m->h_scal);
@@ -614,9 +614,6 @@ DevMesh *kf_device(const GEOMETRY *g)
       KF_CUDA(upload(&m->in1_ptr, iptr.data(), N + 1));
       KF_CUDA(upload(&m->in1_edge, iedge.data(), E));
       KF_CUDA(cudaMalloc(&m->eres, std::max<size_t>(E, 1) * sizeof(double4)));
-      // fast mode sums each node's n0 side in the edge pass (KFUN3D_RESIDUAL_SEG=0: not)
-      const char *senv = getenv("KFUN3D_RESIDUAL_SEG");
-      if (!(senv && strcmp(senv, "0") == 0)) KF_CUDA(cudaMalloc(&m->eseg, std::max<size_t>(E, 1) * sizeof(double4)));
       // visit-order copies for the residual passes when the visit order is
       // not the mesh's own (KFUN3D_VISIT_COPIES=0: not): the edges' end
       // points and each incidence's other end as visit positions, the
@@ -631,9 +628,17 @@ DevMesh *kf_device(const GEOMETRY *g)
           const uint32_t nd = ord[p2];
           xv[p2] = make_double4(g->n->xyz->x0[nd], g->n->xyz->x1[nd], g->n->xyz->x2[nd], 0.0);
         }
-        std::vector<uint32_t> othm(2 * (size_t)E);
+        std::vector<uint32_t> othm(2 * (size_t)E), edgm(2 * (size_t)E);
         KF_CUDA(cudaMemcpy(othm.data(), m->inc_oth, 2 * (size_t)E * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-        for (size_t k = 0; k < 2 * (size_t)E; k++) othv[k] = rowv[othm[k]];
+        KF_CUDA(cudaMemcpy(edgm.data(), m->inc_edge, 2 * (size_t)E * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        std::vector<double4> ig(2 * (size_t)E);
+        const double *gx0 = g->e->xyzn->x0, *gx1 = g->e->xyzn->x1, *gx2 = g->e->xyzn->x2, *gx3 = g->e->xyzn->x3;
+        for (size_t k = 0; k < 2 * (size_t)E; k++) {
+          othv[k] = rowv[othm[k]];
+          const uint32_t e = edgm[k] & 0x7fffffffu;
+          ig[k] = make_double4(gx0[e], gx1[e], gx2[e], gx3[e]);
+        }
+        KF_CUDA(upload(&m->inc_geo, ig.data(), ig.size()));
         for (uint32_t e = 0; e < E; e++) { e0v[e] = rowv[n0s[e]]; e1v[e] = rowv[n1s[e]]; }
         KF_CUDA(upload(&m->inc_othv, othv.data(), othv.size()));
         KF_CUDA(upload(&m->n0v, e0v.data(), E));

@@ -58,6 +58,7 @@ void activate(DevMesh &m, const IluSet &s)
   m.fill_blk = s.fill_blk; m.fill_diag = s.fill_diag; m.fill_last = s.fill_last; m.fill_lpos = s.fill_lpos;
   m.pk[0] = s.pk[0];
   m.pk[1] = s.pk[1];
+  m.row_node = s.row_node;
 }
 
 // Tiles of the tile-major order (KFUN3D_ILU_PERM=tiles): columns along the
@@ -327,6 +328,9 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
     up(&s.fill_diag, fd);
     up(&s.fill_last, fl);
     up(&s.fill_lpos, fp);
+    std::vector<uint32_t> rn(N);   // node of each renumbered row
+    for (size_t i = 0; i < N; i++) rn[rank[i]] = (uint32_t)i;
+    up(&s.row_node, rn);
   }
   up(&m.ilu_rank, rank);
   if (ok && cudaMalloc(&m.pb, 4 * N * sizeof(double)) != cudaSuccess) ok = false;
@@ -381,7 +385,7 @@ void kf_ilu_release(DevMesh &m)
   }
   IluSet &s = m.iset[1];
   void *ptrs[] = {s.ia, s.ja, s.diag, s.tblk, s.lpos, s.last_lower, s.pair_ptr, s.pairs, s.lev_l, s.lev_u,
-                  s.lev_ptr_d, s.desc_l, s.desc_u, s.fill_blk, s.fill_diag, s.fill_last, s.fill_lpos,
+                  s.lev_ptr_d, s.desc_l, s.desc_u, s.fill_blk, s.fill_diag, s.fill_last, s.fill_lpos, s.row_node,
                   m.ilu_rank, m.pb, m.px};
   for (void *p : ptrs)
     if (p) cudaFree(p);

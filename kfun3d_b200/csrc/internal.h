@@ -139,6 +139,7 @@ struct IluSet {
   uint32_t *fill_diag = nullptr;   // [N] diagonal block of each node
   uint32_t *fill_last = nullptr;   // [N] the node's row's last-touched lower block (or ~0)
   uint32_t *fill_lpos = nullptr;   // [N] the node's row's first persistent L slot
+  uint32_t *row_node = nullptr;    // [N] node of each matrix row (null: the identity)
   PackedSweep pk[2];               // packed level schedule (trsv_mode 8)
 };
 
@@ -177,6 +178,7 @@ struct DevMesh {
   bool visit = false;
   double4 *qv = nullptr, *xyzv = nullptr, *gxv = nullptr, *gyv = nullptr, *gzv = nullptr;
   uint32_t *inc_othv = nullptr, *n0v = nullptr, *n1v = nullptr;
+  double4 *inc_geo = nullptr;     // [2E] edge geometry per incidence (CSR order), for the time step and fill
   // two-pass residual (every edge has n0 < n1); edge arrays in storage
   // order: grouped by n0 in node-visit order (ord), each group in edge order
   bool two_pass = false;
@@ -187,7 +189,6 @@ struct DevMesh {
   uint32_t *in1_ptr = nullptr;    // [N+1] edges with n1 = ord[p], in edge order
   uint32_t *in1_edge = nullptr;   // [E] their storage positions
   double4 *eres = nullptr;        // [E] edge fluxes, storage order
-  double4 *eseg = nullptr;        // [E] fast mode: n0-run sums of a warp's edges at the runs' first positions
   uint32_t *wf_nodes = nullptr;   // [3F] wall faces in colour order
   double *wf_n = nullptr;         // [3F] wall-face normals -(1/6) a x b
   uint32_t *col = nullptr;        // [ncol+1] wall-face colour offsets
@@ -260,6 +261,7 @@ struct DevMesh {
   double *pb = nullptr, *px = nullptr;   // [4N] right-hand side and solution, spatial numbering
   int graph_ilu = 0;              // ILU set the Arnoldi graphs were captured with
   uint32_t *fill_blk = nullptr, *fill_diag = nullptr, *fill_last = nullptr, *fill_lpos = nullptr;
+  uint32_t *row_node = nullptr;   // active set's node of each matrix row (null: the identity)
   // flexible GMRES (right preconditioning) and the learned preconditioner
   double *Z = nullptr;            // [30][4N] preconditioned basis vectors
   double *qold = nullptr;         // [4N] state before the last update

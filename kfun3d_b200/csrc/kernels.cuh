@@ -15,6 +15,7 @@
 // sector per gather); edge geometry is a double4 (unit normal, area) per edge;
 // each node's incident edges are a contiguous run of the incidence arrays.
 #include <cstdint>
+#include <type_traits>
 
 #include "internal.h"
 
@@ -660,85 +661,25 @@ __global__ void __launch_bounds__(256) k_flux_nodes(uint32_t N, const uint32_t *
   r[n] = acc;
 }
 
-// Fast-mode form of the two-pass residual with the n0 side summed in the
-// edge pass: a warp's 32 consecutive stored edges hold runs of equal n0 (the
-// storage is grouped by n0), so a segmented suffix sum over the warp (five
-// fixed shuffle steps) leaves each run's total in its first lane, which
-// writes it to seg[its storage position].  Every edge's flux still goes to
-// res for the n1 side.  The node pass then reads a node's n0 side as the
-// partial sums at the start of its group and at every warp boundary inside it
-// (one or two, instead of all of its edges' fluxes).  The sums are taken in
-// another order than the reference's, so exact mode keeps k_flux_edges.
-template <bool FIRST_ORDER>
-__global__ void __launch_bounds__(128) k_flux_edges_seg(uint32_t E, const uint32_t *__restrict__ n0,
-                                                        const uint32_t *__restrict__ n1,
-                                                        const double4 *__restrict__ egeo,
-                                                        const double4 *__restrict__ xyz,
-                                                        const double4 *__restrict__ q,
-                                                        const double4 *__restrict__ gx,
-                                                        const double4 *__restrict__ gy,
-                                                        const double4 *__restrict__ gz, double4 *__restrict__ res,
-                                                        double4 *__restrict__ seg)
+// k_flux_nodes with four lanes per node, lane r summing flux component r in
+// the same order (so the same result): a quad reads each edge flux as one
+// 32-byte sector, and four times as many nodes' gathers are in flight.
+__global__ void __launch_bounds__(256) k_flux_nodes4(uint32_t N, const uint32_t *__restrict__ ord,
+                                                     const uint32_t *__restrict__ in1_ptr,
+                                                     const uint32_t *__restrict__ in1_edge,
+                                                     const uint32_t *__restrict__ eoff,
+                                                     const double *__restrict__ res, double *__restrict__ r)
 {
-  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
-  double4 f = make_double4(0, 0, 0, 0);
-  uint32_t a = 0xffffffffu;
-  if (e < E) {
-    a = n0[e];
-    const uint32_t o = n1[e];
-    const double4 geo = egeo[e];
-    const double4 qa = q[a], xa = xyz[a], qb = q[o], xb = xyz[o];
-    const double xm = 0.5 * (xa.x + xb.x), ym = 0.5 * (xa.y + xb.y), zm = 0.5 * (xa.z + xb.z);
-    double4 sL, sR;
-    if (FIRST_ORDER) {
-      const double4 z = make_double4(0, 0, 0, 0);
-      sL = recon(qa, z, z, z, xm - xa.x, ym - xa.y, zm - xa.z);
-      sR = recon(qb, z, z, z, xm - xb.x, ym - xb.y, zm - xb.z);
-    } else {
-      sL = recon(qa, gx[a], gy[a], gz[a], xm - xa.x, ym - xa.y, zm - xa.z);
-      sR = recon(qb, gx[o], gy[o], gz[o], xm - xb.x, ym - xb.y, zm - xb.z);
-    }
-    f = edge_flux(geo, sL, sR);
-    res[e] = f;
-  }
-  // segmented suffix sum over runs of equal n0 (runs are contiguous)
-  double4 acc = f;
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const uint32_t ao = __shfl_down_sync(0xffffffffu, a, off);
-    const double vx = __shfl_down_sync(0xffffffffu, acc.x, off), vy = __shfl_down_sync(0xffffffffu, acc.y, off);
-    const double vz = __shfl_down_sync(0xffffffffu, acc.z, off), vw = __shfl_down_sync(0xffffffffu, acc.w, off);
-    if (lane + off < 32 && ao == a) {
-      acc.x += vx;
-      acc.y += vy;
-      acc.z += vz;
-      acc.w += vw;
-    }
-  }
-  const uint32_t ap = __shfl_up_sync(0xffffffffu, a, 1);
-  if (e < E && (lane == 0 || ap != a)) seg[e] = acc;
-}
-
-__global__ void __launch_bounds__(256) k_flux_nodes_seg(uint32_t N, const uint32_t *__restrict__ ord,
-                                                        const uint32_t *__restrict__ in1_ptr,
-                                                        const uint32_t *__restrict__ in1_edge,
-                                                        const uint32_t *__restrict__ eoff,
-                                                        const double4 *__restrict__ res,
-                                                        const double4 *__restrict__ seg, double4 *__restrict__ r)
-{
-  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t p = gid >> 2, c = gid & 3;
   if (p >= N) return;
   const uint32_t n = ord[p];
-  double4 acc = make_double4(0, 0, 0, 0);
+  double acc = 0.0;
   const uint32_t k1 = in1_ptr[p + 1];
-  for (uint32_t k = in1_ptr[p]; k < k1; k++) acc = sub4(acc, res[in1_edge[k]]);
-  const uint32_t e0 = eoff[p], e1 = eoff[p + 1];
-  if (e0 < e1) {
-    acc = add4(acc, seg[e0]);
-    for (uint32_t h = (e0 | 31u) + 1; h < e1; h += 32) acc = add4(acc, seg[h]);
-  }
-  r[n] = acc;
+  for (uint32_t k = in1_ptr[p]; k < k1; k++) acc = acc - res[4 * (size_t)in1_edge[k] + c];
+  const uint32_t e1 = eoff[p + 1];
+  for (uint32_t e = eoff[p]; e < e1; e++) acc = acc + res[4 * (size_t)e + c];
+  r[4 * (size_t)n + c] = acc;
 }
 
 // Boundary terms, after all edges: wall faces by colour (src/flux.c:467-539),
@@ -782,6 +723,10 @@ __global__ void k_residual_boundary(uint32_t nb, const uint32_t *__restrict__ bn
 
 // src/timestep.c:58-91 as a gather; nodes without boundary terms are divided
 // by the CFL number here, boundary nodes in k_timestep_boundary.
+// VISIT: q and the incidences' other ends in visit order (row p of the
+// incidence is node p of q), and the geometry per incidence (inc_geo[k])
+// instead of per edge.
+template <bool VISIT>
 __global__ void __launch_bounds__(256) k_timestep(uint32_t N, const uint32_t *__restrict__ ord,
                                                   const uint32_t *__restrict__ inc_ptr,
                                                   const uint32_t *__restrict__ inc_oth,
@@ -794,13 +739,13 @@ __global__ void __launch_bounds__(256) k_timestep(uint32_t N, const uint32_t *__
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= N) return;
   const uint32_t n = ord[p];
-  const double4 qs = q[n];
+  const double4 qs = q[VISIT ? p : n];
   double acc = 0.0;
   const uint32_t k1 = inc_ptr[p + 1];
   for (uint32_t k = inc_ptr[p]; k < k1; k++) {
     const uint32_t ev = inc_edge[k];
     const bool is_n1 = ev >> 31;
-    const double4 geo = egeo[ev & 0x7fffffffu];
+    const double4 geo = egeo[VISIT ? k : (ev & 0x7fffffffu)];
     const double4 qo = q[inc_oth[k]];
     const double4 qa = is_n1 ? qo : qs, qb = is_n1 ? qs : qo;
     const double xnorm = geo.x * geo.w, ynorm = geo.y * geo.w, znorm = geo.z * geo.w;
@@ -1006,8 +951,12 @@ template <> __device__ __forceinline__ void store_block<float>(float *dst, const
 // in edge order; the off-diagonal block of each edge, v1 in row n0 and -v0 in
 // row n1, is written once.  The row's first persistent L slot receives the
 // last lower block the reference's fill would touch (matrix/matrix.cpp:239).
-template <typename T>
-__global__ void __launch_bounds__(128) k_fill(uint32_t N, const uint32_t *__restrict__ rowof,
+// Threads run in the active pattern's row order (row_node maps a row to its
+// node; null: the identity, the mesh's own pattern), so consecutive threads
+// write consecutive rows in both ILU(0) orders.
+template <typename T, bool VISIT>
+__global__ void __launch_bounds__(128) k_fill(uint32_t N, const uint32_t *__restrict__ row_node,
+                                              const uint32_t *__restrict__ rowof,
                                               const uint32_t *__restrict__ inc_ptr,
                                               const uint32_t *__restrict__ inc_oth,
                                               const uint32_t *__restrict__ inc_edge,
@@ -1021,10 +970,11 @@ __global__ void __launch_bounds__(128) k_fill(uint32_t N, const uint32_t *__rest
                                               double *__restrict__ lslot,
                                               const uint32_t *__restrict__ bnd_of, double *__restrict__ dscr)
 {
-  const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
-  const uint32_t p = rowof[n];   // nodes in their own order: the matrix rows are written in sequence
-  const double4 qs = q[n];
+  const uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= N) return;
+  const uint32_t n = row_node ? row_node[row] : row;
+  const uint32_t p = rowof[n];
+  const double4 qs = q[VISIT ? p : n];
   double D[16];
 #pragma unroll
   for (int i = 0; i < 16; i++) D[i] = 0.0;
@@ -1035,7 +985,7 @@ __global__ void __launch_bounds__(128) k_fill(uint32_t N, const uint32_t *__rest
   for (uint32_t k = inc_ptr[p]; k < k1; k++) {
     const uint32_t ev = inc_edge[k];
     const bool is_n1 = ev >> 31;
-    const double4 geo = egeo[ev & 0x7fffffffu];
+    const double4 geo = egeo[VISIT ? k : (ev & 0x7fffffffu)];
     const double4 qo = q[inc_oth[k]];
     double v0[16], v1[16], off[16];
     edge_jacobians(geo, is_n1 ? qo : qs, is_n1 ? qs : qo, v0, v1);
@@ -1912,13 +1862,17 @@ __device__ __forceinline__ void block_row(const double *a, double &a0, double &a
   a0 = u.x; a1 = u.y; a2 = v.x; a3 = v.y;
 }
 
+#ifndef KF_PK_GATHER
+#define KF_PK_GATHER 4   // column states gathered at once per row (8 measured slower: fewer rows in flight)
+#endif
+
 // One level of the packed schedule (matrix/sptrsv.cpp:173-209), one CTA per
 // chunk (up to ROWS rows of the level, four lanes per row, lane r = component
 // r).  Before the previous level has finished (griddepcontrol.wait) the CTA
 // stages its chunk of the packed factor -- one contiguous run -- into shared
 // memory with a single bulk copy, and loads the chunk's columns, rows and
 // (lower sweep) right-hand side; after it, it gathers the final x of the
-// columns (four at a time) and subtracts the block products in column order,
+// columns (KF_PK_GATHER at a time) and subtracts the block products in column order,
 // each product summed from zero in component order as the reference does.
 // The upper sweep then applies the inverted diagonal block (the first block
 // of the row's run).  The chunk's blocks in shared memory: 16 T each, then
@@ -1964,10 +1918,10 @@ __global__ void __launch_bounds__(4 * ROWS, 256 / ROWS) k_trsv_packed(uint32_t c
     k = k0 + 1;
   }
   const double2 *x2 = reinterpret_cast<const double2 *>(x);
-  for (; k < k1; k += 4) {
-    double2 lo[4], hi[4];
+  for (; k < k1; k += KF_PK_GATHER) {
+    double2 lo[KF_PK_GATHER], hi[KF_PK_GATHER];
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
+    for (int c = 0; c < KF_PK_GATHER; c++) {
       if (k + c < k1) {
         const size_t col = sc[k + c];
         lo[c] = __ldcg(x2 + 2 * col);
@@ -1975,7 +1929,7 @@ __global__ void __launch_bounds__(4 * ROWS, 256 / ROWS) k_trsv_packed(uint32_t c
       }
     }
 #pragma unroll
-    for (int c = 0; c < 4; c++) {
+    for (int c = 0; c < KF_PK_GATHER; c++) {
       if (k + c < k1) {
         double a0, a1, a2, a3;
         block_row(sa + 16 * (size_t)(k + c) + 4 * r, a0, a1, a2, a3);
@@ -2243,19 +2197,6 @@ void residual(DevMesh &m, const double *q, double *r, int first_order, double u,
     const double4 *Q = m.visit ? m.qv : (const double4 *)q;
     const double4 *X = m.visit ? m.xyzv : m.xyz;
     const uint32_t *E0 = m.visit ? m.n0v : m.n0s, *E1 = m.visit ? m.n1v : m.n1;
-#if KF_FAST
-    if (m.eseg) {
-      if (first_order)
-        k_flux_edges_seg<true><<<blocks(m.E, 128), 128, 0, m.stream>>>(m.E, E0, E1, m.egeo_s, X, Q, nullptr, nullptr,
-                                                                        nullptr, m.eres, m.eseg);
-      else
-        k_flux_edges_seg<false><<<blocks(m.E, 128), 128, 0, m.stream>>>(m.E, E0, E1, m.egeo_s, X, Q, G[0], G[1], G[2],
-                                                                         m.eres, m.eseg);
-      k_flux_nodes_seg<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.in1_ptr, m.in1_edge, m.eoff, m.eres,
-                                                               m.eseg, (double4 *)r);
-      kf_count_launch(2);
-    } else
-#endif
     {
       if (first_order)
         k_flux_edges<true><<<blocks(m.E, 128), 128, 0, m.stream>>>(m.E, E0, E1, m.egeo_s, X, Q, nullptr, nullptr,
@@ -2263,8 +2204,8 @@ void residual(DevMesh &m, const double *q, double *r, int first_order, double u,
       else
         k_flux_edges<false><<<blocks(m.E, 128), 128, 0, m.stream>>>(m.E, E0, E1, m.egeo_s, X, Q, G[0], G[1], G[2],
                                                                      m.eres);
-      k_flux_nodes<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.in1_ptr, m.in1_edge, m.eoff, m.eres,
-                                                           (double4 *)r);
+      k_flux_nodes4<<<blocks(4 * (size_t)m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.in1_ptr, m.in1_edge, m.eoff,
+                                                                         (const double *)m.eres, r);
       kf_count_launch(2);
     }
   } else if (first_order)
@@ -2286,8 +2227,14 @@ void residual(DevMesh &m, const double *q, double *r, int first_order, double u,
 
 void timestep(DevMesh &m, const double *q, double cfl)
 {
-  k_timestep<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo,
-                                                      (const double4 *)q, m.bnd_of, cfl, m.cdt);
+  if (m.visit && m.inc_geo) {
+    visit_state(m, q);
+    k_timestep<true><<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.inc_ptr, m.inc_othv, m.inc_edge,
+                                                              m.inc_geo, m.qv, m.bnd_of, cfl, m.cdt);
+  } else {
+    k_timestep<false><<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.inc_ptr, m.inc_oth, m.inc_edge, m.egeo,
+                                                               (const double4 *)q, m.bnd_of, cfl, m.cdt);
+  }
   kf_count_launch();
   if (m.nb) {
     k_timestep_boundary<<<blocks(m.nb, 64), 64, 0, m.stream>>>(m.nb, m.bnd_node, m.bnd_ptr, m.bnd_ent, m.s_n,
@@ -2298,10 +2245,23 @@ void timestep(DevMesh &m, const double *q, double cfl)
 
 void fill(DevMesh &m, const double *q, double u, double v, int precision)
 {
+  const bool vis = m.visit && m.inc_geo;
+  if (vis) visit_state(m, q);
+  const uint32_t *oth = vis ? m.inc_othv : m.inc_oth;
+  const double4 *geo = vis ? m.inc_geo : m.egeo, *qq = vis ? m.qv : (const double4 *)q;
+  auto fill_fn = [&](auto *A, double *lslot, double *dscr) {
+    using T = std::remove_pointer_t<decltype(A)>;
+    if (vis)
+      k_fill<T, true><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.row_node, m.rowof, m.inc_ptr, oth, m.inc_edge,
+                                                              m.fill_blk, geo, qq, m.cdt, m.fill_diag, m.fill_last,
+                                                              m.fill_lpos, A, lslot, m.bnd_of, dscr);
+    else
+      k_fill<T, false><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.row_node, m.rowof, m.inc_ptr, oth, m.inc_edge,
+                                                               m.fill_blk, geo, qq, m.cdt, m.fill_diag, m.fill_last,
+                                                               m.fill_lpos, A, lslot, m.bnd_of, dscr);
+  };
   if (precision == 0) {
-    k_fill<double><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.rowof, m.inc_ptr, m.inc_oth, m.inc_edge, m.fill_blk,
-                                                          m.egeo, (const double4 *)q, m.cdt, m.fill_diag, m.fill_last,
-                                                          m.fill_lpos, m.A, m.lslot, m.bnd_of, nullptr);
+    fill_fn(m.A, m.lslot, nullptr);
     kf_count_launch();
     if (m.nb) {
       k_fill_boundary<double><<<blocks(m.nb, 64), 64, 0, m.stream>>>(m.nb, m.bnd_node, m.bnd_ptr, m.bnd_ent, m.s_n,
@@ -2310,9 +2270,7 @@ void fill(DevMesh &m, const double *q, double u, double v, int precision)
       kf_count_launch();
     }
   } else {
-    k_fill<float><<<blocks(m.N, 128), 128, 0, m.stream>>>(m.N, m.rowof, m.inc_ptr, m.inc_oth, m.inc_edge, m.fill_blk,
-                                                         m.egeo, (const double4 *)q, m.cdt, m.fill_diag, m.fill_last,
-                                                         m.fill_lpos, m.Af, nullptr, m.bnd_of, m.dscr);
+    fill_fn(m.Af, nullptr, m.dscr);
     kf_count_launch();
     if (m.nb) {
       k_fill_boundary<float><<<blocks(m.nb, 64), 64, 0, m.stream>>>(m.nb, m.bnd_node, m.bnd_ptr, m.bnd_ent, m.s_n,

@@ -193,20 +193,25 @@ def training_set(workdir, n_meshes=128, n=40, seed=0, stride=-3, cap=160, bump=(
     return out
 
 
-def train(net, data, steps, batch=8, lr=1e-3, seed=0, log=None, log_every=100):
+def train(net, data, steps, batch=8, lr=1e-3, seed=0, log=None, log_every=100, by_mesh=False):
     """Adam on the mean squared error over pairs: each step draws `batch`
     pairs at random (the kernels accumulate their gradients), then one Adam
-    step.  Returns the per-step loss."""
+    step.  by_mesh: the batch is `batch` different meshes, one pair drawn
+    from each.  Returns the per-step loss."""
     rng = np.random.default_rng(seed)
     index = [(k, j) for k, s in enumerate(data) for j in range(len(s))]
     if not index:
         raise ValueError("no training pairs")
+    meshes = [k for k, s in enumerate(data) if len(s)]
     losses = []
     for it in range(steps):
-        pick = rng.choice(len(index), size=min(batch, len(index)), replace=False)
+        if by_mesh:
+            ks = rng.choice(len(meshes), size=min(batch, len(meshes)), replace=False)
+            pick = [(meshes[k], int(rng.integers(len(data[meshes[k]])))) for k in ks]
+        else:
+            pick = [index[q] for q in rng.choice(len(index), size=min(batch, len(index)), replace=False)]
         loss = 0.0
-        for q in pick:
-            k, j = index[q]
+        for k, j in pick:
             s = data[k]
             loss += net.accumulate(s.graph, s.x0[j], s.target[j], 1.0 / (len(pick) * 4 * s.graph.nnodes))
         net.adam_step(lr=lr)

@@ -33,6 +33,8 @@ def main(argv=None):
     ap.add_argument("--cap", type=int, default=200, help="at most this many pairs per mesh")
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--batch-by-mesh", action="store_true",
+                    help="each batch is --batch different meshes, one pair from each")
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--eval-n", type=int, default=40, help="held-out mesh size (0: no evaluation)")
@@ -61,7 +63,8 @@ def main(argv=None):
         log(f"{rep['pairs']} pairs in {rep['pairs_seconds']:.1f} s; zero-correction loss {rep['zero_loss']:.4e}")
         net = learned.Network(seed=a.seed + 1)
         t0 = time.time()
-        losses = learned.train(net, data, a.steps, batch=a.batch, lr=a.lr, seed=a.seed, log=log, log_every=250)
+        losses = learned.train(net, data, a.steps, batch=a.batch, lr=a.lr, seed=a.seed, log=log, log_every=250,
+                               by_mesh=a.batch_by_mesh)
         rep["train_seconds"] = time.time() - t0
         rep["final_loss"] = float(np.mean(losses[-100:]))
         rep["loss_curve"] = [float(np.mean(losses[i:i + 100])) for i in range(0, len(losses), 100)]

@@ -88,9 +88,11 @@ FORMS = [
 
 
 def test_exact_box70_history_is_the_reference(box_mesh):
-    """The first four Newton steps (312 GMRES iterations) of the 70^3 solve,
-    every printed quantity bit for bit (exact mode runs without CUDA graphs,
-    so the whole 1039-iteration history is left to the fast-mode checks)."""
+    """The first three Newton steps (177 GMRES iterations) of the 70^3 solve,
+    every printed quantity bit for bit (exact mode runs without CUDA graphs
+    and with the reference's sequence of reductions, about 0.5 s an iteration
+    at this size, so the whole 1039-iteration history is left to the
+    fast-mode checks)."""
     gold = fixture("box70_forces.json")
     path = box_mesh(70, seed=1, bump=0.1)
     assert sha256(path) == gold["mesh_sha256"], "the generator no longer writes the fixture's mesh"
@@ -99,9 +101,9 @@ def test_exact_box70_history_is_the_reference(box_mesh):
     kf.set_ilu_order(0)
     kf.set_aoa(gold["params"]["aoa"])
     m = kf.Mesh(path)
-    hist = m.solve(ts_max=4, stop_ratio=gold["params"]["stop_ratio"])
-    assert len(hist) == 4
-    for h, w in zip(hist, gold["steps"][:4]):
+    hist = m.solve(ts_max=3, stop_ratio=gold["params"]["stop_ratio"])
+    assert len(hist) == 3
+    for h, w in zip(hist, gold["steps"][:3]):
         assert h["gmres_its"] == w["gmres_its"], h["step"]
         for k in ("cfl", "fnorm", "lift", "drag", "momn"):
             assert repr(h[k]) == w[k], (h["step"], k, h[k], w[k])
