@@ -493,6 +493,18 @@ def run_gpu_arm(args, cfg):
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
                 "peak_kind": peak_kind, "algorithmic_bytes": B[dominant]}
 
+    # set-up (outside the timed region): the device mirror, its block pattern
+    # built on the device, the spatial order's set, against the same pattern
+    # built on the host threads (checked equal element for element)
+    setup = None
+    if dist.rank == 0:
+        us = lambda k: round(m.query(k) / 1e6, 4)   # noqa: E731
+        setup = {"mirror_s": us("setup_us"), "pattern_on_device_s": us("pattern_us"),
+                 "spatial_order_s": us("spatial_setup_us")}
+        setup["pattern_matches_host"] = m.query("pattern_matches_host") == 1
+        setup["pattern_on_host_threads_s"] = us("host_pattern_us")
+        setup["host_threads"] = min(32, os.cpu_count() or 1)   # the host build's thread count
+
     cpu = None
     if dist.rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
         from oracle import ref
@@ -530,6 +542,7 @@ def run_gpu_arm(args, cfg):
             "gmres_iterations_per_s": gmres_its / value,
             "gpu_launches": int(launches),
             "comparison": comparison,
+            "setup": setup,
             "clocks": clocks,
             "cpu_baseline": cpu,
             "wall_s": wall,

@@ -75,8 +75,9 @@ void fun3d_printf(const uint32_t c, const char *format, ...);
 void Kernel(GEOMETRY *g);
 
 /* matrix/wrapper.cpp:23-28.  Creates the opaque matrix handle stored in
-   g->matrix (block pattern of the edge graph plus the diagonal).  No device
-   memory is touched until the first kernel call. */
+   g->matrix.  The handle keeps the edges; the block pattern of the edge graph
+   (with its level sets and ILU(0) product lists) is built on the device with
+   the mirror, at the first kernel call.  No device memory is touched before. */
 void *CXX_Matrix_Init(const size_t nnodes, const size_t nedges, const unsigned int block_size,
                       const unsigned int nthreads, const unsigned int *n0, const unsigned int *n1);
 /* matrix/wrapper.cpp:30-34 */
@@ -145,7 +146,7 @@ void kfun3d_set_precision(int p);
        KFUN3D_ERR_ARG.
    KFUN3D_ILU_PERM in the environment, read when the order is built:
    "sweep" renumbers by ascending x + y + z over the whole mesh, "tiles" tile
-   by tile for the tiled triangular sweep (KFUN3D_SPTRSV=tiled), "morton" by
+   by tile (one tile per SM, each tile swept by x + y + z), "morton" by
    the Morton order of the coordinates; KFUN3D_ILU_SLABS sets the number of
    slabs of the default order;
    "identity" keeps the mesh numbering through the same renumbering code
@@ -273,8 +274,16 @@ void kfun3d_device_release(GEOMETRY *g);
    terms recomputed on the device from per-node coefficients made there equal
    the GEOMETRY's stored terms bit for bit, "visit_order_copies" -> 1 when
    the residual passes work on copies of the node data in their spatial visit
-   order, "mgs_resident" -> 1 when Gram-Schmidt keeps the vector on chip.
-   -1 for an unknown key or on error. */
+   order, "mgs_resident" -> 1 when Gram-Schmidt keeps the vector on chip,
+   "pattern_matches_host" / "spatial_pattern_matches_host" -> 1 when the
+   block pattern, level lists and ILU(0) product lists built on the device
+   (mesh numbering / spatial renumbering; -1 while the latter is not built)
+   equal a host build from the same edges element for element, else 0,
+   "setup_us" / "pattern_us" / "spatial_setup_us" -> host wall time in
+   microseconds of building the mirror / its block pattern on the device /
+   the spatial order's set, "host_pattern_us" -> that of the host build the
+   last "pattern_matches_host" made (-1 before one).  -1 for an unknown key
+   or on error. */
 long kfun3d_device_query(const GEOMETRY *g, const char *key);
 
 /* ---------------------------------------------------------------------

@@ -2,6 +2,7 @@
 // GEOMETRY (built once per GEOMETRY, on its first kernel call).
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -236,8 +237,16 @@ extern "C" void *CXX_Matrix_Init(const size_t nnodes, const size_t nedges, const
     return nullptr;
   }
   MatrixHandle *h = new MatrixHandle();
-  kf_build_pattern(h->pat, nnodes, nedges, n0, n1);
+  h->e0.assign(n0, n0 + nedges);
+  h->e1.assign(n1, n1 + nedges);
+  h->pat.n = nnodes;   // the pattern itself: on the device with the mirror, or kf_host_pattern
   return h;
+}
+
+const HostPattern &kf_host_pattern(MatrixHandle *h)
+{
+  if (h->pat.ia.empty()) kf_build_pattern(h->pat, h->pat.n, h->e0.size(), h->e0.data(), h->e1.data());
+  return h->pat;
 }
 
 static void release_device(MatrixHandle *h);
@@ -406,6 +415,26 @@ extern "C" long kfun3d_device_query(const GEOMETRY *g, const char *key)
   if (strcmp(key, "lsq_terms_match") == 0) return m->lsq_match ? 1 : 0;
   if (strcmp(key, "visit_order_copies") == 0) return m->visit ? 1 : 0;
   if (strcmp(key, "mgs_resident") == 0) return m->mgs_resident ? 1 : 0;
+  if (strcmp(key, "setup_us") == 0) return m->setup_us;
+  if (strcmp(key, "pattern_us") == 0) return m->pattern_us;
+  if (strcmp(key, "spatial_setup_us") == 0) return m->spatial_us;
+  if (strcmp(key, "host_pattern_us") == 0) return m->host_pattern_us;
+  if (strcmp(key, "pattern_matches_host") == 0) {
+    const MatrixHandle *h = kf_handle(g);
+    return kf_pattern_matches(m->iset[0], m->N, m->E, h->e0.data(), h->e1.data(), m->stream, &m->host_pattern_us);
+  }
+  if (strcmp(key, "spatial_pattern_matches_host") == 0) {
+    if (!m->iset[1].valid) return -1;
+    std::vector<uint32_t> rank(m->N);
+    if (cudaMemcpy(rank.data(), m->ilu_rank, m->N * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      cudaGetLastError();
+      return -1;
+    }
+    const MatrixHandle *h = kf_handle(g);
+    std::vector<uint32_t> pn0(m->E), pn1(m->E);
+    for (size_t e = 0; e < m->E; e++) { pn0[e] = rank[h->e0[e]]; pn1[e] = rank[h->e1[e]]; }
+    return kf_pattern_matches(m->iset[1], m->N, m->E, pn0.data(), pn1.data(), m->stream, nullptr);
+  }
   return -1;
 }
 
@@ -437,9 +466,12 @@ DevMesh *kf_device(const GEOMETRY *g)
     }
     return nullptr;
   }
-  const HostPattern &p = h->pat;
+  const auto t_start = std::chrono::steady_clock::now();
+  auto us_since = [](std::chrono::steady_clock::time_point t) {
+    return (long)std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t).count();
+  };
   const uint32_t N = (uint32_t)g->n->sz, E = (uint32_t)g->e->sz;
-  if (p.n != N) {
+  if (h->pat.n != N || h->e0.size() != E) {
     kf_set_error(KFUN3D_ERR_ARG, "matrix handle does not match the GEOMETRY");
     return nullptr;
   }
@@ -450,6 +482,20 @@ DevMesh *kf_device(const GEOMETRY *g)
   h->owner = g;
   KF_CUDA(cudaGetDevice(&m->device));
   KF_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+  // the block pattern, persistent L slots and ILU(0) product lists, built on
+  // the device; the host keeps the arrays its set-up code below reads
+  {
+    DevPattern dp;
+    const auto t_pat = std::chrono::steady_clock::now();
+    if (kf_build_pattern_device(h->pat, dp, N, E, h->e0.data(), h->e1.data(), m->stream) != KFUN3D_OK) {
+      release_device(h);
+      return nullptr;
+    }
+    m->ia = dp.ia; m->ja = dp.ja; m->diag = dp.diag; m->tblk = dp.tblk; m->lpos = dp.lpos;
+    m->last_lower = dp.last_lower; m->pair_ptr = dp.pair_ptr; m->pairs = dp.pairs;
+    m->pattern_us = us_since(t_pat);
+  }
+  const HostPattern &p = h->pat;
   m->N = N;
   m->E = E;
   m->Ns = (uint32_t)g->b->s->sz;
@@ -702,15 +748,8 @@ DevMesh *kf_device(const GEOMETRY *g)
     KF_CUDA(upload(&m->bnd_ptr, bptr.data(), bptr.size()));
     KF_CUDA(upload(&m->bnd_ent, bent.data(), bent.size()));
   }
-  // block pattern, persistent L slots, level sets
-  KF_CUDA(upload(&m->ia, p.ia.data(), p.ia.size()));
-  KF_CUDA(upload(&m->ja, p.ja.data(), p.ja.size()));
-  KF_CUDA(upload(&m->diag, p.diag.data(), p.diag.size()));
-  KF_CUDA(upload(&m->tblk, p.tblk.data(), p.tblk.size()));
-  KF_CUDA(upload(&m->lpos, p.lpos.data(), p.lpos.size()));
-  KF_CUDA(upload(&m->last_lower, p.last_lower.data(), p.last_lower.size()));
-  KF_CUDA(upload(&m->pair_ptr, p.pair_ptr.data(), p.pair_ptr.size()));
-  KF_CUDA(upload(&m->pairs, reinterpret_cast<const uint2 *>(p.pairs.data()), p.pairs.size() / 2));
+  // level sets (the block pattern, persistent L slots and ILU(0) product
+  // lists were built on the device above)
   const std::vector<uint32_t> &lev_l = p.lev_l, &lev_u = p.lev_u;
   KF_CUDA(upload(&m->lev_l, lev_l.data(), lev_l.size()));
   KF_CUDA(upload(&m->lev_u, lev_u.data(), lev_u.size()));
@@ -845,8 +884,10 @@ DevMesh *kf_device(const GEOMETRY *g)
   // when they reproduce the GEOMETRY's stored ones bit for bit
   if (kf_exact::lsq_setup(*m) != KFUN3D_OK) {
     kf_set_error(KFUN3D_ERR_CUDA, "device mirror: least-squares coefficients failed");
+    release_device(h);
     return nullptr;
   }
   KF_CUDA(cudaDeviceSynchronize());
+  m->setup_us = us_since(t_start);
   return m;
 }

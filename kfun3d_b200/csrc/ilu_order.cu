@@ -11,6 +11,7 @@
 // renumbered pattern.  Not a parity path: the reference factors in its own
 // order, which stays the default (kfun3d_set_ilu_order(0)).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -252,22 +253,17 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
   const std::vector<uint32_t> rank = spatial_rank(g, N, tile);
   std::vector<uint32_t> pn0(E), pn1(E);
   for (size_t e = 0; e < E; e++) { pn0[e] = rank[n0[e]]; pn1[e] = rank[n1[e]]; }
+  // the permuted block pattern, built on the device
   HostPattern p;
-  kf_build_pattern(p, N, E, pn0.data(), pn1.data());
+  DevPattern dp;
+  if (kf_build_pattern_device(p, dp, N, E, pn0.data(), pn1.data(), m.stream) != KFUN3D_OK) return KFUN3D_ERR_CUDA;
   IluSet &s = m.iset[1];
+  s.ia = dp.ia; s.ja = dp.ja; s.diag = dp.diag; s.tblk = dp.tblk; s.lpos = dp.lpos;
+  s.last_lower = dp.last_lower; s.pair_ptr = dp.pair_ptr; s.pairs = dp.pairs;
   bool ok = true;
   auto up = [&](auto **dst, const auto &vec) {
     if (ok && upload(dst, vec.data(), vec.size()) != cudaSuccess) ok = false;
   };
-  up(&s.ia, p.ia);
-  up(&s.ja, p.ja);
-  up(&s.diag, p.diag);
-  up(&s.tblk, p.tblk);
-  up(&s.lpos, p.lpos);
-  up(&s.last_lower, p.last_lower);
-  up(&s.pair_ptr, p.pair_ptr);
-  if (ok && upload(&s.pairs, reinterpret_cast<const uint2 *>(p.pairs.data()), p.pairs.size() / 2) != cudaSuccess)
-    ok = false;
   up(&s.lev_l, p.lev_l);
   up(&s.lev_u, p.lev_u);
   s.lev_l_ptr = p.lev_l_ptr;
@@ -363,8 +359,11 @@ int kf_ilu_select(DevMesh &m, const GEOMETRY *g, int order)
   if (order == m.ilu_active) return KFUN3D_OK;
   if (order == 1 && !m.iset[1].valid) {
     kf_ilu_release(m);   // what an earlier attempt that ran out of memory left
+    const auto t0 = std::chrono::steady_clock::now();
     const int rc = build_spatial(m, g);
     if (rc != KFUN3D_OK) return rc;
+    m.spatial_us = (long)std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0)
+                       .count();
   }
   activate(m, m.iset[order]);
   m.ilu_active = order;

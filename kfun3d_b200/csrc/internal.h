@@ -45,6 +45,9 @@ struct HostPattern {
   // reference adds back.
   std::vector<uint32_t> pair_ptr;
   std::vector<uint32_t, uninit_alloc<uint32_t>> pairs;
+  // built on the device (kf_build_pattern_device): tblk, pair_ptr and pairs
+  // are then only on the device
+  bool on_device = false;
 };
 
 void kf_build_pattern(HostPattern &p, size_t nnodes, size_t nedges, const unsigned int *n0,
@@ -52,15 +55,22 @@ void kf_build_pattern(HostPattern &p, size_t nnodes, size_t nedges, const unsign
 
 struct DevMesh;
 
-// The opaque handle behind GEOMETRY::matrix.
+// The opaque handle behind GEOMETRY::matrix.  The edges given to
+// CXX_Matrix_Init are kept; the block pattern is built on the device with the
+// device mirror, or on the host threads when host code asks for it first
+// (kf_host_pattern).
 struct MatrixHandle {
   uint32_t magic = 0x4B463344u;   // "KF3D"
-  HostPattern pat;
+  std::vector<uint32_t> e0, e1;   // the edges (n0, n1)
+  HostPattern pat;                // pat.n is set at CXX_Matrix_Init, the rest when built
   DevMesh *dev = nullptr;
   const GEOMETRY *owner = nullptr;
 };
 
 MatrixHandle *kf_handle(const GEOMETRY *g);
+// The handle's host pattern, built on the host threads if it has not been
+// built yet (with the full product lists), for host-side readers.
+const HostPattern &kf_host_pattern(MatrixHandle *h);
 
 #ifdef __CUDACC__
 
@@ -150,6 +160,25 @@ int kf_build_packed(PackedSweep pk[2], const HostPattern &p, const std::vector<u
                     const std::vector<uint4> &desc_u);
 void kf_free_packed(PackedSweep pk[2]);
 
+// The block pattern built on the device (setup_device.cu): the device arrays,
+// and into `host` the arrays the host set-up code reads (ia, ja, diag, lpos,
+// last_lower, the level lists).  KFUN3D_OK or an error code, nothing left
+// allocated on error.
+struct DevPattern {
+  uint32_t *ia = nullptr, *ja = nullptr, *diag = nullptr, *tblk = nullptr, *lpos = nullptr;
+  uint32_t *last_lower = nullptr, *pair_ptr = nullptr;
+  uint2 *pairs = nullptr;
+  size_t npairs = 0;
+};
+int kf_build_pattern_device(HostPattern &host, DevPattern &d, size_t N, size_t E, const unsigned int *n0,
+                            const unsigned int *n1, cudaStream_t st);
+void kf_free_device_pattern(DevPattern &d);
+// 1 when every pattern array of `s` (on the device) and its level lists equal
+// kf_build_pattern's for the same edges, 0 when one differs, -1 on a CUDA error;
+// *host_us (if given) the host build's wall time in microseconds
+int kf_pattern_matches(const IluSet &s, size_t N, size_t E, const unsigned int *n0, const unsigned int *n1,
+                       cudaStream_t st, long *host_us);
+
 // Device mirror of one GEOMETRY.  Node-indexed arrays follow the reference's
 // numbering; edge-indexed arrays its (sorted) edge order.
 struct DevMesh {
@@ -170,6 +199,10 @@ struct DevMesh {
   uint32_t wstride = 0;           // 2E rounded up to a multiple of 4 (16-byte aligned rows)
   unsigned grad_smem = 0;         // dynamic shared memory of k_gradient_tma (0: not used)
   double4 *lsq_coef = nullptr;    // [2N] least-squares coefficients per node, computed on the device
+  // host wall time of the set-up, microseconds: the whole device mirror, its
+  // block pattern on the device, the spatial ILU(0) order's set (0 until built)
+  long setup_us = 0, pattern_us = 0, spatial_us = 0;
+  long host_pattern_us = -1;      // the same pattern on the host threads (set by the pattern check)
   bool lsq_match = false;         // the terms recomputed from lsq_coef equal the stored ones bit for bit
   int grad_lanes = 1;             // lanes per node of the gradient in the mesh's order (1 or 4)
   // visit-order copies for the residual passes on large meshes (spatial_order

@@ -1,0 +1,445 @@
+// kfun3d_b200: the block pattern of the edge graph built on the device.
+//
+// The same arrays kf_build_pattern makes on the host threads (device_mesh.cu;
+// matrix/init.cpp:7-74 for the pattern and 194-274 for the level sets, the
+// reference's fill order src/fill.c:496-511 for the persistent-L-slot rule,
+// matrix/ilu.cpp:71-84 for the ILU(0) products), bit for bit:
+//   ia/ja   rows of the diagonal and one block per incident edge, columns
+//           sorted (edges append to their rows through atomic slots, then
+//           each row is sorted, so the order of the appends does not matter);
+//   diag    each row's diagonal slot, lpos the first persistent L slot of each
+//           row (exclusive sum of the lower lengths);
+//   tblk    block (i,j) -> index of block (j,i);
+//   last_lower  the lower block of each row that the reference's fill touches
+//           last: the lower neighbour through the row's last incident edge in
+//           edge order (the largest such edge index, by atomicMax);
+//   levels  depth(i) = 1 + max depth over the lower (upper) columns, the
+//           longest-path fixpoint, reached by repeated sweeps (any visiting
+//           order reaches the same fixpoint); rows are then listed by level in
+//           row order on the host (a counting sort of N depths);
+//   pairs   for block (i,k) the merge of row i's columns up to its diagonal
+//           with row k's up to its diagonal: (L slot or ~0, block of U(m,k)),
+//           counted, summed and written in place.
+// The host keeps the arrays its own set-up code reads (ia, ja, diag, lpos,
+// last_lower, level lists); tblk, pair_ptr and pairs stay on the device.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <vector>
+
+#include "internal.h"
+
+namespace {
+
+inline unsigned nblk(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+__global__ void k_pat_count(uint32_t E, const uint32_t *__restrict__ n0, const uint32_t *__restrict__ n1,
+                            uint32_t *cnt)
+{
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  atomicAdd(cnt + n0[e], 1u);
+  atomicAdd(cnt + n1[e], 1u);
+}
+
+__global__ void k_pat_first(uint32_t N, const uint32_t *__restrict__ ia, uint32_t *ja, uint32_t *fillp)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  ja[ia[i]] = i;
+  fillp[i] = ia[i] + 1;
+}
+
+__global__ void k_pat_fill(uint32_t E, const uint32_t *__restrict__ n0, const uint32_t *__restrict__ n1,
+                           uint32_t *fillp, uint32_t *ja, uint32_t *lastE)
+{
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  const uint32_t a = n0[e], b = n1[e];
+  ja[atomicAdd(fillp + a, 1u)] = b;
+  ja[atomicAdd(fillp + b, 1u)] = a;
+  // the edge's lower end point is a lower neighbour of the other
+  if (b < a) atomicMax(lastE + a, e + 1);
+  if (a < b) atomicMax(lastE + b, e + 1);
+}
+
+// row i sorted (insertion sort: rows hold about 15 entries), its diagonal
+// slot, its lower length
+__global__ void k_pat_sort(uint32_t N, const uint32_t *__restrict__ ia, uint32_t *ja, uint32_t *diag,
+                           uint32_t *lcnt)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const uint32_t b = ia[i], e = ia[i + 1];
+  for (uint32_t k = b + 1; k < e; k++) {
+    const uint32_t v = ja[k];
+    uint32_t m = k;
+    while (m > b && ja[m - 1] > v) {
+      ja[m] = ja[m - 1];
+      m--;
+    }
+    ja[m] = v;
+  }
+  uint32_t d = b;
+  while (d < e && ja[d] != i) d++;
+  diag[i] = d;
+  lcnt[i] = d - b;
+}
+
+__device__ __forceinline__ uint32_t find_col(const uint32_t *__restrict__ ja, uint32_t b, uint32_t e, uint32_t c)
+{
+  while (b < e) {   // first position with ja >= c
+    const uint32_t m = (b + e) >> 1;
+    if (ja[m] < c) b = m + 1;
+    else e = m;
+  }
+  return b;
+}
+
+__global__ void k_pat_tblk(uint32_t N, const uint32_t *__restrict__ ia, const uint32_t *__restrict__ ja,
+                           uint32_t *tblk)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  for (uint32_t j = ia[i]; j < ia[i + 1]; j++) {
+    const uint32_t k = ja[j];
+    const uint32_t p = find_col(ja, ia[k], ia[k + 1], i);
+    tblk[j] = (p < ia[k + 1] && ja[p] == i) ? p : 0xffffffffu;
+  }
+}
+
+__global__ void k_pat_last_lower(uint32_t N, const uint32_t *__restrict__ n0, const uint32_t *__restrict__ n1,
+                                 const uint32_t *__restrict__ lastE, const uint32_t *__restrict__ ia,
+                                 const uint32_t *__restrict__ ja, uint32_t *last_lower)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const uint32_t le = lastE[i];
+  if (!le) {
+    last_lower[i] = 0xffffffffu;
+    return;
+  }
+  const uint32_t e = le - 1, o = n0[e] == i ? n1[e] : n0[e];
+  const uint32_t p = find_col(ja, ia[i], ia[i + 1], o);
+  last_lower[i] = (p < ia[i + 1] && ja[p] == o) ? p : 0xffffffffu;
+}
+
+// one relaxation sweep of depth(i) = 1 + max depth over the lower (LOWER) or
+// upper columns; *changed set when any depth grew
+template <bool LOWER>
+__global__ void k_pat_levels(uint32_t N, const uint32_t *__restrict__ ia, const uint32_t *__restrict__ ja,
+                             const uint32_t *__restrict__ diag, uint32_t *depth, uint32_t *changed)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const uint32_t jb = LOWER ? ia[i] : diag[i] + 1, je = LOWER ? diag[i] : ia[i + 1];
+  uint32_t d = 1;
+  for (uint32_t j = jb; j < je; j++) d = max(d, ((volatile uint32_t *)depth)[ja[j]] + 1);
+  if (d > depth[i]) {
+    depth[i] = d;
+    *changed = 1;
+  }
+}
+
+// ILU(0) products of every block of row i (matrix/ilu.cpp:71-84): COUNT
+// writes the number per block, otherwise the (L slot or ~0, U block) pairs
+template <bool COUNT>
+__global__ void k_pat_pairs(uint32_t N, const uint32_t *__restrict__ ia, const uint32_t *__restrict__ ja,
+                            const uint32_t *__restrict__ diag, const uint32_t *__restrict__ lpos,
+                            const uint32_t *__restrict__ tblk, uint32_t *cnt, const uint32_t *__restrict__ pair_ptr,
+                            uint2 *pairs)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const uint32_t di = diag[i], ai = ia[i];
+  for (uint32_t j = ia[i]; j < ia[i + 1]; j++) {
+    const uint32_t k = ja[j], dk = diag[k];
+    uint32_t pl = ai, pu = ia[k], c = 0, o = COUNT ? 0 : pair_ptr[j];
+    while (pl <= di && pu <= dk) {
+      const uint32_t cl = ja[pl], cu = ja[pu];
+      if (cl == cu) {
+        if (!COUNT) pairs[o + c] = make_uint2(cl == i ? 0xffffffffu : lpos[i] + (pl - ai), tblk[pu]);
+        c++;
+      }
+      if (cl <= cu) pl++;
+      if (cl >= cu) pu++;
+    }
+    if (COUNT) cnt[j] = c;
+  }
+}
+
+// ---------------------------------------------------------------- exclusive scan
+// out[0..n] = exclusive prefix sums of in[0..n-1] (out[n] = the total), in
+// blocks of 1024 with the block totals scanned recursively.
+
+__global__ void k_scan_block(size_t n, const uint32_t *__restrict__ in, uint32_t *out, uint32_t *bsum)
+{
+  __shared__ uint32_t s[1024];
+  const size_t i = (size_t)blockIdx.x * 1024 + threadIdx.x;
+  const uint32_t v = i < n ? in[i] : 0;
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (unsigned off = 1; off < 1024; off <<= 1) {
+    const uint32_t t = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
+    __syncthreads();
+    s[threadIdx.x] += t;
+    __syncthreads();
+  }
+  if (i < n) out[i] = s[threadIdx.x] - v;
+  if (threadIdx.x == 1023) bsum[blockIdx.x] = s[1023];
+}
+
+__global__ void k_scan_add(size_t n, uint32_t *out, const uint32_t *__restrict__ boff)
+{
+  const size_t i = (size_t)blockIdx.x * 1024 + threadIdx.x;
+  if (i < n) out[i] += boff[blockIdx.x];
+}
+
+__global__ void k_scan_total(size_t n, const uint32_t *__restrict__ in, uint32_t *out)
+{
+  out[n] = n ? out[n - 1] + in[n - 1] : 0;
+}
+
+cudaError_t scan(size_t n, const uint32_t *in, uint32_t *out, cudaStream_t st)
+{
+  if (n == 0) {
+    k_scan_total<<<1, 1, 0, st>>>(0, in, out);
+    return cudaGetLastError();
+  }
+  const size_t nb = (n + 1023) / 1024;
+  uint32_t *bsum = nullptr, *boff = nullptr;
+  cudaError_t e = cudaMallocAsync(&bsum, nb * sizeof(uint32_t), st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&boff, (nb + 1) * sizeof(uint32_t), st);
+  if (e != cudaSuccess) {
+    if (bsum) cudaFreeAsync(bsum, st);
+    return e;
+  }
+  k_scan_block<<<(unsigned)nb, 1024, 0, st>>>(n, in, out, bsum);
+  kf_count_launch();
+  if (nb > 1) {
+    e = scan(nb, bsum, boff, st);
+    if (e == cudaSuccess) {
+      k_scan_add<<<(unsigned)nb, 1024, 0, st>>>(n, out, boff);
+      kf_count_launch();
+    }
+  }
+  k_scan_total<<<1, 1, 0, st>>>(n, in, out);
+  kf_count_launch();
+  cudaFreeAsync(bsum, st);
+  cudaFreeAsync(boff, st);
+  return e == cudaSuccess ? cudaGetLastError() : e;
+}
+
+// rows listed by level in row order from their depths (counting sort)
+void levels_from_depth(const std::vector<uint32_t> &depth, std::vector<uint32_t> &rows, std::vector<uint32_t> &ptr)
+{
+  const size_t N = depth.size();
+  uint32_t nlev = 1;
+  for (uint32_t d : depth) nlev = d > nlev ? d : nlev;
+  ptr.assign(nlev + 1, 0);
+  for (size_t i = 0; i < N; i++) ptr[depth[i]]++;
+  for (uint32_t l = 0; l < nlev; l++) ptr[l + 1] += ptr[l];
+  rows.assign(N, 0);
+  std::vector<uint32_t> top(ptr.begin(), ptr.end() - 1);
+  for (size_t i = 0; i < N; i++) rows[top[depth[i] - 1]++] = (uint32_t)i;
+}
+
+}  // namespace
+
+int kf_pattern_matches(const IluSet &s, size_t N, size_t E, const unsigned int *n0, const unsigned int *n1,
+                       cudaStream_t st, long *host_us)
+{
+  HostPattern r;
+  const auto t0 = std::chrono::steady_clock::now();
+  kf_build_pattern(r, N, E, n0, n1);
+  if (host_us)
+    *host_us = (long)std::chrono::duration_cast<std::chrono::microseconds>(std::chrono::steady_clock::now() - t0)
+                   .count();
+  bool ok = true, same = true;
+  auto cmp = [&](const uint32_t *dev, const uint32_t *host, size_t n) {
+    if (!ok || !same) return;
+    std::vector<uint32_t> v(n);
+    if (n && (cudaMemcpyAsync(v.data(), dev, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+              cudaStreamSynchronize(st) != cudaSuccess)) {
+      ok = false;
+      return;
+    }
+    same = std::equal(v.begin(), v.end(), host);
+  };
+  cmp(s.ia, r.ia.data(), N + 1);
+  cmp(s.ja, r.ja.data(), r.nnz);
+  cmp(s.diag, r.diag.data(), N);
+  cmp(s.tblk, r.tblk.data(), r.nnz);
+  cmp(s.lpos, r.lpos.data(), N + 1);
+  cmp(s.last_lower, r.last_lower.data(), N);
+  cmp(s.pair_ptr, r.pair_ptr.data(), r.nnz + 1);
+  cmp(reinterpret_cast<const uint32_t *>(s.pairs), r.pairs.data(), r.pairs.size());
+  cmp(s.lev_l, r.lev_l.data(), N);
+  cmp(s.lev_u, r.lev_u.data(), N);
+  same = same && s.lev_l_ptr == r.lev_l_ptr && s.lev_u_ptr == r.lev_u_ptr;
+  if (!ok) {
+    cudaGetLastError();
+    kf_set_error(KFUN3D_ERR_CUDA, "pattern check: a copy from the device failed");
+    return -1;
+  }
+  return same ? 1 : 0;
+}
+
+void kf_free_device_pattern(DevPattern &d)
+{
+  void *ptrs[] = {d.ia, d.ja, d.diag, d.tblk, d.lpos, d.last_lower, d.pair_ptr, d.pairs};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  d = DevPattern{};
+}
+
+int kf_build_pattern_device(HostPattern &p, DevPattern &d, size_t N, size_t E, const unsigned int *n0,
+                            const unsigned int *n1, cudaStream_t st)
+{
+  d = DevPattern{};
+  // every end point a row of the matrix (the kernels below index by them)
+  if (N == 0 || N >= 0xffffffffu || E >= 0x7fffffffu) {
+    kf_set_error(KFUN3D_ERR_ARG, "block pattern: no nodes, or more nodes or edges than 32-bit indices hold");
+    return KFUN3D_ERR_ARG;
+  }
+  for (size_t e = 0; e < E; e++)
+    if (n0[e] >= N || n1[e] >= N) {
+      kf_set_error(KFUN3D_ERR_ARG, "block pattern: an edge end point is not a node");
+      return KFUN3D_ERR_ARG;
+    }
+  uint32_t *dn0 = nullptr, *dn1 = nullptr, *cnt = nullptr, *fillp = nullptr, *lastE = nullptr, *lcnt = nullptr;
+  uint32_t *depth = nullptr, *changed = nullptr;
+  bool ok = true;
+  auto ck = [&](cudaError_t e) {
+    if (e != cudaSuccess && ok) {
+      ok = false;
+      cudaGetLastError();
+    }
+  };
+  const size_t N1 = N + 1;
+  ck(cudaMalloc(&dn0, (E + 1) * sizeof(uint32_t)));
+  ck(cudaMalloc(&dn1, (E + 1) * sizeof(uint32_t)));
+  ck(cudaMalloc(&cnt, N1 * sizeof(uint32_t)));
+  ck(cudaMalloc(&fillp, N1 * sizeof(uint32_t)));
+  ck(cudaMalloc(&lastE, N1 * sizeof(uint32_t)));
+  ck(cudaMalloc(&lcnt, N1 * sizeof(uint32_t)));
+  ck(cudaMalloc(&depth, 2 * N1 * sizeof(uint32_t)));
+  ck(cudaMalloc(&changed, sizeof(uint32_t)));
+  ck(cudaMalloc(&d.ia, N1 * sizeof(uint32_t)));
+  ck(cudaMalloc(&d.diag, N1 * sizeof(uint32_t)));
+  ck(cudaMalloc(&d.lpos, N1 * sizeof(uint32_t)));
+  ck(cudaMalloc(&d.last_lower, N1 * sizeof(uint32_t)));
+  if (ok && E) {
+    ck(cudaMemcpyAsync(dn0, n0, E * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    ck(cudaMemcpyAsync(dn1, n1, E * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  }
+  size_t nnz = 0;
+  const std::vector<uint32_t> ones(N, 1u);
+  if (ok) {
+    // row lengths: 1 (the diagonal) + incident edges
+    ck(cudaMemcpyAsync(cnt, ones.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    ck(cudaMemsetAsync(lastE, 0, N1 * sizeof(uint32_t), st));
+    if (E) {
+      k_pat_count<<<nblk(E, 256), 256, 0, st>>>((uint32_t)E, dn0, dn1, cnt);
+      kf_count_launch();
+    }
+    ck(scan(N, cnt, d.ia, st));
+    uint32_t nz = 0;
+    ck(cudaMemcpyAsync(&nz, d.ia + N, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    ck(cudaStreamSynchronize(st));
+    nnz = nz;
+  }
+  if (ok) {
+    ck(cudaMalloc(&d.ja, (nnz + 1) * sizeof(uint32_t)));
+    ck(cudaMalloc(&d.tblk, (nnz + 1) * sizeof(uint32_t)));
+    ck(cudaMalloc(&d.pair_ptr, (nnz + 1) * sizeof(uint32_t)));
+  }
+  if (ok) {
+    k_pat_first<<<nblk(N, 256), 256, 0, st>>>((uint32_t)N, d.ia, d.ja, fillp);
+    if (E) k_pat_fill<<<nblk(E, 256), 256, 0, st>>>((uint32_t)E, dn0, dn1, fillp, d.ja, lastE);
+    k_pat_sort<<<nblk(N, 128), 128, 0, st>>>((uint32_t)N, d.ia, d.ja, d.diag, lcnt);
+    kf_count_launch(E ? 3 : 2);
+    ck(cudaGetLastError());
+    ck(scan(N, lcnt, d.lpos, st));
+    k_pat_tblk<<<nblk(N, 128), 128, 0, st>>>((uint32_t)N, d.ia, d.ja, d.tblk);
+    k_pat_last_lower<<<nblk(N, 256), 256, 0, st>>>((uint32_t)N, dn0, dn1, lastE, d.ia, d.ja, d.last_lower);
+    kf_count_launch(2);
+    ck(cudaGetLastError());
+  }
+  // level sets: relax until no depth grows (at most one sweep more than levels)
+  std::vector<uint32_t> hdepth[2];
+  for (int lower = 1; lower >= 0 && ok; lower--) {
+    uint32_t *dp = depth + (lower ? 0 : N1);
+    ck(cudaMemcpyAsync(dp, ones.data(), N * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    for (size_t it = 0; it <= N && ok; it++) {
+      uint32_t h = 0;
+      ck(cudaMemsetAsync(changed, 0, sizeof(uint32_t), st));
+      if (lower) k_pat_levels<true><<<nblk(N, 256), 256, 0, st>>>((uint32_t)N, d.ia, d.ja, d.diag, dp, changed);
+      else k_pat_levels<false><<<nblk(N, 256), 256, 0, st>>>((uint32_t)N, d.ia, d.ja, d.diag, dp, changed);
+      kf_count_launch();
+      ck(cudaGetLastError());
+      ck(cudaMemcpyAsync(&h, changed, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+      ck(cudaStreamSynchronize(st));
+      if (!h) break;
+    }
+    hdepth[lower ? 0 : 1].resize(N);
+    ck(cudaMemcpyAsync(hdepth[lower ? 0 : 1].data(), dp, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  }
+  // ILU(0) product lists: counts per block (into a buffer of nnz entries),
+  // their exclusive sums, then the pairs
+  if (ok) {
+    ck(cudaStreamSynchronize(st));
+    cudaFree(fillp);   // the row slots are no longer needed
+    fillp = nullptr;
+    ck(cudaMalloc(&fillp, (nnz + 1) * sizeof(uint32_t)));
+  }
+  if (ok) {
+    k_pat_pairs<true><<<nblk(N, 128), 128, 0, st>>>((uint32_t)N, d.ia, d.ja, d.diag, d.lpos, d.tblk, fillp, nullptr,
+                                                   nullptr);
+    kf_count_launch();
+    ck(cudaGetLastError());
+    ck(scan(nnz, fillp, d.pair_ptr, st));
+    uint32_t np = 0;
+    ck(cudaMemcpyAsync(&np, d.pair_ptr + nnz, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    ck(cudaStreamSynchronize(st));
+    d.npairs = np;
+    if (ok) ck(cudaMalloc(&d.pairs, (size_t)std::max<uint32_t>(np, 1) * sizeof(uint2)));
+    if (ok) {
+      k_pat_pairs<false><<<nblk(N, 128), 128, 0, st>>>((uint32_t)N, d.ia, d.ja, d.diag, d.lpos, d.tblk, nullptr,
+                                                      d.pair_ptr, d.pairs);
+      kf_count_launch();
+      ck(cudaGetLastError());
+    }
+  }
+  // the host's copy of what its set-up code reads
+  if (ok) {
+    p = HostPattern{};
+    p.n = N;
+    p.nnz = nnz;
+    p.ia.resize(N1);
+    p.ja.resize(nnz);
+    p.diag.resize(N);
+    p.lpos.resize(N1);
+    p.last_lower.resize(N);
+    ck(cudaMemcpyAsync(p.ia.data(), d.ia, N1 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    ck(cudaMemcpyAsync(p.ja.data(), d.ja, nnz * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    ck(cudaMemcpyAsync(p.diag.data(), d.diag, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    ck(cudaMemcpyAsync(p.lpos.data(), d.lpos, N1 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    ck(cudaMemcpyAsync(p.last_lower.data(), d.last_lower, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    ck(cudaStreamSynchronize(st));
+  }
+  if (ok) {
+    levels_from_depth(hdepth[0], p.lev_l, p.lev_l_ptr);
+    levels_from_depth(hdepth[1], p.lev_u, p.lev_u_ptr);
+    p.on_device = true;
+  }
+  void *tmp[] = {dn0, dn1, cnt, fillp, lastE, lcnt, depth, changed};
+  for (void *t : tmp)
+    if (t) cudaFree(t);
+  if (!ok) {
+    kf_free_device_pattern(d);
+    kf_set_error(KFUN3D_ERR_CUDA, "block pattern on the device: a CUDA call failed");
+    return KFUN3D_ERR_CUDA;
+  }
+  return KFUN3D_OK;
+}

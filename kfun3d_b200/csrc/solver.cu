@@ -1553,7 +1553,7 @@ extern "C" long kfun3d_matrix_read(const GEOMETRY *g, unsigned int *ia, unsigned
     kf_set_error(KFUN3D_ERR_ARG, "GEOMETRY::matrix is not a kfun3d_b200 handle");
     return -1;
   }
-  const HostPattern &p = h->pat;
+  const HostPattern &p = kf_host_pattern(h);
   if (ia) memcpy(ia, p.ia.data(), p.ia.size() * sizeof(unsigned int));
   if (ja) memcpy(ja, p.ja.data(), p.ja.size() * sizeof(unsigned int));
   if (blocks) {

@@ -276,9 +276,10 @@ def test_exact_kernels_any_node_order(box_mesh, order, monkeypatch):
 
 
 def test_exact_factor_on_a_mesh_built_by_the_threaded_host_paths(box_mesh):
-    """42^3 (74,088 rows) builds the block pattern, the level sets and the
-    ILU(0) product lists on several host threads; factor and solves must
-    still equal the oracle's bit for bit."""
+    """42^3 (74,088 rows) runs the host-side set-up (incidence lists, visit
+    order, level descriptors) on several host threads, and the block pattern
+    with its many-CTA scans on the device; factor and solves must still equal
+    the oracle's bit for bit."""
     kf.set_mode("exact")
     kf.set_precision(0)
     kf.set_aoa(3.06)
@@ -295,4 +296,25 @@ def test_exact_factor_on_a_mesh_built_by_the_threaded_host_paths(box_mesh):
         assert np.array_equal(m.matrix()[2], M.blocks()), step
         b = np.random.default_rng(13 + step).standard_normal(v.dofs)
         assert np.array_equal(m.sptrsv(b), M.sptrsv(b)), step
+    assert kf.last_status() == 0
+
+
+def test_block_pattern_built_on_the_device_equals_the_host_build(box_mesh):
+    """The block pattern, transpose map, persistent L slots, last-touched
+    lower blocks, level lists and ILU(0) product lists that the device builds
+    (setup_device.cu) equal kf_build_pattern's on the host, element for
+    element, in the mesh numbering and in the spatial renumbering; meshes from
+    one scan block to several, randomly and regularly numbered."""
+    kf.set_aoa(3.06)
+    for path in (MESH_A, box_mesh(10, seed=3), box_mesh(42, seed=13), box_mesh(23, seed=7, permute=False)):
+        kf.set_ilu_order(0)
+        m = kf.Mesh(path)
+        assert m.query("pattern_matches_host") == 1, path
+        assert m.query("spatial_pattern_matches_host") == -1, path   # not built yet
+        kf.set_ilu_order(1)
+        m.flux(m.view.q.copy())    # the first entry point in the spatial order builds it
+        assert m.query("spatial_pattern_matches_host") == 1, path
+        assert m.query("pattern_matches_host") == 1, path
+        assert m.query("pattern_us") > 0 and m.query("setup_us") >= m.query("pattern_us")
+    kf.set_ilu_order(0)
     assert kf.last_status() == 0
