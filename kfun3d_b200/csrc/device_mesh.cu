@@ -407,6 +407,121 @@ static void release_device(MatrixHandle *h)
   h->dev = nullptr;
 }
 
+// The mirror's edge geometry, incidence lists, two-pass edge storage and
+// visit-order copies rebuilt on the host threads from the GEOMETRY (in the
+// visit order the mirror uses) and compared with the device-built arrays,
+// element for element and bit for bit: 1 equal, 0 different, -1 CUDA error.
+static int lists_match_host(const DevMesh &m, const GEOMETRY *g, const HostPattern &p)
+{
+  const uint32_t N = m.N, E = m.E;
+  const unsigned int *n0 = g->e->eptr->n0, *n1 = g->e->eptr->n1;
+  bool ok = true, same = true;
+  auto down = [&](auto &vec, const void *src) {
+    if (ok && !vec.empty() && cudaMemcpy(vec.data(), src, vec.size() * sizeof(vec[0]), cudaMemcpyDeviceToHost) != cudaSuccess)
+      ok = false;
+  };
+  auto cmp = [&](const auto &host, const void *dev) {
+    if (!ok || !same) return;
+    auto d = host;
+    down(d, dev);
+    same = ok && memcmp(d.data(), host.data(), host.size() * sizeof(host[0])) == 0;
+  };
+  std::vector<uint32_t> ord(N), rowof(N);
+  down(ord, m.ord);
+  for (uint32_t q = 0; q < N; q++) rowof[ord[q]] = q;
+  std::vector<double4> eg(E);
+  for (uint32_t e = 0; e < E; e++)
+    eg[e] = make_double4(g->e->xyzn->x0[e], g->e->xyzn->x1[e], g->e->xyzn->x2[e], g->e->xyzn->x3[e]);
+  cmp(eg, m.egeo);
+  cmp(rowof, m.rowof);
+  // incidence: per visit position, the node's edges in edge order
+  std::vector<uint32_t> deg(N, 0), ptr(N + 1, 0);
+  for (uint32_t e = 0; e < E; e++) { deg[n0[e]]++; deg[n1[e]]++; }
+  for (uint32_t q = 0; q < N; q++) ptr[q + 1] = ptr[q] + deg[ord[q]];
+  const size_t ninc = 2 * (size_t)E, wst = m.wstride;
+  std::vector<uint32_t> oth(wst + 4, 0), edg(ninc), blk(ninc), pos(N);
+  std::vector<double> w(3 * wst + 4, 0.0);
+  for (uint32_t i = 0; i < N; i++) pos[i] = ptr[rowof[i]];
+  const double *w0[3] = {g->e->w->w0->x0, g->e->w->w0->x1, g->e->w->w0->x2};
+  const double *w1[3] = {g->e->w->w1->x0, g->e->w->w1->x1, g->e->w->w1->x2};
+  for (uint32_t e = 0; e < E; e++) {
+    const uint32_t a = n0[e], b = n1[e];
+    uint32_t k = pos[a]++;
+    oth[k] = b; edg[k] = e;
+    for (int c = 0; c < 3; c++) w[c * wst + k] = w0[c][e];
+    k = pos[b]++;
+    oth[k] = a; edg[k] = e | 0x80000000u;
+    for (int c = 0; c < 3; c++) w[c * wst + k] = w1[c][e];
+  }
+  parallel_ranges(N, [&](size_t r0, size_t r1) {
+    for (size_t row = r0; row < r1; row++)
+      for (uint32_t k = ptr[row]; k < ptr[row + 1]; k++) {
+        auto b = p.ja.begin() + p.ia[ord[row]], en = p.ja.begin() + p.ia[ord[row] + 1];
+        blk[k] = (uint32_t)(std::lower_bound(b, en, oth[k]) - p.ja.begin());
+      }
+  });
+  cmp(ptr, m.inc_ptr);
+  cmp(oth, m.inc_oth);
+  cmp(edg, m.inc_edge);
+  cmp(blk, m.inc_blk);
+  cmp(w, m.inc_w);
+  if (m.two_pass) {
+    // storage: groups by n0 in visit order, each in edge order
+    std::vector<uint32_t> r0(N + 1, 0), c1(N, 0);
+    for (uint32_t e = 0; e < E; e++) { r0[n0[e] + 1]++; c1[n1[e]]++; }
+    for (uint32_t i = 0; i < N; i++) r0[i + 1] += r0[i];
+    std::vector<uint32_t> eoff(N + 1, 0), spos(E), n0s(E), n1s(E), iptr(N + 1, 0), iedge(E);
+    std::vector<double4> egs(E);
+    uint32_t next = 0;
+    for (uint32_t q = 0; q < N; q++) {
+      const uint32_t nd = ord[q];
+      eoff[q] = next;
+      for (uint32_t e = r0[nd]; e < r0[nd + 1]; e++) {
+        spos[e] = next;
+        n0s[next] = nd;
+        n1s[next] = n1[e];
+        egs[next] = eg[e];
+        next++;
+      }
+      iptr[q + 1] = iptr[q] + c1[nd];
+    }
+    eoff[N] = next;
+    std::vector<uint32_t> ipos(N);
+    for (uint32_t q = 0; q < N; q++) ipos[ord[q]] = iptr[q];
+    for (uint32_t e = 0; e < E; e++) iedge[ipos[n1[e]]++] = spos[e];
+    cmp(eoff, m.eoff);
+    cmp(n0s, m.n0s);
+    cmp(n1s, m.n1);
+    cmp(egs, m.egeo_s);
+    cmp(iptr, m.in1_ptr);
+    cmp(iedge, m.in1_edge);
+    if (m.visit) {
+      std::vector<uint32_t> othv(ninc), e0v(E), e1v(E);
+      std::vector<double4> xv(N), ig(ninc);
+      for (uint32_t q = 0; q < N; q++) {
+        const uint32_t nd = ord[q];
+        xv[q] = make_double4(g->n->xyz->x0[nd], g->n->xyz->x1[nd], g->n->xyz->x2[nd], 0.0);
+      }
+      for (size_t k = 0; k < ninc; k++) {
+        othv[k] = rowof[oth[k]];
+        ig[k] = eg[edg[k] & 0x7fffffffu];
+      }
+      for (uint32_t e = 0; e < E; e++) { e0v[e] = rowof[n0s[e]]; e1v[e] = rowof[n1s[e]]; }
+      cmp(othv, m.inc_othv);
+      cmp(ig, m.inc_geo);
+      cmp(e0v, m.n0v);
+      cmp(e1v, m.n1v);
+      cmp(xv, m.xyzv);
+    }
+  }
+  if (!ok) {
+    cudaGetLastError();
+    kf_set_error(KFUN3D_ERR_CUDA, "mesh list check: a copy from the device failed");
+    return -1;
+  }
+  return same ? 1 : 0;
+}
+
 extern "C" long kfun3d_device_query(const GEOMETRY *g, const char *key)
 {
   DevMesh *m = key ? kf_device(g) : nullptr;
@@ -419,6 +534,7 @@ extern "C" long kfun3d_device_query(const GEOMETRY *g, const char *key)
   if (strcmp(key, "pattern_us") == 0) return m->pattern_us;
   if (strcmp(key, "spatial_setup_us") == 0) return m->spatial_us;
   if (strcmp(key, "host_pattern_us") == 0) return m->host_pattern_us;
+  if (strcmp(key, "lists_match_host") == 0) return lists_match_host(*m, g, kf_host_pattern(kf_handle(g)));
   if (strcmp(key, "pattern_matches_host") == 0) {
     const MatrixHandle *h = kf_handle(g);
     return kf_pattern_matches(m->iset[0], m->N, m->E, h->e0.data(), h->e1.data(), m->stream, &m->host_pattern_us);
@@ -477,11 +593,13 @@ DevMesh *kf_device(const GEOMETRY *g)
   }
   const unsigned int *n0 = g->e->eptr->n0, *n1 = g->e->eptr->n1;
 
+  SetupTrace tr("device mirror");
   DevMesh *m = new DevMesh();
   h->dev = m;
   h->owner = g;
   KF_CUDA(cudaGetDevice(&m->device));
   KF_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+  tr.mark("CUDA context and stream");
   // the block pattern, persistent L slots and ILU(0) product lists, built on
   // the device; the host keeps the arrays its set-up code below reads
   {
@@ -495,6 +613,7 @@ DevMesh *kf_device(const GEOMETRY *g)
     m->last_lower = dp.last_lower; m->pair_ptr = dp.pair_ptr; m->pairs = dp.pairs;
     m->pattern_us = us_since(t_pat);
   }
+  tr.mark("block pattern on the device");
   const HostPattern &p = h->pat;
   m->N = N;
   m->E = E;
@@ -505,14 +624,11 @@ DevMesh *kf_device(const GEOMETRY *g)
   m->nnz = (uint32_t)p.nnz;
   m->nlower = p.lpos[N];
 
-  // edge geometry and node coordinates
+  // node coordinates
   {
-    std::vector<double4> eg(E), xyz(N);
-    for (uint32_t e = 0; e < E; e++)
-      eg[e] = make_double4(g->e->xyzn->x0[e], g->e->xyzn->x1[e], g->e->xyzn->x2[e], g->e->xyzn->x3[e]);
+    std::vector<double4> xyz(N);
     for (uint32_t i = 0; i < N; i++)
       xyz[i] = make_double4(g->n->xyz->x0[i], g->n->xyz->x1[i], g->n->xyz->x2[i], 0.0);
-    KF_CUDA(upload(&m->egeo, eg.data(), E));
     KF_CUDA(upload(&m->xyz, xyz.data(), N));
   }
   // Order in which the node-centric kernels visit nodes: on meshes whose node
@@ -560,48 +676,36 @@ DevMesh *kf_device(const GEOMETRY *g)
       std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
     }
     KF_CUDA(upload(&m->ord, ord.data(), N));
-  }
-  // node incidence in edge order, with the least-squares terms seen from the
-  // node (w0 at n0, w1 at n1) and the block of (node, other); row p of the
-  // CSR belongs to node ord[p]
-  {
-    std::vector<uint32_t> deg(N, 0), ptr(N + 1, 0), rowof(N);
-    for (uint32_t e = 0; e < E; e++) { deg[n0[e]]++; deg[n1[e]]++; }
-    for (uint32_t p2 = 0; p2 < N; p2++) {
-      ptr[p2 + 1] = ptr[p2] + deg[ord[p2]];
-      rowof[ord[p2]] = p2;
-    }
+    std::vector<uint32_t> rowof(N);
+    for (uint32_t q = 0; q < N; q++) rowof[ord[q]] = q;
     KF_CUDA(upload(&m->rowof, rowof.data(), N));
-    const size_t ninc = 2 * (size_t)E;
-    const size_t wst = (ninc + 3) & ~(size_t)3;   // rows of inc_w start on 16 bytes
-    m->wstride = (uint32_t)wst;
-    std::vector<uint32_t> oth(wst + 4, 0), edg(ninc), blk(ninc), pos(N);
-    for (uint32_t i = 0; i < N; i++) pos[i] = ptr[rowof[i]];
-    std::vector<double> w(3 * wst + 4, 0.0);
-    const double *w0[3] = {g->e->w->w0->x0, g->e->w->w0->x1, g->e->w->w0->x2};
-    const double *w1[3] = {g->e->w->w1->x0, g->e->w->w1->x1, g->e->w->w1->x2};
-    auto find = [&](uint32_t row, uint32_t col) -> uint32_t {
-      auto b = p.ja.begin() + p.ia[row], en = p.ja.begin() + p.ia[row + 1];
-      return (uint32_t)(std::lower_bound(b, en, col) - p.ja.begin());
-    };
-    for (uint32_t e = 0; e < E; e++) {
-      const uint32_t a = n0[e], b = n1[e];
-      uint32_t k = pos[a]++;
-      oth[k] = b; edg[k] = e;
-      for (int c = 0; c < 3; c++) w[c * wst + k] = w0[c][e];
-      k = pos[b]++;
-      oth[k] = a; edg[k] = e | 0x80000000u;
-      for (int c = 0; c < 3; c++) w[c * wst + k] = w1[c][e];
+  }
+  tr.mark("visit order");
+  // two-pass residual structure when the edges are sorted by n0 with n0 < n1
+  // everywhere; visit-order copies of the node data when the visit order is
+  // not the mesh's own (KFUN3D_VISIT_COPIES=0: not)
+  {
+    bool ok = true;
+    for (uint32_t e = 0; e < E && ok; e++) {
+      if (n0[e] >= n1[e]) ok = false;
+      if (e && n0[e] < n0[e - 1]) ok = false;
     }
-    parallel_ranges(N, [&](size_t r0, size_t r1) {   // block of (node, other), row by row
-      for (size_t row = r0; row < r1; row++)
-        for (uint32_t k = ptr[row]; k < ptr[row + 1]; k++) blk[k] = find(ord[row], oth[k]);
-    });
-    KF_CUDA(upload(&m->inc_ptr, ptr.data(), N + 1));
-    KF_CUDA(upload(&m->inc_oth, oth.data(), oth.size()));
-    KF_CUDA(upload(&m->inc_edge, edg.data(), ninc));
-    KF_CUDA(upload(&m->inc_blk, blk.data(), ninc));
-    KF_CUDA(upload(&m->inc_w, w.data(), w.size()));
+    const char *env = getenv("KFUN3D_RESIDUAL");
+    m->two_pass = ok && !(env && strcmp(env, "gather") == 0);
+    const char *venv = getenv("KFUN3D_VISIT_COPIES");
+    m->visit = m->two_pass && m->spatial_order && !(venv && strcmp(venv, "0") == 0);
+  }
+  // edge geometry, node incidence in edge order (with the least-squares
+  // terms seen from the node and the block of (node, other)), the two-pass
+  // residual's edge storage and the visit-order copies, built on the device
+  if (kf_build_mesh_lists_device(*m, g) != KFUN3D_OK) {
+    release_device(h);
+    return nullptr;
+  }
+  tr.mark("incidence lists, residual structure, visit-order copies");
+  {
+    std::vector<uint32_t> ptr(N + 1);
+    KF_CUDA(cudaMemcpy(ptr.data(), m->inc_ptr, ((size_t)N + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     // shared memory of the staged gradient: the widest 128-node block range
     size_t maxcnt = 0;
     for (uint32_t nb = 0; nb < N; nb += 128) {
@@ -618,82 +722,6 @@ DevMesh *kf_device(const GEOMETRY *g)
     if (genv && strcmp(genv, "plain") == 0) tma = false;
     if (genv && strcmp(genv, "tma") == 0) tma = smem <= 200 * 1024;
     m->grad_smem = tma ? (unsigned)smem : 0;
-  }
-  // two-pass residual structure: edges sorted by n0 with n0 < n1 everywhere
-  {
-    bool ok = true;
-    for (uint32_t e = 0; e < E && ok; e++) {
-      if (n0[e] >= n1[e]) ok = false;
-      if (e && n0[e] < n0[e - 1]) ok = false;
-    }
-    const char *env = getenv("KFUN3D_RESIDUAL");
-    m->two_pass = ok && !(env && strcmp(env, "gather") == 0);
-    if (m->two_pass) {
-      // reference ranges of the edges with n0 = node (contiguous, edges sorted by n0)
-      std::vector<uint32_t> r0(N + 1, 0), c1(N, 0);
-      for (uint32_t e = 0; e < E; e++) { r0[n0[e] + 1]++; c1[n1[e]]++; }
-      for (uint32_t i = 0; i < N; i++) r0[i + 1] += r0[i];
-      // storage: groups by n0 in visit order, each in edge order
-      std::vector<uint32_t> eoff(N + 1, 0), spos(E), n0s(E), n1s(E), iptr(N + 1, 0), iedge(E);
-      std::vector<double4> egs(E);
-      uint32_t next = 0;
-      for (uint32_t p2 = 0; p2 < N; p2++) {
-        const uint32_t nd = ord[p2];
-        eoff[p2] = next;
-        for (uint32_t e = r0[nd]; e < r0[nd + 1]; e++) {
-          spos[e] = next;
-          n0s[next] = nd;
-          n1s[next] = n1[e];
-          egs[next] = make_double4(g->e->xyzn->x0[e], g->e->xyzn->x1[e], g->e->xyzn->x2[e], g->e->xyzn->x3[e]);
-          next++;
-        }
-        iptr[p2 + 1] = iptr[p2] + c1[nd];
-      }
-      eoff[N] = next;
-      std::vector<uint32_t> ipos(N);
-      for (uint32_t p2 = 0; p2 < N; p2++) ipos[ord[p2]] = iptr[p2];
-      for (uint32_t e = 0; e < E; e++) iedge[ipos[n1[e]]++] = spos[e];
-      KF_CUDA(upload(&m->eoff, eoff.data(), N + 1));
-      KF_CUDA(upload(&m->n0s, n0s.data(), E));
-      KF_CUDA(upload(&m->n1, n1s.data(), E));
-      KF_CUDA(upload(&m->egeo_s, egs.data(), E));
-      KF_CUDA(upload(&m->in1_ptr, iptr.data(), N + 1));
-      KF_CUDA(upload(&m->in1_edge, iedge.data(), E));
-      KF_CUDA(cudaMalloc(&m->eres, std::max<size_t>(E, 1) * sizeof(double4)));
-      // visit-order copies for the residual passes when the visit order is
-      // not the mesh's own (KFUN3D_VISIT_COPIES=0: not): the edges' end
-      // points and each incidence's other end as visit positions, the
-      // coordinates in visit order, room for the state and the gradients
-      const char *venv = getenv("KFUN3D_VISIT_COPIES");
-      m->visit = m->spatial_order && !(venv && strcmp(venv, "0") == 0);
-      if (m->visit) {
-        std::vector<uint32_t> rowv(N), othv(2 * (size_t)E), e0v(E), e1v(E);
-        std::vector<double4> xv(N);
-        for (uint32_t p2 = 0; p2 < N; p2++) {
-          rowv[ord[p2]] = p2;
-          const uint32_t nd = ord[p2];
-          xv[p2] = make_double4(g->n->xyz->x0[nd], g->n->xyz->x1[nd], g->n->xyz->x2[nd], 0.0);
-        }
-        std::vector<uint32_t> othm(2 * (size_t)E), edgm(2 * (size_t)E);
-        KF_CUDA(cudaMemcpy(othm.data(), m->inc_oth, 2 * (size_t)E * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-        KF_CUDA(cudaMemcpy(edgm.data(), m->inc_edge, 2 * (size_t)E * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-        std::vector<double4> ig(2 * (size_t)E);
-        const double *gx0 = g->e->xyzn->x0, *gx1 = g->e->xyzn->x1, *gx2 = g->e->xyzn->x2, *gx3 = g->e->xyzn->x3;
-        for (size_t k = 0; k < 2 * (size_t)E; k++) {
-          othv[k] = rowv[othm[k]];
-          const uint32_t e = edgm[k] & 0x7fffffffu;
-          ig[k] = make_double4(gx0[e], gx1[e], gx2[e], gx3[e]);
-        }
-        KF_CUDA(upload(&m->inc_geo, ig.data(), ig.size()));
-        for (uint32_t e = 0; e < E; e++) { e0v[e] = rowv[n0s[e]]; e1v[e] = rowv[n1s[e]]; }
-        KF_CUDA(upload(&m->inc_othv, othv.data(), othv.size()));
-        KF_CUDA(upload(&m->n0v, e0v.data(), E));
-        KF_CUDA(upload(&m->n1v, e1v.data(), E));
-        KF_CUDA(upload(&m->xyzv, xv.data(), N));
-        double4 **vv[] = {&m->qv, &m->gxv, &m->gyv, &m->gzv};
-        for (double4 **v : vv) KF_CUDA(cudaMalloc(v, (size_t)N * sizeof(double4)));
-      }
-    }
   }
   // wall faces (colour order) with normals -(1/6) a x b (src/flux.c:485-508)
   {
@@ -748,6 +776,7 @@ DevMesh *kf_device(const GEOMETRY *g)
     KF_CUDA(upload(&m->bnd_ptr, bptr.data(), bptr.size()));
     KF_CUDA(upload(&m->bnd_ent, bent.data(), bent.size()));
   }
+  tr.mark("boundary lists");
   // level sets (the block pattern, persistent L slots and ILU(0) product
   // lists were built on the device above)
   const std::vector<uint32_t> &lev_l = p.lev_l, &lev_u = p.lev_u;
@@ -864,6 +893,7 @@ DevMesh *kf_device(const GEOMETRY *g)
     const char *genv = getenv("KFUN3D_GRAPHS");
     m->use_graphs = !(genv && strcmp(genv, "0") == 0);
   }
+  tr.mark("matrix, vectors, level descriptors, packed schedule");
   KF_CUDA(cudaMallocHost(&m->h_scal, 256 * sizeof(double)));
   {
     IluSet &s0 = m->iset[0];
@@ -888,6 +918,7 @@ DevMesh *kf_device(const GEOMETRY *g)
     return nullptr;
   }
   KF_CUDA(cudaDeviceSynchronize());
+  tr.mark("least-squares coefficients");
   m->setup_us = us_since(t_start);
   return m;
 }

@@ -427,6 +427,7 @@ template <class F> void parallel_ranges(size_t n, F f)
 
 extern "C" GEOMETRY *kfun3d_setup_load(const char *path)
 {
+  SetupTrace tr("load");
   FILE *fs = fopen(path, "rb");
   if (!fs) { kf_set_error(KFUN3D_ERR_IO, "cannot open mesh file"); return nullptr; }
   fseek(fs, 0, SEEK_END);
@@ -435,6 +436,7 @@ extern "C" GEOMETRY *kfun3d_setup_load(const char *path)
   std::vector<unsigned char> buf((size_t)fsz);
   if (fread(buf.data(), 1, (size_t)fsz, fs) != (size_t)fsz) { fclose(fs); kf_set_error(KFUN3D_ERR_IO, "short read"); return nullptr; }
   fclose(fs);
+  tr.mark("file read");
   Reader rd{buf.data(), buf.data() + fsz};
   uint32_t p[13];
   rd.u32(p, 13);
@@ -448,7 +450,9 @@ extern "C" GEOMETRY *kfun3d_setup_load(const char *path)
   rd.f64(nbuf.data(), 4 * E);
   std::vector<uint32_t> order(E), tmp(E);
   for (size_t i = 0; i < E; i++) order[i] = (uint32_t)i;
+  tr.mark("edges decoded");
   if (E) index_sort(ebuf.data(), order.data(), order.data() + E, tmp.data(), true, E > 100000 ? sort_levels() : 0);
+  tr.mark("index sort");
   g->e = alloc<struct etbl>(1);
   g->e->sz = E;
   g->e->eptr = alloc<struct edge>(1);
@@ -466,6 +470,7 @@ extern "C" GEOMETRY *kfun3d_setup_load(const char *path)
     g->e->xyzn->x2[i] = nbuf[s + 2 * E];
     g->e->xyzn->x3[i] = nbuf[s + 3 * E];
   }
+  tr.mark("edges permuted");
   // nodes (src/nodes.c:19-56); the dual volume is read and dropped
   g->n = alloc<struct ntbl>(1);
   g->n->sz = N;
@@ -517,7 +522,9 @@ extern "C" GEOMETRY *kfun3d_setup_load(const char *path)
   g->c->b = 4;
   g->c->b2 = 16;
   g->c->sz = 4 * N;
+  tr.mark("nodes and boundaries");
   g->matrix = CXX_Matrix_Init(N, E, 4, 1, g->e->eptr->n0, g->e->eptr->n1);
+  tr.mark("matrix handle");
 
   // one thread owns every node and edge (src/subdomains.c:116-188 at T = 1)
   g->s = alloc<struct stbl>(1);
@@ -552,6 +559,7 @@ extern "C" GEOMETRY *kfun3d_setup_load(const char *path)
     g->t->i[c] = sum;
   }
 
+  tr.mark("wall colouring");
   // least-squares weights (src/weights.c:299-398).  The reference's edge
   // loops add into both end points; here every node gathers over its edges in
   // edge order (the same additions in the same order) and the nodes run in
@@ -685,6 +693,7 @@ extern "C" GEOMETRY *kfun3d_setup_load(const char *path)
     g->e->w->w1->x0 = t1x; g->e->w->w1->x1 = t1y; g->e->w->w1->x2 = t1z;
   }
 
+  tr.mark("least-squares weights");
   // free-stream initial state (src/guess.c:8-20)
   g->q = alloc<struct qtbl>(1);
   g->q->q = alloc<double>(4 * N);

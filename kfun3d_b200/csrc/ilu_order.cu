@@ -249,14 +249,18 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m.device);
   const uint32_t T = (uint32_t)std::max(1, nsm);
+  SetupTrace tr("spatial order");
   const std::vector<uint32_t> tile = partition_tiles(g->n->xyz->x0, g->n->xyz->x1, g->n->xyz->x2, N, T);
+  tr.mark("tiles");
   const std::vector<uint32_t> rank = spatial_rank(g, N, tile);
+  tr.mark("rank");
   std::vector<uint32_t> pn0(E), pn1(E);
   for (size_t e = 0; e < E; e++) { pn0[e] = rank[n0[e]]; pn1[e] = rank[n1[e]]; }
   // the permuted block pattern, built on the device
   HostPattern p;
   DevPattern dp;
   if (kf_build_pattern_device(p, dp, N, E, pn0.data(), pn1.data(), m.stream) != KFUN3D_OK) return KFUN3D_ERR_CUDA;
+  tr.mark("renumbered edges, block pattern on the device");
   IluSet &s = m.iset[1];
   s.ia = dp.ia; s.ja = dp.ja; s.diag = dp.diag; s.tblk = dp.tblk; s.lpos = dp.lpos;
   s.last_lower = dp.last_lower; s.pair_ptr = dp.pair_ptr; s.pairs = dp.pairs;
@@ -294,6 +298,7 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
     up(&s.desc_u, du);
     if (ok && kf_build_packed(s.pk, p, dl, du) == KFUN3D_ERR_CUDA) ok = false;
   }
+  tr.mark("level descriptors, packed schedule");
   // the fill's view of the renumbered pattern, per node of the mesh
   {
     std::vector<uint32_t> inc_ptr(N + 1), inc_oth(2 * E), ord(N);
@@ -345,6 +350,7 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
     kf_set_error(KFUN3D_ERR_CUDA, "spatial ILU(0) order: out of device memory");
     return KFUN3D_ERR_CUDA;
   }
+  tr.mark("fill targets");
   s.valid = true;
   return KFUN3D_OK;
 }

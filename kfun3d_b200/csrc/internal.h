@@ -1,8 +1,11 @@
 // kfun3d_b200 internals shared by the host and CUDA translation units.
 #pragma once
 
+#include <chrono>
 #include <cstddef>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <memory>
 #include <vector>
 
@@ -15,6 +18,24 @@ struct double4_host { double x, y, z, w; };
 #endif
 
 void kf_set_error(int code, const char *msg);
+
+// Set-up phase trace: with KFUN3D_SETUP_TRACE=1 in the environment, each
+// mark() prints to stderr the host wall time since the tracer's previous mark.
+struct SetupTrace {
+  const char *scope;
+  bool on;
+  std::chrono::steady_clock::time_point t;
+  explicit SetupTrace(const char *s)
+      : scope(s), on(getenv("KFUN3D_SETUP_TRACE") && atoi(getenv("KFUN3D_SETUP_TRACE")) > 0),
+        t(std::chrono::steady_clock::now()) {}
+  void mark(const char *phase)
+  {
+    if (!on) return;
+    const auto n = std::chrono::steady_clock::now();
+    fprintf(stderr, "kfun3d_b200 set-up: %s: %s %.3f s\n", scope, phase, std::chrono::duration<double>(n - t).count());
+    t = n;
+  }
+};
 int kf_mode();
 int kf_precision();
 int kf_first_order();
@@ -173,6 +194,13 @@ struct DevPattern {
 int kf_build_pattern_device(HostPattern &host, DevPattern &d, size_t N, size_t E, const unsigned int *n0,
                             const unsigned int *n1, cudaStream_t st);
 void kf_free_device_pattern(DevPattern &d);
+// The mirror's edge geometry (egeo), node incidence lists (inc_*), two-pass
+// edge storage (eoff, n0s, n1, egeo_s, in1_*) and visit-order copies
+// (inc_othv, inc_geo, n0v, n1v, xyzv), built on the device from the
+// GEOMETRY's edges, edge geometry and least-squares terms; m.ord, m.rowof,
+// m.xyz, the block pattern, m.two_pass and m.visit are set before.  KFUN3D_OK
+// or an error code (the arrays made so far are the mirror's, freed with it).
+int kf_build_mesh_lists_device(DevMesh &m, const GEOMETRY *g);
 // 1 when every pattern array of `s` (on the device) and its level lists equal
 // kf_build_pattern's for the same edges, 0 when one differs, -1 on a CUDA error;
 // *host_us (if given) the host build's wall time in microseconds

@@ -230,6 +230,144 @@ cudaError_t scan(size_t n, const uint32_t *in, uint32_t *out, cudaStream_t st)
   return e == cudaSuccess ? cudaGetLastError() : e;
 }
 
+// ------------------------------------------------------- mesh lists of the mirror
+
+__global__ void k_pack4(uint32_t n, const double *__restrict__ a, const double *__restrict__ b,
+                        const double *__restrict__ c, const double *__restrict__ d, double4 *out)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = make_double4(a[i], b[i], c[i], d[i]);
+}
+
+// incident edges of node ord[p] (row p): 1 + their count is the node's
+// pattern row length
+__global__ void k_inc_count(uint32_t N, const uint32_t *__restrict__ ord, const uint32_t *__restrict__ ia,
+                            uint32_t *cnt)
+{
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t i = ord[p];
+  cnt[p] = ia[i + 1] - ia[i] - 1;
+}
+
+__global__ void k_inc_place(uint32_t E, const uint32_t *__restrict__ n0, const uint32_t *__restrict__ n1,
+                            const uint32_t *__restrict__ rowof, const uint32_t *__restrict__ ptr, uint32_t *slot,
+                            uint32_t *edg)
+{
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  const uint32_t a = n0[e], b = n1[e];
+  edg[ptr[rowof[a]] + atomicAdd(slot + a, 1u)] = e;
+  edg[ptr[rowof[b]] + atomicAdd(slot + b, 1u)] = e | 0x80000000u;
+}
+
+// each row back in edge order (an edge appears once per row), then its other
+// end points, least-squares terms seen from the node and blocks of (node, other)
+__global__ void k_inc_rows(uint32_t N, const uint32_t *__restrict__ ord, const uint32_t *__restrict__ ptr,
+                           uint32_t *edg, const uint32_t *__restrict__ n0, const uint32_t *__restrict__ n1,
+                           const double *__restrict__ w, size_t E, const uint32_t *__restrict__ ia,
+                           const uint32_t *__restrict__ ja, uint32_t *oth, double *incw, size_t wst, uint32_t *blk)
+{
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t b = ptr[p], en = ptr[p + 1], node = ord[p];
+  for (uint32_t k = b + 1; k < en; k++) {
+    const uint32_t v = edg[k];
+    uint32_t m = k;
+    while (m > b && (edg[m - 1] & 0x7fffffffu) > (v & 0x7fffffffu)) {
+      edg[m] = edg[m - 1];
+      m--;
+    }
+    edg[m] = v;
+  }
+  for (uint32_t k = b; k < en; k++) {
+    const uint32_t v = edg[k], e = v & 0x7fffffffu, side = v >> 31;
+    const uint32_t o = side ? n0[e] : n1[e];
+    oth[k] = o;
+    for (int c = 0; c < 3; c++) incw[c * wst + k] = w[(3 * side + c) * E + e];
+    blk[k] = find_col(ja, ia[node], ia[node + 1], o);
+  }
+}
+
+// first edge with n0 >= i (edges sorted by n0)
+__global__ void k_n0_start(uint32_t N, uint32_t E, const uint32_t *__restrict__ n0, uint32_t *r0)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > N) return;
+  uint32_t lo = 0, hi = E;
+  while (lo < hi) {
+    const uint32_t m = (lo + hi) >> 1;
+    if (n0[m] < i) lo = m + 1;
+    else hi = m;
+  }
+  r0[i] = lo;
+}
+
+// per visit position: edges with n0 = ord[p] (storage group size) and the
+// node's n1-side incidences
+__global__ void k_group_counts(uint32_t N, const uint32_t *__restrict__ ord, const uint32_t *__restrict__ r0,
+                               const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ edg, uint32_t *c0,
+                               uint32_t *c1)
+{
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t i = ord[p];
+  c0[p] = r0[i + 1] - r0[i];
+  uint32_t c = 0;
+  for (uint32_t k = ptr[p]; k < ptr[p + 1]; k++) c += edg[k] >> 31;
+  c1[p] = c;
+}
+
+__global__ void k_store_edges(uint32_t E, const uint32_t *__restrict__ n0, const uint32_t *__restrict__ n1,
+                              const uint32_t *__restrict__ rowof, const uint32_t *__restrict__ eoff,
+                              const uint32_t *__restrict__ r0, const double4 *__restrict__ egeo, uint32_t *spos,
+                              uint32_t *n0s, uint32_t *n1s, double4 *egs)
+{
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  const uint32_t a = n0[e], s = eoff[rowof[a]] + (e - r0[a]);
+  spos[e] = s;
+  n0s[s] = a;
+  n1s[s] = n1[e];
+  egs[s] = egeo[e];
+}
+
+__global__ void k_in1_edges(uint32_t N, const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ edg,
+                            const uint32_t *__restrict__ iptr, const uint32_t *__restrict__ spos, uint32_t *iedge)
+{
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  uint32_t j = iptr[p];
+  for (uint32_t k = ptr[p]; k < ptr[p + 1]; k++)
+    if (edg[k] >> 31) iedge[j++] = spos[edg[k] & 0x7fffffffu];
+}
+
+__global__ void k_visit_incidence(size_t n, const uint32_t *__restrict__ oth, const uint32_t *__restrict__ edg,
+                                  const uint32_t *__restrict__ rowof, const double4 *__restrict__ egeo,
+                                  uint32_t *othv, double4 *geo)
+{
+  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  othv[k] = rowof[oth[k]];
+  geo[k] = egeo[edg[k] & 0x7fffffffu];
+}
+
+__global__ void k_visit_edges(uint32_t E, const uint32_t *__restrict__ n0s, const uint32_t *__restrict__ n1s,
+                              const uint32_t *__restrict__ rowof, uint32_t *e0v, uint32_t *e1v)
+{
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= E) return;
+  e0v[s] = rowof[n0s[s]];
+  e1v[s] = rowof[n1s[s]];
+}
+
+__global__ void k_visit_nodes(uint32_t N, const uint32_t *__restrict__ ord, const double4 *__restrict__ xyz,
+                              double4 *xv)
+{
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < N) xv[p] = xyz[ord[p]];
+}
+
 // rows listed by level in row order from their depths (counting sort)
 void levels_from_depth(const std::vector<uint32_t> &depth, std::vector<uint32_t> &rows, std::vector<uint32_t> &ptr)
 {
@@ -439,6 +577,139 @@ int kf_build_pattern_device(HostPattern &p, DevPattern &d, size_t N, size_t E, c
   if (!ok) {
     kf_free_device_pattern(d);
     kf_set_error(KFUN3D_ERR_CUDA, "block pattern on the device: a CUDA call failed");
+    return KFUN3D_ERR_CUDA;
+  }
+  return KFUN3D_OK;
+}
+
+int kf_build_mesh_lists_device(DevMesh &m, const GEOMETRY *g)
+{
+  const uint32_t N = m.N, E = m.E;
+  const cudaStream_t st = m.stream;
+  const size_t ninc = 2 * (size_t)E, wst = (ninc + 3) & ~(size_t)3;
+  m.wstride = (uint32_t)wst;
+  uint32_t *dn0 = nullptr, *dn1 = nullptr, *cnt = nullptr, *slot = nullptr, *r0 = nullptr, *c1 = nullptr,
+           *spos = nullptr;
+  double *raw = nullptr;   // [4][E] edge geometry, then [6][E] least-squares terms (w0, w1)
+  bool ok = true;
+  auto ck = [&](cudaError_t e) {
+    if (e != cudaSuccess && ok) {
+      ok = false;
+      cudaGetLastError();
+    }
+  };
+  auto up = [&](void *dst, const void *src, size_t bytes) {
+    if (ok && bytes) ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+  };
+  const size_t E1 = (size_t)E + 1, N1 = (size_t)N + 1;
+  ck(cudaMalloc(&dn0, E1 * sizeof(uint32_t)));
+  ck(cudaMalloc(&dn1, E1 * sizeof(uint32_t)));
+  ck(cudaMalloc(&cnt, N1 * sizeof(uint32_t)));
+  ck(cudaMalloc(&slot, N1 * sizeof(uint32_t)));
+  ck(cudaMalloc(&raw, 6 * E1 * sizeof(double)));
+  ck(cudaMalloc(&m.egeo, E1 * sizeof(double4)));
+  ck(cudaMalloc(&m.inc_ptr, N1 * sizeof(uint32_t)));
+  ck(cudaMalloc(&m.inc_oth, (wst + 4) * sizeof(uint32_t)));
+  ck(cudaMalloc(&m.inc_edge, (ninc + 1) * sizeof(uint32_t)));
+  ck(cudaMalloc(&m.inc_blk, (ninc + 1) * sizeof(uint32_t)));
+  ck(cudaMalloc(&m.inc_w, (3 * wst + 4) * sizeof(double)));
+  up(dn0, g->e->eptr->n0, (size_t)E * sizeof(uint32_t));
+  up(dn1, g->e->eptr->n1, (size_t)E * sizeof(uint32_t));
+  // edge geometry (unit normal, area) packed per edge
+  {
+    const double *src[4] = {g->e->xyzn->x0, g->e->xyzn->x1, g->e->xyzn->x2, g->e->xyzn->x3};
+    for (int c = 0; c < 4; c++) up(raw + c * (size_t)E, src[c], (size_t)E * sizeof(double));
+    if (ok && E) {
+      k_pack4<<<nblk(E, 256), 256, 0, st>>>(E, raw, raw + E, raw + 2 * (size_t)E, raw + 3 * (size_t)E, m.egeo);
+      kf_count_launch();
+      ck(cudaGetLastError());
+    }
+  }
+  // node incidence in edge order (row p belongs to node ord[p])
+  if (ok) {
+    const double *src[6] = {g->e->w->w0->x0, g->e->w->w0->x1, g->e->w->w0->x2,
+                            g->e->w->w1->x0, g->e->w->w1->x1, g->e->w->w1->x2};
+    for (int c = 0; c < 6; c++) up(raw + c * (size_t)E, src[c], (size_t)E * sizeof(double));
+    ck(cudaMemsetAsync(slot, 0, N1 * sizeof(uint32_t), st));
+    ck(cudaMemsetAsync(m.inc_oth, 0, (wst + 4) * sizeof(uint32_t), st));
+    ck(cudaMemsetAsync(m.inc_w, 0, (3 * wst + 4) * sizeof(double), st));
+  }
+  if (ok) {
+    k_inc_count<<<nblk(N, 256), 256, 0, st>>>(N, m.ord, m.ia, cnt);
+    kf_count_launch();
+    ck(cudaGetLastError());
+    ck(scan(N, cnt, m.inc_ptr, st));
+  }
+  if (ok) {
+    if (E) {
+      k_inc_place<<<nblk(E, 256), 256, 0, st>>>(E, dn0, dn1, m.rowof, m.inc_ptr, slot, m.inc_edge);
+      kf_count_launch();
+    }
+    k_inc_rows<<<nblk(N, 128), 128, 0, st>>>(N, m.ord, m.inc_ptr, m.inc_edge, dn0, dn1, raw, E, m.ia, m.ja,
+                                            m.inc_oth, m.inc_w, wst, m.inc_blk);
+    kf_count_launch();
+    ck(cudaGetLastError());
+  }
+  // two-pass residual storage: groups by n0 in visit order, each in edge order
+  if (ok && m.two_pass) {
+    ck(cudaMalloc(&r0, N1 * sizeof(uint32_t)));
+    ck(cudaMalloc(&c1, N1 * sizeof(uint32_t)));
+    ck(cudaMalloc(&spos, E1 * sizeof(uint32_t)));
+    ck(cudaMalloc(&m.eoff, N1 * sizeof(uint32_t)));
+    ck(cudaMalloc(&m.n0s, E1 * sizeof(uint32_t)));
+    ck(cudaMalloc(&m.n1, E1 * sizeof(uint32_t)));
+    ck(cudaMalloc(&m.egeo_s, E1 * sizeof(double4)));
+    ck(cudaMalloc(&m.in1_ptr, N1 * sizeof(uint32_t)));
+    ck(cudaMalloc(&m.in1_edge, E1 * sizeof(uint32_t)));
+    ck(cudaMalloc(&m.eres, E1 * sizeof(double4)));
+    if (ok) {
+      k_n0_start<<<nblk(N1, 256), 256, 0, st>>>(N, E, dn0, r0);
+      k_group_counts<<<nblk(N, 256), 256, 0, st>>>(N, m.ord, r0, m.inc_ptr, m.inc_edge, cnt, c1);
+      kf_count_launch(2);
+      ck(cudaGetLastError());
+      ck(scan(N, cnt, m.eoff, st));
+      ck(scan(N, c1, m.in1_ptr, st));
+    }
+    if (ok) {
+      if (E) {
+        k_store_edges<<<nblk(E, 256), 256, 0, st>>>(E, dn0, dn1, m.rowof, m.eoff, r0, m.egeo, spos, m.n0s, m.n1,
+                                                   m.egeo_s);
+        kf_count_launch();
+      }
+      k_in1_edges<<<nblk(N, 256), 256, 0, st>>>(N, m.inc_ptr, m.inc_edge, m.in1_ptr, spos, m.in1_edge);
+      kf_count_launch();
+      ck(cudaGetLastError());
+    }
+    // visit-order copies: each incidence's other end as a visit position and
+    // its edge geometry, the edges' end points as visit positions, the
+    // coordinates in visit order, room for the state and the gradients
+    if (ok && m.visit) {
+      ck(cudaMalloc(&m.inc_othv, (ninc + 1) * sizeof(uint32_t)));
+      ck(cudaMalloc(&m.inc_geo, (ninc + 1) * sizeof(double4)));
+      ck(cudaMalloc(&m.n0v, E1 * sizeof(uint32_t)));
+      ck(cudaMalloc(&m.n1v, E1 * sizeof(uint32_t)));
+      ck(cudaMalloc(&m.xyzv, N1 * sizeof(double4)));
+      double4 **vv[] = {&m.qv, &m.gxv, &m.gyv, &m.gzv};
+      for (double4 **v : vv) ck(cudaMalloc(v, N1 * sizeof(double4)));
+      if (ok) {
+        if (E) {
+          k_visit_incidence<<<nblk(ninc, 256), 256, 0, st>>>(ninc, m.inc_oth, m.inc_edge, m.rowof, m.egeo,
+                                                             m.inc_othv, m.inc_geo);
+          k_visit_edges<<<nblk(E, 256), 256, 0, st>>>(E, m.n0s, m.n1, m.rowof, m.n0v, m.n1v);
+          kf_count_launch(2);
+        }
+        k_visit_nodes<<<nblk(N, 256), 256, 0, st>>>(N, m.ord, m.xyz, m.xyzv);
+        kf_count_launch();
+        ck(cudaGetLastError());
+      }
+    }
+  }
+  ck(cudaStreamSynchronize(st));
+  void *tmp[] = {dn0, dn1, cnt, slot, raw, r0, c1, spos};
+  for (void *t : tmp)
+    if (t) cudaFree(t);
+  if (!ok) {
+    kf_set_error(KFUN3D_ERR_CUDA, "device mirror: building the incidence lists on the device failed");
     return KFUN3D_ERR_CUDA;
   }
   return KFUN3D_OK;

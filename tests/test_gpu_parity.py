@@ -256,6 +256,10 @@ def test_exact_kernels_any_node_order(box_mesh, order, monkeypatch):
     kf.set_aoa(3.06)
     for path in (box_mesh(12, seed=41), MESH_A):
         m = kf.Mesh(path)
+        # the incidence lists, edge storage and visit-order copies built on
+        # the device equal the host's sequential build element for element
+        assert m.query("lists_match_host") == 1, (order, path)
+        assert m.query("visit_order_copies") == (1 if order == "morton" else 0), (order, path)
         v = m.view
         q = seeded_state(v.q.copy(), 41)
         (g1, r1) = m.flux(q)
@@ -310,7 +314,10 @@ def test_block_pattern_built_on_the_device_equals_the_host_build(box_mesh):
         kf.set_ilu_order(0)
         m = kf.Mesh(path)
         assert m.query("pattern_matches_host") == 1, path
-        assert m.query("spatial_pattern_matches_host") == -1, path   # not built yet
+        assert m.query("lists_match_host") == 1, path
+        with pytest.raises(RuntimeError):   # not built yet: the query answers -1
+            m.query("spatial_pattern_matches_host")
+        kf.clear_status()
         kf.set_ilu_order(1)
         m.flux(m.view.q.copy())    # the first entry point in the spatial order builds it
         assert m.query("spatial_pattern_matches_host") == 1, path
