@@ -288,11 +288,15 @@ MatrixHandle *kf_handle(const GEOMETRY *g)
     }                                                                             \
   } while (0)
 
+// A copy from pageable host memory may return before its last DMA has
+// landed; the wait makes the data safe for kernels on the mirror's own
+// (non-blocking) stream.
 template <class T> static cudaError_t upload(T **dst, const T *src, size_t n)
 {
   cudaError_t e = cudaMalloc((void **)dst, std::max<size_t>(n, 1) * sizeof(T));
   if (e != cudaSuccess || n == 0) return e;
-  return cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+  e = cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? cudaStreamSynchronize(cudaStreamLegacy) : e;
 }
 
 void kf_ilu_release(DevMesh &m);
@@ -316,42 +320,73 @@ void kf_free_packed(PackedSweep pk[2])
 // Each level's slots are cut into chunks, one CTA each, twice: at most 32 rows
 // and 256 blocks, and at most 64 rows and 512 blocks.  KFUN3D_ERR_ARG (and
 // nothing allocated) when a row has more than KF_PK_ROW_MAX blocks.
+// (f(i) for every i in [0, n), interleaved over the host's threads: for
+// items of uneven size, such as levels)
+template <class F> static void parallel_items(size_t n, size_t work, F f)
+{
+  const unsigned T = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  if (work < 65536 || T == 1 || n < 2) {
+    for (size_t i = 0; i < n; i++) f(i);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < T; t++)
+    th.emplace_back([&, t] {
+      for (size_t i = t; i < n; i += T) f(i);
+    });
+  for (auto &x : th) x.join();
+}
+
+void kf_level_descriptors(const HostPattern &p, std::vector<uint4> &dl, std::vector<uint4> &du)
+{
+  const size_t N = p.n;
+  dl.resize(N);
+  du.resize(N);
+  parallel_ranges(N, [&](size_t a, size_t b) {
+    for (size_t q = a; q < b; q++) {
+      const uint32_t i = p.lev_l[q];
+      dl[q] = make_uint4(i, p.ia[i], p.diag[i], 0);
+      const uint32_t k = p.lev_u[q];
+      du[q] = make_uint4(k, p.diag[k] + 1, p.ia[k + 1], 0);
+    }
+  });
+  auto by_length = [N](std::vector<uint4> &d, const std::vector<uint32_t> &ptr) {
+    parallel_items(ptr.size() - 1, N, [&](size_t l) {
+      std::stable_sort(d.begin() + ptr[l], d.begin() + ptr[l + 1],
+                       [](const uint4 &a, const uint4 &b) { return a.z - a.y > b.z - b.y; });
+    });
+  };
+  by_length(dl, p.lev_l_ptr);
+  by_length(du, p.lev_u_ptr);
+}
+
 int kf_build_packed(PackedSweep pk[2], const HostPattern &p, const std::vector<uint4> &desc_l,
-                    const std::vector<uint4> &desc_u)
+                    const std::vector<uint4> &desc_u, const uint4 *ddesc_l, const uint4 *ddesc_u,
+                    const uint32_t *ja, const uint32_t *diag, cudaStream_t st)
 {
   const size_t N = p.n;
   for (int sw = 0; sw < 2; sw++) {
     const std::vector<uint4> &d = sw == 0 ? desc_l : desc_u;
     const std::vector<uint32_t> &lp = sw == 0 ? p.lev_l_ptr : p.lev_u_ptr;
-    std::vector<uint32_t> row(N), first(N + 1), col, src;
+    std::vector<uint32_t> first(N + 1);
     size_t nblk = 0;
     for (size_t s = 0; s < N; s++) {
       const size_t len = (d[s].z - d[s].y) + (sw == 1 ? 1u : 0u);
       if (len > KF_PK_ROW_MAX) { kf_free_packed(pk); return KFUN3D_ERR_ARG; }
+      first[s] = (uint32_t)std::min<size_t>(nblk, 0xffffffffu);
       nblk += len;
     }
     if (nblk >= 0xffffffffu) { kf_free_packed(pk); return KFUN3D_ERR_ARG; }
-    col.resize(nblk);
-    src.resize(nblk);
-    size_t k = 0;
-    for (size_t s = 0; s < N; s++) {
-      const uint4 ds = d[s];
-      row[s] = ds.x;
-      first[s] = (uint32_t)k;
-      if (sw == 1) {
-        col[k] = ds.x;
-        src[k++] = p.diag[ds.x];
-      }
-      for (uint32_t j = ds.y; j < ds.z; j++) {
-        col[k] = p.ja[j];
-        src[k++] = j;
-      }
-    }
-    first[N] = (uint32_t)k;
+    first[N] = (uint32_t)nblk;
     PackedSweep &o = pk[sw];
     o.nblk = (uint32_t)nblk;
-    bool ok = upload(&o.row, row.data(), N) == cudaSuccess && upload(&o.first, first.data(), N + 1) == cudaSuccess &&
-              upload(&o.col, col.data(), nblk) == cudaSuccess && upload(&o.src, src.data(), nblk) == cudaSuccess;
+    // the streams (slot rows, block columns, source blocks) written on the device
+    bool ok = upload(&o.first, first.data(), N + 1) == cudaSuccess &&
+              cudaMalloc(&o.row, std::max<size_t>(N, 1) * sizeof(uint32_t)) == cudaSuccess &&
+              cudaMalloc(&o.col, std::max<size_t>(nblk, 1) * sizeof(uint32_t)) == cudaSuccess &&
+              cudaMalloc(&o.src, std::max<size_t>(nblk, 1) * sizeof(uint32_t)) == cudaSuccess;
+    ok = ok && kf_packed_streams_device((uint32_t)N, sw == 1, sw == 0 ? ddesc_l : ddesc_u, o.first, ja, diag, o.row,
+                                        o.col, o.src, st) == KFUN3D_OK;
     for (int cut = 0; cut < 2 && ok; cut++) {
       const uint32_t rows = cut == 0 ? 32u : 64u, budget = 8u * rows;
       std::vector<uint4> chunk;
@@ -372,6 +407,7 @@ int kf_build_packed(PackedSweep pk[2], const HostPattern &p, const std::vector<u
       o.maxblk[cut] = maxblk;
       ok = upload(&o.chunk[cut], chunk.data(), chunk.size()) == cudaSuccess;
     }
+    if (ok) ok = cudaStreamSynchronize(st) == cudaSuccess;
     if (!ok) {
       cudaGetLastError();
       kf_free_packed(pk);
@@ -828,29 +864,15 @@ DevMesh *kf_device(const GEOMETRY *g)
     m->trsv_mgrid = (unsigned)nsm * (unsigned)m->trsv_mgrid_per;
     const char *lenv = getenv("KFUN3D_SPTRSV_LANES");   // lanes per row: 8 (default), 4 or 16
     if (lenv && (atoi(lenv) == 4 || atoi(lenv) == 8 || atoi(lenv) == 16)) m->trsv_lanes = atoi(lenv);
-    std::vector<uint4> dl(N), du(N);
-    for (uint32_t s = 0; s < N; s++) {
-      const uint32_t i = lev_l[s];
-      dl[s] = make_uint4(i, p.ia[i], p.diag[i], 0);
-      const uint32_t k = lev_u[s];
-      du[s] = make_uint4(k, p.diag[k] + 1, p.ia[k + 1], 0);
-    }
-    // within a level the rows are independent: longest first, so that the
-    // groups that take a second row take short ones (less waiting at the
-    // level barrier)
-    auto by_length = [](std::vector<uint4> &d, const std::vector<uint32_t> &ptr) {
-      for (size_t l = 0; l + 1 < ptr.size(); l++)
-        std::stable_sort(d.begin() + ptr[l], d.begin() + ptr[l + 1],
-                         [](const uint4 &a, const uint4 &b) { return a.z - a.y > b.z - b.y; });
-    };
-    by_length(dl, p.lev_l_ptr);
-    by_length(du, p.lev_u_ptr);
+    std::vector<uint4> dl, du;
+    kf_level_descriptors(p, dl, du);
     KF_CUDA(upload(&m->desc_l, dl.data(), N));
     KF_CUDA(upload(&m->desc_u, du.data(), N));
     // the packed factor (room for FP64 blocks, shared by both ILU orders) and
     // this pattern's packed level schedule
     KF_CUDA(cudaMalloc(&m->pk_buf, 16 * (size_t)m->nnz * sizeof(double)));
-    const int pkrc = kf_build_packed(m->iset[0].pk, p, dl, du);   // ERR_ARG: rows too long, no packed schedule
+    // ERR_ARG: rows too long, no packed schedule
+    const int pkrc = kf_build_packed(m->iset[0].pk, p, dl, du, m->desc_l, m->desc_u, m->ja, m->diag, m->stream);
     if (pkrc == KFUN3D_ERR_CUDA) {
       kf_set_error(KFUN3D_ERR_CUDA, "device mirror: building the packed triangular-solve schedule failed");
       return nullptr;

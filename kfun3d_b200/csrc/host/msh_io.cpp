@@ -53,26 +53,50 @@ struct Writer {
   }
 };
 
+// f(begin, end) over [0, n) split across the host's threads (sequential for
+// small n); every index is handled by exactly one call.
+template <class F> void parallel_ranges(size_t n, F f)
+{
+  const unsigned T = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  if (n < 65536 || T == 1) {
+    f((size_t)0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t chunk = (n + T - 1) / T;
+  for (unsigned t = 0; t < T; t++) {
+    const size_t a = t * chunk, b = std::min(n, a + chunk);
+    if (a < b) th.emplace_back(f, a, b);
+  }
+  for (auto &x : th) x.join();
+}
+
 struct Reader {
   const unsigned char *p, *end;
   bool ok = true;
   void u32(uint32_t *a, size_t n) {
     if ((size_t)(end - p) < 4 * n) { ok = false; return; }
-    for (size_t i = 0; i < n; i++) {
-      uint32_t u;
-      memcpy(&u, p + 4 * i, 4);
-      a[i] = bswap32(u);
-    }
+    const unsigned char *src = p;
+    parallel_ranges(n, [&](size_t i0, size_t i1) {
+      for (size_t i = i0; i < i1; i++) {
+        uint32_t u;
+        memcpy(&u, src + 4 * i, 4);
+        a[i] = bswap32(u);
+      }
+    });
     p += 4 * n;
   }
   void f64(double *a, size_t n) {
     if ((size_t)(end - p) < 8 * n) { ok = false; return; }
-    for (size_t i = 0; i < n; i++) {
-      uint64_t u;
-      memcpy(&u, p + 8 * i, 8);
-      u = bswap64(u);
-      memcpy(a + i, &u, 8);
-    }
+    const unsigned char *src = p;
+    parallel_ranges(n, [&](size_t i0, size_t i1) {
+      for (size_t i = i0; i < i1; i++) {
+        uint64_t u;
+        memcpy(&u, src + 8 * i, 8);
+        u = bswap64(u);
+        memcpy(a + i, &u, 8);
+      }
+    });
     p += 8 * n;
   }
   void skip(size_t bytes) {
@@ -405,24 +429,6 @@ int sort_levels()
 
 template <class T> T *alloc(size_t n) { return (T *)calloc(n ? n : 1, sizeof(T)); }
 
-// f(begin, end) over [0, n) split across the host's threads (sequential for
-// small n); every index is handled by exactly one call.
-template <class F> void parallel_ranges(size_t n, F f)
-{
-  const unsigned T = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  if (n < 65536 || T == 1) {
-    f((size_t)0, n);
-    return;
-  }
-  std::vector<std::thread> th;
-  const size_t chunk = (n + T - 1) / T;
-  for (unsigned t = 0; t < T; t++) {
-    const size_t a = t * chunk, b = std::min(n, a + chunk);
-    if (a < b) th.emplace_back(f, a, b);
-  }
-  for (auto &x : th) x.join();
-}
-
 }  // namespace
 
 extern "C" GEOMETRY *kfun3d_setup_load(const char *path)
@@ -461,15 +467,17 @@ extern "C" GEOMETRY *kfun3d_setup_load(const char *path)
   g->e->xyzn = alloc<struct xyzn>(1);
   g->e->xyzn->x0 = alloc<double>(E); g->e->xyzn->x1 = alloc<double>(E);
   g->e->xyzn->x2 = alloc<double>(E); g->e->xyzn->x3 = alloc<double>(E);
-  for (size_t i = 0; i < E; i++) {
-    const uint32_t s = order[i];
-    g->e->eptr->n0[i] = ebuf[s] - 1;
-    g->e->eptr->n1[i] = ebuf[s + E] - 1;
-    g->e->xyzn->x0[i] = nbuf[s];
-    g->e->xyzn->x1[i] = nbuf[s + E];
-    g->e->xyzn->x2[i] = nbuf[s + 2 * E];
-    g->e->xyzn->x3[i] = nbuf[s + 3 * E];
-  }
+  parallel_ranges(E, [&](size_t i0, size_t i1) {
+    for (size_t i = i0; i < i1; i++) {
+      const uint32_t s = order[i];
+      g->e->eptr->n0[i] = ebuf[s] - 1;
+      g->e->eptr->n1[i] = ebuf[s + E] - 1;
+      g->e->xyzn->x0[i] = nbuf[s];
+      g->e->xyzn->x1[i] = nbuf[s + E];
+      g->e->xyzn->x2[i] = nbuf[s + 2 * E];
+      g->e->xyzn->x3[i] = nbuf[s + 3 * E];
+    }
+  });
   tr.mark("edges permuted");
   // nodes (src/nodes.c:19-56); the dual volume is read and dropped
   g->n = alloc<struct ntbl>(1);

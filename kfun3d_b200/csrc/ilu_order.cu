@@ -23,11 +23,13 @@
 
 namespace {
 
+// (waits for the copy to land: see device_mesh.cu's upload)
 template <class T> cudaError_t upload(T **dst, const T *src, size_t n)
 {
   cudaError_t e = cudaMalloc((void **)dst, std::max<size_t>(n, 1) * sizeof(T));
   if (e != cudaSuccess || n == 0) return e;
-  return cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+  e = cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? cudaStreamSynchronize(cudaStreamLegacy) : e;
 }
 
 template <class F> void parallel_ranges(size_t n, F f)
@@ -250,8 +252,11 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m.device);
   const uint32_t T = (uint32_t)std::max(1, nsm);
   SetupTrace tr("spatial order");
-  const std::vector<uint32_t> tile = partition_tiles(g->n->xyz->x0, g->n->xyz->x1, g->n->xyz->x2, N, T);
-  tr.mark("tiles");
+  // tiles only for the tile-major order
+  const char *perm = getenv("KFUN3D_ILU_PERM");
+  const std::vector<uint32_t> tile = perm && strcmp(perm, "tiles") == 0
+                                         ? partition_tiles(g->n->xyz->x0, g->n->xyz->x1, g->n->xyz->x2, N, T)
+                                         : std::vector<uint32_t>();
   const std::vector<uint32_t> rank = spatial_rank(g, N, tile);
   tr.mark("rank");
   std::vector<uint32_t> pn0(E), pn1(E);
@@ -280,60 +285,18 @@ int build_spatial(DevMesh &m, const GEOMETRY *g)
     up(&s.lev_ptr_d, lp);
   }
   {
-    std::vector<uint4> dl(N), du(N);
-    for (size_t q = 0; q < N; q++) {
-      const uint32_t i = p.lev_l[q];
-      dl[q] = make_uint4(i, p.ia[i], p.diag[i], 0);
-      const uint32_t k = p.lev_u[q];
-      du[q] = make_uint4(k, p.diag[k] + 1, p.ia[k + 1], 0);
-    }
-    auto by_length = [](std::vector<uint4> &d, const std::vector<uint32_t> &ptr) {
-      for (size_t l = 0; l + 1 < ptr.size(); l++)
-        std::stable_sort(d.begin() + ptr[l], d.begin() + ptr[l + 1],
-                         [](const uint4 &a, const uint4 &b) { return a.z - a.y > b.z - b.y; });
-    };
-    by_length(dl, p.lev_l_ptr);
-    by_length(du, p.lev_u_ptr);
+    std::vector<uint4> dl, du;
+    kf_level_descriptors(p, dl, du);
     up(&s.desc_l, dl);
     up(&s.desc_u, du);
-    if (ok && kf_build_packed(s.pk, p, dl, du) == KFUN3D_ERR_CUDA) ok = false;
+    if (ok && kf_build_packed(s.pk, p, dl, du, s.desc_l, s.desc_u, s.ja, s.diag, m.stream) == KFUN3D_ERR_CUDA)
+      ok = false;
   }
   tr.mark("level descriptors, packed schedule");
-  // the fill's view of the renumbered pattern, per node of the mesh
-  {
-    std::vector<uint32_t> inc_ptr(N + 1), inc_oth(2 * E), ord(N);
-    if (ok && cudaMemcpy(inc_ptr.data(), m.inc_ptr, (N + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
-      ok = false;
-    if (ok && cudaMemcpy(inc_oth.data(), m.inc_oth, 2 * E * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
-      ok = false;
-    if (ok && cudaMemcpy(ord.data(), m.ord, N * sizeof(uint32_t), cudaMemcpyDeviceToHost) != cudaSuccess) ok = false;
-    std::vector<uint32_t> blk(2 * E), fd(N), fl(N), fp(N);
-    if (ok) {
-      auto find = [&](uint32_t row, uint32_t col) -> uint32_t {
-        auto b = p.ja.begin() + p.ia[row], en = p.ja.begin() + p.ia[row + 1];
-        return (uint32_t)(std::lower_bound(b, en, col) - p.ja.begin());
-      };
-      parallel_ranges(N, [&](size_t r0, size_t r1) {
-        for (size_t row = r0; row < r1; row++) {
-          const uint32_t node = ord[row];
-          for (uint32_t k = inc_ptr[row]; k < inc_ptr[row + 1]; k++) blk[k] = find(rank[node], rank[inc_oth[k]]);
-        }
-      });
-      for (size_t i = 0; i < N; i++) {
-        fd[i] = p.diag[rank[i]];
-        fl[i] = p.last_lower[rank[i]];
-        fp[i] = p.lpos[rank[i]];
-      }
-    }
-    up(&s.fill_blk, blk);
-    up(&s.fill_diag, fd);
-    up(&s.fill_last, fl);
-    up(&s.fill_lpos, fp);
-    std::vector<uint32_t> rn(N);   // node of each renumbered row
-    for (size_t i = 0; i < N; i++) rn[rank[i]] = (uint32_t)i;
-    up(&s.row_node, rn);
-  }
+  // the fill's view of the renumbered pattern, per node of the mesh, and
+  // the node of each renumbered row (on the device)
   up(&m.ilu_rank, rank);
+  if (ok && kf_fill_targets_device(m, s) != KFUN3D_OK) ok = false;
   if (ok && cudaMalloc(&m.pb, 4 * N * sizeof(double)) != cudaSuccess) ok = false;
   if (ok && cudaMalloc(&m.px, 4 * N * sizeof(double)) != cudaSuccess) ok = false;
   // one launch per level (programmatic dependent launch, each CTA's rows one
@@ -423,7 +386,10 @@ extern "C" int kfun3d_ilu_order_plan(const GEOMETRY *g, unsigned int tiles, unsi
     return -1;
   }
   const size_t N = g->n->sz, E = g->e->sz;
-  const std::vector<uint32_t> tile = partition_tiles(g->n->xyz->x0, g->n->xyz->x1, g->n->xyz->x2, N, tiles);
+  const char *perm = getenv("KFUN3D_ILU_PERM");
+  const std::vector<uint32_t> tile = perm && strcmp(perm, "tiles") == 0
+                                         ? partition_tiles(g->n->xyz->x0, g->n->xyz->x1, g->n->xyz->x2, N, tiles)
+                                         : std::vector<uint32_t>();
   const std::vector<uint32_t> r = spatial_rank(g, N, tile);
   if (rank) std::copy(r.begin(), r.end(), rank);
   if (nlev_lower || nlev_upper) {

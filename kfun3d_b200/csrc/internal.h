@@ -174,11 +174,21 @@ struct IluSet {
   PackedSweep pk[2];               // packed level schedule (trsv_mode 8)
 };
 
+// Level-slot descriptors of both sweeps, (row, first block, end block, 0):
+// the lower sweep's blocks left of the diagonal, the upper sweep's right of
+// it; within a level the longest rows first (stable), so that the groups that
+// take a second row take short ones.
+void kf_level_descriptors(const HostPattern &p, std::vector<uint4> &desc_l, std::vector<uint4> &desc_u);
 // Builds the packed level schedule of one pattern from its level-slot
-// descriptors (row, first block, end block) and level offsets; KFUN3D_OK, or
-// an error code with nothing left allocated.
+// descriptors (host copies for the chunk cuts, device copies for the
+// streams) and level offsets; ja and diag are the pattern's device arrays.
+// KFUN3D_OK, KFUN3D_ERR_ARG (a row too long: no packed schedule) or
+// KFUN3D_ERR_CUDA, with nothing left allocated on error.
 int kf_build_packed(PackedSweep pk[2], const HostPattern &p, const std::vector<uint4> &desc_l,
-                    const std::vector<uint4> &desc_u);
+                    const std::vector<uint4> &desc_u, const uint4 *ddesc_l, const uint4 *ddesc_u,
+                    const uint32_t *ja, const uint32_t *diag, cudaStream_t st);
+int kf_packed_streams_device(uint32_t N, bool upper, const uint4 *desc, const uint32_t *first, const uint32_t *ja,
+                             const uint32_t *diag, uint32_t *row, uint32_t *col, uint32_t *src, cudaStream_t st);
 void kf_free_packed(PackedSweep pk[2]);
 
 // The block pattern built on the device (setup_device.cu): the device arrays,
@@ -201,6 +211,10 @@ void kf_free_device_pattern(DevPattern &d);
 // m.xyz, the block pattern, m.two_pass and m.visit are set before.  KFUN3D_OK
 // or an error code (the arrays made so far are the mirror's, freed with it).
 int kf_build_mesh_lists_device(DevMesh &m, const GEOMETRY *g);
+// The fill's targets in the renumbered pattern of `s` (fill_blk per
+// incidence, fill_diag / fill_last / fill_lpos per node, row_node per row),
+// from m.ilu_rank and the mirror's incidence lists, on the device.
+int kf_fill_targets_device(const DevMesh &m, IluSet &s);
 // 1 when every pattern array of `s` (on the device) and its level lists equal
 // kf_build_pattern's for the same edges, 0 when one differs, -1 on a CUDA error;
 // *host_us (if given) the host build's wall time in microseconds

@@ -368,6 +368,47 @@ __global__ void k_visit_nodes(uint32_t N, const uint32_t *__restrict__ ord, cons
   if (p < N) xv[p] = xyz[ord[p]];
 }
 
+// packed level schedule: the stream positions of slot s are [first[s],
+// first[s+1]): for the upper sweep the row's diagonal block first, then the
+// row's blocks of its descriptor's range, in column order
+__global__ void k_packed_streams(uint32_t N, bool upper, const uint4 *__restrict__ desc,
+                                 const uint32_t *__restrict__ first, const uint32_t *__restrict__ ja,
+                                 const uint32_t *__restrict__ diag, uint32_t *row, uint32_t *col, uint32_t *src)
+{
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= N) return;
+  const uint4 d = desc[q];
+  uint32_t k = first[q];
+  row[q] = d.x;
+  if (upper) {
+    col[k] = d.x;
+    src[k++] = diag[d.x];
+  }
+  for (uint32_t j = d.y; j < d.z; j++) {
+    col[k] = ja[j];
+    src[k++] = j;
+  }
+}
+
+// the fill's view of a renumbered pattern, per incidence (visit row p, node
+// ord[p]) and per node of the mesh
+__global__ void k_fill_targets(uint32_t N, const uint32_t *__restrict__ ord, const uint32_t *__restrict__ rank,
+                               const uint32_t *__restrict__ inc_ptr, const uint32_t *__restrict__ inc_oth,
+                               const uint32_t *__restrict__ ia, const uint32_t *__restrict__ ja,
+                               const uint32_t *__restrict__ diag, const uint32_t *__restrict__ last_lower,
+                               const uint32_t *__restrict__ lpos, uint32_t *blk, uint32_t *fd, uint32_t *fl,
+                               uint32_t *fp, uint32_t *row_node)
+{
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const uint32_t node = ord[p], r = rank[node];
+  for (uint32_t k = inc_ptr[p]; k < inc_ptr[p + 1]; k++) blk[k] = find_col(ja, ia[r], ia[r + 1], rank[inc_oth[k]]);
+  fd[node] = diag[r];
+  fl[node] = last_lower[r];
+  fp[node] = lpos[r];
+  row_node[r] = node;
+}
+
 // rows listed by level in row order from their depths (counting sort)
 void levels_from_depth(const std::vector<uint32_t> &depth, std::vector<uint32_t> &rows, std::vector<uint32_t> &ptr)
 {
@@ -710,6 +751,47 @@ int kf_build_mesh_lists_device(DevMesh &m, const GEOMETRY *g)
     if (t) cudaFree(t);
   if (!ok) {
     kf_set_error(KFUN3D_ERR_CUDA, "device mirror: building the incidence lists on the device failed");
+    return KFUN3D_ERR_CUDA;
+  }
+  return KFUN3D_OK;
+}
+
+int kf_packed_streams_device(uint32_t N, bool upper, const uint4 *desc, const uint32_t *first, const uint32_t *ja,
+                             const uint32_t *diag, uint32_t *row, uint32_t *col, uint32_t *src, cudaStream_t st)
+{
+  if (N) {
+    k_packed_streams<<<nblk(N, 256), 256, 0, st>>>(N, upper, desc, first, ja, diag, row, col, src);
+    kf_count_launch();
+  }
+  return cudaGetLastError() == cudaSuccess ? KFUN3D_OK : KFUN3D_ERR_CUDA;
+}
+
+int kf_fill_targets_device(const DevMesh &m, IluSet &s)
+{
+  const uint32_t N = m.N;
+  const size_t ninc = 2 * (size_t)m.E;
+  bool ok = true;
+  auto ck = [&](cudaError_t e) {
+    if (e != cudaSuccess && ok) {
+      ok = false;
+      cudaGetLastError();
+    }
+  };
+  ck(cudaMalloc(&s.fill_blk, (ninc + 1) * sizeof(uint32_t)));
+  ck(cudaMalloc(&s.fill_diag, ((size_t)N + 1) * sizeof(uint32_t)));
+  ck(cudaMalloc(&s.fill_last, ((size_t)N + 1) * sizeof(uint32_t)));
+  ck(cudaMalloc(&s.fill_lpos, ((size_t)N + 1) * sizeof(uint32_t)));
+  ck(cudaMalloc(&s.row_node, ((size_t)N + 1) * sizeof(uint32_t)));
+  if (ok && N) {
+    k_fill_targets<<<nblk(N, 128), 128, 0, m.stream>>>(N, m.ord, m.ilu_rank, m.inc_ptr, m.inc_oth, s.ia, s.ja,
+                                                       s.diag, s.last_lower, s.lpos, s.fill_blk, s.fill_diag,
+                                                       s.fill_last, s.fill_lpos, s.row_node);
+    kf_count_launch();
+    ck(cudaGetLastError());
+  }
+  ck(cudaStreamSynchronize(m.stream));
+  if (!ok) {
+    kf_set_error(KFUN3D_ERR_CUDA, "spatial ILU(0) order: fill targets on the device failed");
     return KFUN3D_ERR_CUDA;
   }
   return KFUN3D_OK;
