@@ -709,7 +709,7 @@ DevMesh *kf_device(const GEOMETRY *g)
         }
         key[i] = k;
       }
-      std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+      kf_sort_by_key(ord, key);
     }
     KF_CUDA(upload(&m->ord, ord.data(), N));
     std::vector<uint32_t> rowof(N);

@@ -215,7 +215,7 @@ std::vector<uint32_t> spatial_rank(const GEOMETRY *g, size_t N, const std::vecto
       }
       key[i] = k;
     }
-    std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+    kf_sort_by_key(ord, key);
   } else {
     std::vector<double> key(N);
     for (size_t i = 0; i < N; i++) key[i] = (X[i] + Y[i]) + Z[i];
@@ -236,7 +236,7 @@ std::vector<uint32_t> spatial_rank(const GEOMETRY *g, size_t N, const std::vecto
           key[i] = -std::fabs(key[i] - (lo + (sl + 0.5) * w));
         }
       }
-      std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+      kf_sort_by_key(ord, key);
     }
   }
   for (size_t p = 0; p < N; p++) rank[ord[p]] = (uint32_t)p;

@@ -6,7 +6,9 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <memory>
+#include <thread>
 #include <vector>
 
 #include "kfun3d_b200.h"
@@ -18,6 +20,42 @@ struct double4_host { double x, y, z, w; };
 #endif
 
 void kf_set_error(int code, const char *msg);
+
+// ord = 0 .. n-1 ordered by key, ties by index (what a stable sort by key
+// gives), on the host's threads: chunks sorted under that total order, then
+// merged pairwise.
+template <class K> void kf_sort_by_key(std::vector<uint32_t> &ord, const std::vector<K> &key)
+{
+  const size_t n = key.size();
+  ord.resize(n);
+  for (size_t i = 0; i < n; i++) ord[i] = (uint32_t)i;
+  auto less = [&key](uint32_t a, uint32_t b) { return key[a] < key[b] || (!(key[b] < key[a]) && a < b); };
+  unsigned T = 1;
+  while (T * 2 <= std::min(16u, std::thread::hardware_concurrency())) T *= 2;
+  if (n < 65536 || T == 1) {
+    std::sort(ord.begin(), ord.end(), less);
+    return;
+  }
+  std::vector<size_t> cut(T + 1);
+  for (unsigned t = 0; t <= T; t++) cut[t] = n * t / T;
+  {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < T; t++)
+      th.emplace_back([&, t] { std::sort(ord.begin() + cut[t], ord.begin() + cut[t + 1], less); });
+    for (auto &x : th) x.join();
+  }
+  std::vector<uint32_t> tmp(n);
+  for (unsigned w = 1; w < T; w *= 2) {
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < T; t += 2 * w)
+      th.emplace_back([&, t] {
+        std::merge(ord.begin() + cut[t], ord.begin() + cut[t + w], ord.begin() + cut[t + w],
+                   ord.begin() + cut[t + 2 * w], tmp.begin() + cut[t], less);
+      });
+    for (auto &x : th) x.join();
+    ord.swap(tmp);
+  }
+}
 
 // Set-up phase trace: with KFUN3D_SETUP_TRACE=1 in the environment, each
 // mark() prints to stderr the host wall time since the tracer's previous mark.

@@ -197,6 +197,18 @@ def test_plan_on_the_host(box_mesh, perm, monkeypatch):
     assert nu == _depth(v.n0, v.n1, N - 1 - rank)
 
 
+@pytest.mark.parametrize("perm", ["sweep", "morton"])
+def test_plan_threaded_sort_on_a_large_mesh(box_mesh, perm, monkeypatch):
+    """42^3 (74,088 nodes) sorts on several host threads (chunks sorted, then
+    merged pairwise, ties by node index); the order must still be exactly the
+    stable sort restated above."""
+    monkeypatch.setenv("KFUN3D_ILU_PERM", perm)
+    m = kf.Mesh(box_mesh(42, seed=13))
+    rank, _, _ = m.ilu_order_plan()
+    xyz = [c.copy() for c in m.view.xyz]
+    assert np.array_equal(rank, sweep_rank(xyz) if perm == "sweep" else morton_rank(xyz))
+
+
 def test_plan_slab_sweeps_have_fewer_levels(box_mesh, monkeypatch):
     m = kf.Mesh(box_mesh(20, seed=37))
     _, nl_slabs, _ = m.ilu_order_plan()
