@@ -579,13 +579,45 @@ def run_network_probe(args, cfg, kf, m):
             "loss_first": losses[0], "loss_last": losses[-1]}
 
 
+def run_setup_probe(cfg, kf, path):
+    """--kernel setup: the set-up of the workload's mesh, host wall time per
+    stage: the .msh load (reference-order GEOMETRY), the device mirror (block
+    pattern, incidence lists and edge storage built on the device), the
+    spatial ILU(0) order's set (built by the first entry point that runs in
+    it), and the same block pattern built on the host threads for comparison.
+    CUDA's own start-up is paid before the timers start."""
+    import torch
+    if torch.cuda.is_available():
+        torch.zeros(1, device="cuda")
+    t0 = time.perf_counter()
+    m = kf.Mesh(path)
+    t1 = time.perf_counter()
+    m.query("setup_us")                  # builds the device mirror
+    t2 = time.perf_counter()
+    m.flux(m.view.q.copy())              # the first entry point builds the workload's ILU(0) order
+    t3 = time.perf_counter()
+    us = lambda k: m.query(k) / 1e6      # noqa: E731
+    out = {"kernel": "setup", "config": cfg["workload"], "load_s": t1 - t0, "mirror_s": t2 - t1,
+           "first_flux_s": t3 - t2, "mirror_in_library_s": us("setup_us"), "pattern_on_device_s": us("pattern_us"),
+           "spatial_order_s": us("spatial_setup_us") if cfg.get("ilu_order", 0) else 0.0}
+    out["pattern_matches_host"] = m.query("pattern_matches_host") == 1
+    out["pattern_on_host_threads_s"] = us("host_pattern_us")
+    out["lists_match_host"] = m.query("lists_match_host") == 1
+    m.close()
+    return out
+
+
 def run_kernel_probe(args, cfg):
     """--kernel NAME: time one kernel family `reps` times on the workload's mesh
     and print {"kernel", "ms", "gbs"} -- the command the profiles use to
     capture a single kernel under ncu."""
     import kfun3d_b200 as kf
     configure(kf, cfg)
-    m = kf.Mesh(mesh_path(cfg))
+    path = mesh_path(cfg)
+    if args.kernel == "setup":
+        print(json.dumps(run_setup_probe(cfg, kf, path)))
+        return
+    m = kf.Mesh(path)
     if args.kernel in ("mpnn_apply", "mpnn_train"):
         print(json.dumps(run_network_probe(args, cfg, kf, m)))
         m.close()
@@ -611,7 +643,7 @@ def main():
                          "(default: the reference's own count from its full run, tests/golden/)")
     ap.add_argument("--kernel", default=None,
                     help="time one kernel family (flux, gradient, edge_flux, timestep, fill, ilu, sptrsv, mgs, "
-                         "gmres_iter, mpnn_apply, mpnn_train) instead of the solve")
+                         "gmres_iter, mpnn_apply, mpnn_train) or the set-up (setup) instead of the solve")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--n", type=int, default=None,
                     help="with --kernel: mesh of n^3 nodes instead of the workload's (same seed and bump)")
