@@ -901,9 +901,26 @@ int upload_tables(int device)
 template <class K>
 unsigned persistent_grid(K kernel, size_t smem, int nsm, int cap)
 {
-  int per = 0;
+  // CTAs of 128 threads an SM holds, from the kernel's registers (allocated
+  // in units of 8 a thread) and shared memory (with the per-CTA reserve),
+  // at most `cap` (the SM's 512 TMEM columns).  The occupancy query answers
+  // one CTA an SM for these kernels, so the count is formed here; a grid
+  // larger than what is resident would still be correct (every CTA loops
+  // over its tiles on its own, and a TMEM allocation waits for a free one).
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 128, smem);
+  cudaFuncAttributes fa{};
+  int dev = 0, regs_sm = 65536, smem_sm = 0, reserve = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  cudaDeviceGetAttribute(&reserve, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+  int per = 1;
+  if (cudaFuncGetAttributes(&fa, kernel) == cudaSuccess && fa.numRegs > 0) {
+    const int by_regs = regs_sm / (((fa.numRegs + 7) / 8) * 8 * 128);
+    const int by_smem = smem_sm / (int)(smem + fa.sharedSizeBytes + (size_t)reserve);
+    per = std::min(by_regs, by_smem);
+  }
+  cudaGetLastError();
   per = std::max(1, std::min(per, cap));
   return (unsigned)(nsm * per);
 }
