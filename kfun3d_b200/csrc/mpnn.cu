@@ -127,6 +127,11 @@ struct GraphDev {
   uint32_t *oth = nullptr;     // [R] sending node j
   uint32_t *rev = nullptr;     // [R] row of (j <- i)
   uint2 *efeat = nullptr;      // [R] BF16 (n_x, n_y, n_z, a / mean a) seen from i
+  // tiles of whole nodes for the edge MLP with the message sum in its
+  // epilogue: (first row, rows <= 128, first node, nodes); null when a node
+  // has more than 128 rows
+  uint4 *plan = nullptr;
+  uint32_t nplan = 0;
 };
 
 // ------------------------------------------------------------ gathers (X rows)
@@ -220,6 +225,20 @@ struct OutBf16 {   // rows of 32 BF16
   }
 };
 
+// The edge MLP's messages summed per receiving node inside the tile (tiles of
+// whole nodes, OutSegSum::plan): each row's message rounded to BF16, then per
+// node and component the FP32 sum over the node's rows in row order from
+// zero, rounded to BF16 -- what GatherNode forms from stored messages, so the
+// node MLP reads the sums (agg_in) and the messages never reach memory.
+struct OutSegSum {
+  const uint4 *plan;        // per tile: (first row, rows, first node, nodes)
+  const uint32_t *seg;      // [N+1] first row of each node
+  uint16_t *agg;            // [N][32] BF16
+  uint32_t ntiles;
+};
+template <class O> struct SegSum { static constexpr bool value = false; };
+template <> struct SegSum<OutSegSum> { static constexpr bool value = true; };
+
 struct OutResidual {   // dst = BF16(src + v)
   const uint4 *src;
   uint4 *dst;
@@ -290,13 +309,24 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(G gat, O out, uint32_t rows, co
   const uint32_t tm = tslot;
   const uint32_t lane = (uint32_t)(warp * 32) << 16;
   uint32_t phase = 0;
-  const uint32_t ntiles = (rows + 127) / 128;
+  constexpr bool SEG = SegSum<O>::value;
+  uint32_t ntiles = (rows + 127) / 128;
+  if constexpr (SEG) ntiles = out.ntiles;
+  // a tile's first row and row count (SEG: the plan's tiles of whole nodes)
+  auto span = [&](uint32_t tile) -> uint2 {
+    if constexpr (SEG) {
+      const uint4 pl = out.plan[tile];
+      return make_uint2(pl.x, pl.y);
+    }
+    const uint32_t r0 = tile * 128;
+    return make_uint2(r0, rows - r0 < 128u ? rows - r0 : 128u);
+  };
   // the next tile's rows are gathered into registers while this tile's GEMMs
   // and epilogues run (software pipeline of depth one)
   uint4 c[K1 / 8];
   auto gather = [&](uint32_t tile) {
-    const uint32_t r = tile * 128 + t;
-    if (tile < ntiles && r < rows) gat.load(r, c);
+    const uint2 sp = tile < ntiles ? span(tile) : make_uint2(0, 0);
+    if ((uint32_t)t < sp.y) gat.load(sp.x + t, c);
     else {
 #pragma unroll
       for (int k = 0; k < K1 / 8; k++) c[k] = make_uint4(0, 0, 0, 0);
@@ -304,8 +334,9 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(G gat, O out, uint32_t rows, co
   };
   gather(blockIdx.x);
   for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const uint32_t row = tile * 128 + t;
-    const bool valid = row < rows;
+    const uint2 sp = span(tile);
+    const uint32_t row = sp.x + t;
+    const bool valid = (uint32_t)t < sp.y;
 #pragma unroll
     for (int k = 0; k < K1 / 8; k++) st_chunk(Xs, t, k, K1, c[k]);
     fence_proxy_async();
@@ -337,7 +368,31 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(G gat, O out, uint32_t rows, co
       float v[32];
       if (N2 == 32) tmem_ld32(tm + lane + 32, v);
       else tmem_ld16(tm + lane + 32, v);
-      if (valid) out.store(row, v);
+      if constexpr (SEG) {
+        // the row's message rounded to BF16, staged in the X tile (free: the
+        // first GEMM has completed and the next tile's rows are in registers)
+        float *S = reinterpret_cast<float *>(Xs);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          float f[8];
+          unpack8(pack8(v + 8 * k), f);
+#pragma unroll
+          for (int u = 0; u < 8; u++) S[32 * t + 8 * k + u] = f[u];
+        }
+        __syncthreads();
+        const uint4 pl = out.plan[tile];
+        const int l32 = t & 31;
+        for (uint32_t j = (uint32_t)warp; j < pl.w; j += 4) {   // warp per node, lane per component
+          const uint32_t node = pl.z + j;
+          const uint32_t r0 = out.seg[node] - pl.x, r1 = out.seg[node + 1] - pl.x;
+          float sum = 0.f;
+          for (uint32_t r = r0; r < r1; r++) sum += S[32 * r + l32];
+          const __nv_bfloat16 bsum = __float2bfloat16_rn(sum);
+          out.agg[32 * (size_t)node + l32] = *reinterpret_cast<const uint16_t *>(&bsum);
+        }
+      } else {
+        if (valid) out.store(row, v);
+      }
     }
     sync_tc();
     if (s_abort) break;
@@ -934,7 +989,8 @@ int launch_fwd(kfun3d_mpnn *net, G g, O o, uint32_t rows, int layer, uint4 *a1_s
   static unsigned grid_cache[64] = {0};
   unsigned &gc = grid_cache[net->device & 63];
   if (!gc) gc = persistent_grid(kern, smem, net->nsm, 8);   // 64 TMEM columns per CTA: 8 fill the SM's 512
-  const unsigned ntiles = (rows + 127) / 128;
+  unsigned ntiles = (rows + 127) / 128;
+  if constexpr (SegSum<O>::value) ntiles = o.ntiles;
   const unsigned grid = std::min(gc, ntiles);
   const uint4 *W1 = reinterpret_cast<const uint4 *>(net->W + kOff.off[layer]);
   const uint4 *W2 = reinterpret_cast<const uint4 *>(net->W + kOff.off[layer + 1]);
@@ -987,6 +1043,7 @@ int ensure_workspace(kfun3d_mpnn *net, const GraphDev &g, bool train)
   bool ok = true;
   for (int k = 0; k < 4; k++) ok &= net->h[k].need(N * 64) == cudaSuccess;
   ok &= net->msg.need(R * 64) == cudaSuccess;
+  ok &= net->agg[0].need(N * 64) == cudaSuccess;   // the fused edge MLP's sums
   ok &= net->x0.need(N * 16) == cudaSuccess;
   ok &= net->out.need(N * 16) == cudaSuccess;
   if (train) {
@@ -1019,11 +1076,19 @@ int forward(kfun3d_mpnn *net, const GraphDev &g, const uint4 *x0, bool train, co
   auto H = [&](int l) { return train ? h[l] : h[l & 1]; };
   rc = launch_fwd<16, 32>(net, GatherEnc{x0}, OutBf16{H(0)}, g.N, L_ENC1, train ? net->a1_enc.as<uint4>() : nullptr,
                           st);
+  // inference with a tile plan: the message sums formed in the edge MLP
+  const bool fused = !train && g.plan && g.nplan;
   for (int l = 0; l < 3 && !rc; l++) {
-    rc = launch_fwd<80, 32>(net, GatherEdge{H(l), g.rnode, g.oth, g.efeat}, OutBf16{net->msg.as<uint4>()}, g.R,
-                            L_EDGE1(l), train ? net->a1_edge[l].as<uint4>() : nullptr, st);
+    if (fused)
+      rc = launch_fwd<80, 32>(net, GatherEdge{H(l), g.rnode, g.oth, g.efeat},
+                              OutSegSum{g.plan, g.seg, net->agg[0].as<uint16_t>(), g.nplan}, g.R, L_EDGE1(l),
+                              nullptr, st);
+    else
+      rc = launch_fwd<80, 32>(net, GatherEdge{H(l), g.rnode, g.oth, g.efeat}, OutBf16{net->msg.as<uint4>()}, g.R,
+                              L_EDGE1(l), train ? net->a1_edge[l].as<uint4>() : nullptr, st);
     if (rc) break;
-    GatherNode gn{H(l), g.seg, net->msg.as<uint4>(), train ? net->agg[l].as<uint4>() : nullptr, nullptr};
+    GatherNode gn{H(l), g.seg, fused ? nullptr : net->msg.as<uint4>(), train ? net->agg[l].as<uint4>() : nullptr,
+                  fused ? net->agg[0].as<uint4>() : nullptr};
     rc = launch_fwd<80, 32>(net, gn, OutResidual{H(l), H(l + 1)}, g.N, L_NODE1(l),
                             train ? net->a1_node[l].as<uint4>() : nullptr, st);
   }
@@ -1281,6 +1346,24 @@ extern "C" kfun3d_mpnn_graph *kfun3d_mpnn_graph_create(const GEOMETRY *g)
   up(G->d.oth, oth);
   up(G->d.rev, rev);
   up(G->d.efeat, ef);
+  // tiles of whole nodes, at most 128 rows each, in node order
+  // (KFUN3D_MPNN_FUSED=0: none, the messages go through memory)
+  const char *fenv = getenv("KFUN3D_MPNN_FUSED");
+  if (!(fenv && strcmp(fenv, "0") == 0)) {
+    std::vector<uint4> plan;
+    bool fits = true;
+    for (uint32_t i = 0; i < N && fits; ) {
+      if (seg[i + 1] - seg[i] > 128u) fits = false;
+      uint32_t j = i;
+      while (j < N && seg[j + 1] - seg[i] <= 128u) j++;
+      if (fits) plan.push_back(make_uint4(seg[i], seg[j] - seg[i], i, j - i));
+      i = j;
+    }
+    if (fits && !plan.empty()) {
+      up(G->d.plan, plan);
+      G->d.nplan = (uint32_t)plan.size();
+    }
+  }
   if (!ok) {
     kf_set_error(KFUN3D_ERR_CUDA, "kfun3d_mpnn_graph_create: out of device memory");
     kfun3d_mpnn_graph_free(G);
@@ -1293,7 +1376,8 @@ extern "C" void kfun3d_mpnn_graph_free(kfun3d_mpnn_graph *G)
 {
   if (!G) return;
   cudaSetDevice(G->device);
-  for (void *p : {(void *)G->d.seg, (void *)G->d.rnode, (void *)G->d.oth, (void *)G->d.rev, (void *)G->d.efeat})
+  for (void *p : {(void *)G->d.seg, (void *)G->d.rnode, (void *)G->d.oth, (void *)G->d.rev, (void *)G->d.efeat,
+                  (void *)G->d.plan})
     if (p) cudaFree(p);
   delete G;
 }
