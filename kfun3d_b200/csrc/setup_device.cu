@@ -25,6 +25,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <cstring>
+#include <thread>
 #include <vector>
 
 #include "internal.h"
@@ -32,6 +34,64 @@
 namespace {
 
 inline unsigned nblk(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// Host-to-device copies of large pageable arrays through pinned staging
+// buffers: the host's threads fill one buffer while the copies of the
+// previous ones run.  A copy the driver makes from pageable memory goes
+// through one thread's memcpy into its own staging area, which bounds it to
+// a few GB/s.  The buffers live as long as the object (one set-up).
+struct Stager {
+  static constexpr int K = 4;
+  static constexpr size_t CHUNK = 4u << 20;
+  void *buf[K] = {};
+  cudaEvent_t ev[K] = {};
+  bool used[K] = {};
+  int next = 0;
+  bool ok = false;
+  Stager()
+  {
+    ok = true;
+    for (int b = 0; b < K && ok; b++)
+      ok = cudaMallocHost(&buf[b], CHUNK) == cudaSuccess && cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) cudaGetLastError();
+  }
+  ~Stager()
+  {
+    for (int b = 0; b < K; b++) {
+      if (ev[b]) { cudaEventSynchronize(ev[b]); cudaEventDestroy(ev[b]); }
+      if (buf[b]) cudaFreeHost(buf[b]);
+    }
+  }
+  // dst (device) = src (host), stream-ordered on st; false on a CUDA error
+  bool copy(void *dst, const void *src, size_t bytes, cudaStream_t st)
+  {
+    if (!ok) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
+    const unsigned T = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    for (size_t off = 0; off < bytes; off += CHUNK) {
+      const size_t len = std::min(CHUNK, bytes - off);
+      const int b = next;
+      next = (next + 1) % K;
+      if (used[b] && cudaEventSynchronize(ev[b]) != cudaSuccess) return false;   // its previous copy has landed
+      char *d = (char *)buf[b];
+      const char *sp = (const char *)src + off;
+      if (len < (1u << 20) || T == 1) {
+        memcpy(d, sp, len);
+      } else {
+        std::vector<std::thread> th;
+        const size_t part = (len + T - 1) / T;
+        for (unsigned t = 0; t < T; t++) {
+          const size_t a = t * part, e = std::min(len, a + part);
+          if (a < e) th.emplace_back([=] { memcpy(d + a, sp + a, e - a); });
+        }
+        for (auto &x : th) x.join();
+      }
+      if (cudaMemcpyAsync((char *)dst + off, d, len, cudaMemcpyHostToDevice, st) != cudaSuccess) return false;
+      if (cudaEventRecord(ev[b], st) != cudaSuccess) return false;
+      used[b] = true;
+    }
+    return true;
+  }
+};
 
 __global__ void k_pat_count(uint32_t E, const uint32_t *__restrict__ n0, const uint32_t *__restrict__ n1,
                             uint32_t *cnt)
@@ -639,8 +699,9 @@ int kf_build_mesh_lists_device(DevMesh &m, const GEOMETRY *g)
       cudaGetLastError();
     }
   };
+  Stager sg;
   auto up = [&](void *dst, const void *src, size_t bytes) {
-    if (ok && bytes) ck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    if (ok && bytes && !sg.copy(dst, src, bytes, st)) ck(cudaErrorUnknown);
   };
   const size_t E1 = (size_t)E + 1, N1 = (size_t)N + 1;
   ck(cudaMalloc(&dn0, E1 * sizeof(uint32_t)));
