@@ -405,6 +405,7 @@ void kfun3d_reset_launch_count_by(unsigned long long n);   // undo counts taken 
   void fill(DevMesh &m, const double *q, double u, double v, int precision);            \
   void ilu(DevMesh &m, int precision);                                                  \
   void sptrsv(DevMesh &m, const double *b, double *x, int precision);                   \
+  bool sptrsv_permuted(DevMesh &m, const double *b, double *x, int precision);         \
   void sptrsv_flags(DevMesh &m, const double *b, double *x, int precision, uint32_t *flags); \
   int lsq_setup(DevMesh &m);                                                            \
   void gradient_to_mesh_order(DevMesh &m);                                              \

@@ -1876,13 +1876,17 @@ __device__ __forceinline__ void block_row(const double *a, double &a0, double &a
 // each product summed from zero in component order as the reference does.
 // The upper sweep then applies the inverted diagonal block (the first block
 // of the row's run).  The chunk's blocks in shared memory: 16 T each, then
-// their columns.
+// their columns.  With perm (matrix row -> mesh node, a renumbered pattern)
+// the lower sweep reads b at the row's node and the upper sweep also writes
+// the row's result at its node into xout: the permutations of the right-hand
+// side and of the solution without passes of their own.
 template <typename T, bool UPPER, int ROWS>
 __global__ void __launch_bounds__(4 * ROWS, 256 / ROWS) k_trsv_packed(uint32_t c0, const uint4 *__restrict__ chunk,
                                                         const uint32_t *__restrict__ prow,
                                                         const uint32_t *__restrict__ pfirst,
                                                         const uint32_t *__restrict__ pcol, const T *__restrict__ pk,
-                                                        const double *__restrict__ b, double *x, int *err)
+                                                        const double *__restrict__ b, double *x,
+                                                        const uint32_t *__restrict__ perm, double *xout, int *err)
 {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t mbar;
@@ -1900,13 +1904,14 @@ __global__ void __launch_bounds__(4 * ROWS, 256 / ROWS) k_trsv_packed(uint32_t c
   const uint32_t s = ch.x + (threadIdx.x >> 2);
   const int r = threadIdx.x & 3, base = (threadIdx.x & 31) & ~3;
   const bool active = s < ch.y;
-  uint32_t row = 0, k0 = 0, k1 = 0;
+  uint32_t row = 0, k0 = 0, k1 = 0, node = 0;
   double xi = 0.0;
   if (active) {
     row = __ldg(prow + s);
     k0 = __ldg(pfirst + s) - ch.z;
     k1 = __ldg(pfirst + s + 1) - ch.z;
-    if (!UPPER) xi = b[4 * (size_t)row + r];
+    node = perm ? __ldg(perm + row) : row;
+    if (!UPPER) xi = b[4 * (size_t)node + r];
   }
   __syncthreads();   // the columns and the barrier's initialisation, for every thread
   asm volatile("griddepcontrol.wait;" ::: "memory");
@@ -1956,6 +1961,7 @@ __global__ void __launch_bounds__(4 * ROWS, 256 / ROWS) k_trsv_packed(uint32_t c
     xi = y;
   }
   x[4 * (size_t)row + r] = xi;
+  if (UPPER && xout) xout[4 * (size_t)node + r] = xi;
 }
 
 // ------------------------------------------------------------------ sync-free SpTRSV
@@ -2350,7 +2356,9 @@ static void packed_setup()
 // programmatic dependent launch (the first level of the lower sweep waits for
 // the right-hand side normally).  The chunk cut (32 or 64 rows a CTA) is the
 // one chosen for the factor's precision.
-template <typename T> static void sptrsv_packed(DevMesh &m, const double *b, double *x)
+template <typename T>
+static void sptrsv_packed(DevMesh &m, const double *b, double *x, const uint32_t *perm = nullptr,
+                          double *xout = nullptr)
 {
   packed_setup();
   int *err = m.status + 1;
@@ -2370,8 +2378,10 @@ template <typename T> static void sptrsv_packed(DevMesh &m, const double *b, dou
       if (nc == 0) continue;
       const double *bb = b;
       double *xx = x;
-      void *args[] = {&c0, (void *)&chunk, (void *)&pk.row, (void *)&pk.first, (void *)&pk.col, (void *)&P,
-                      (void *)&bb, (void *)&xx, (void *)&err};
+      const uint32_t *pp = perm;
+      double *xo = xout;
+      void *args[] = {&c0,         (void *)&chunk, (void *)&pk.row, (void *)&pk.first, (void *)&pk.col, (void *)&P,
+                      (void *)&bb, (void *)&xx,    (void *)&pp,     (void *)&xo,       (void *)&err};
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3(nc);
       cfg.blockDim = dim3(cut == 0 ? 128 : 256);
@@ -2387,6 +2397,18 @@ template <typename T> static void sptrsv_packed(DevMesh &m, const double *b, dou
       kf_count_launch();
     }
   }
+}
+
+// x = P^T (LU)^-1 P b for a renumbered pattern (m.row_node) through the
+// packed schedule, the permutations folded into its first and last sweeps;
+// false (nothing done) when the active schedule is not the packed one.
+bool sptrsv_permuted(DevMesh &m, const double *b, double *x, int precision)
+{
+  const int mode = (m.trsv_mode == 8 && precision == 0 && !m.pk_fp64) ? 7 : m.trsv_mode;
+  if (mode != 8 || !m.pk[0].chunk[0] || !m.row_node) return false;
+  if (precision == 0) sptrsv_packed<double>(m, b, m.px, m.row_node, x);
+  else sptrsv_packed<float>(m, b, m.px, m.row_node, x);
+  return true;
 }
 
 void sptrsv(DevMesh &m, const double *b, double *x, int precision)

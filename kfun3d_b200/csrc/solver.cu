@@ -521,7 +521,9 @@ struct Ops {
   void sptrsv(DevMesh &m, const double *b, double *x, int p) const
   {
     if (m.ilu_active) {
-      // spatial ILU(0): x = P^T (LU)^-1 P b
+      // spatial ILU(0): x = P^T (LU)^-1 P b, the permutations folded into the
+      // packed sweeps where that schedule runs
+      if (fast ? kf_fast::sptrsv_permuted(m, b, x, p) : kf_exact::sptrsv_permuted(m, b, x, p)) return;
       const unsigned nb = (m.N + 255) / 256;
       k_rows_permute<<<nb, 256, 0, m.stream>>>(m.N, m.ilu_rank, (const double4 *)b, (double4 *)m.pb, 1);
       fast ? kf_fast::sptrsv(m, m.pb, m.px, p) : kf_exact::sptrsv(m, m.pb, m.px, p);
