@@ -375,6 +375,10 @@ struct DevMesh {
   int graph_ilu = 0;              // ILU set the Arnoldi graphs were captured with
   uint32_t *fill_blk = nullptr, *fill_diag = nullptr, *fill_last = nullptr, *fill_lpos = nullptr;
   uint32_t *row_node = nullptr;   // active set's node of each matrix row (null: the identity)
+  // the state whose visit-order copy qv already holds, written together with
+  // it by its producer; the next visit-order gather of that state is skipped
+  // (one-shot)
+  const double *qv_of = nullptr;
   // flexible GMRES (right preconditioning) and the learned preconditioner
   double *Z = nullptr;            // [30][4N] preconditioned basis vectors
   double *qold = nullptr;         // [4N] state before the last update

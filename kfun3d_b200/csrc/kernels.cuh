@@ -2136,6 +2136,9 @@ int lsq_setup(DevMesh &m)
 static void visit_state(DevMesh &m, const double *q)
 {
   if (!m.visit) return;
+  const bool held = m.qv_of == q;
+  m.qv_of = nullptr;
+  if (held) return;
   k_visit_gather<<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, (const double4 *)q, m.qv);
   kf_count_launch();
 }

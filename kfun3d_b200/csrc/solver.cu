@@ -395,6 +395,27 @@ __global__ void k_jv_shift(size_t n, const double *__restrict__ scal, const doub
   w[i] = fast ? fma(a, x[i], q[i]) : a * x[i] + q[i];
 }
 
+// k_jv_shift over the visit order: w at node ord[p] and its visit-order
+// copy qv[p] in one pass (the same arithmetic)
+__global__ void k_jv_shift_visit(uint32_t N, const uint32_t *__restrict__ ord, const double *__restrict__ scal,
+                                 const double *__restrict__ x, const double *__restrict__ q, double *__restrict__ w,
+                                 double4 *__restrict__ qv, int fast)
+{
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const size_t i = ord[p];
+  const double h = JV_EPS * scal[S_QN];
+  const double a = h / scal[S_XN];
+  const double4 xx = reinterpret_cast<const double4 *>(x)[i], qq = reinterpret_cast<const double4 *>(q)[i];
+  double4 o;
+  o.x = fast ? fma(a, xx.x, qq.x) : a * xx.x + qq.x;
+  o.y = fast ? fma(a, xx.y, qq.y) : a * xx.y + qq.y;
+  o.z = fast ? fma(a, xx.z, qq.z) : a * xx.z + qq.z;
+  o.w = fast ? fma(a, xx.w, qq.w) : a * xx.w + qq.w;
+  reinterpret_cast<double4 *>(w)[i] = o;
+  qv[p] = o;
+}
+
 __global__ void k_set_h(double *scal)
 {
   scal[S_H] = JV_EPS * scal[S_QN];
@@ -577,7 +598,13 @@ void dev_jacvec(DevMesh &m, const Ops &o, const double *x, double *y)
   const size_t n = 4 * (size_t)m.N;
   dev_reduce(m, x, x, m.scal + S_XN, 1, o.fast);
   k_set_h<<<1, 1, 0, m.stream>>>(m.scal);
-  k_jv_shift<<<nblk(n, 256), 256, 0, m.stream>>>(n, m.scal, x, m.q, m.w, o.fast);
+  if (m.visit) {
+    // the shifted state and its visit-order copy in one pass
+    k_jv_shift_visit<<<nblk(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.scal, x, m.q, m.w, m.qv, o.fast);
+    m.qv_of = m.w;
+  } else {
+    k_jv_shift<<<nblk(n, 256), 256, 0, m.stream>>>(n, m.scal, x, m.q, m.w, o.fast);
+  }
   kf_count_launch(2);
   dev_residual(m, o, m.w, y);
   o.jv_combine(m, y, m.r, m.w, m.q);

@@ -106,6 +106,30 @@ def test_exact_solve_meshA_matches_reference_history():
     assert np.array_equal(m.view.q, q)
 
 
+@pytest.mark.parametrize("path", ["meshA", "box12"])
+def test_exact_solve_with_visit_order_copies(box_mesh, path, monkeypatch):
+    """With the node data in a Morton visit order (the residual's visit-order
+    copies, and the matrix-free product forming the shifted state and its
+    visit-order copy in one pass) the exact-mode solve is the mesh order's,
+    step for step and bit for bit."""
+    mesh = MESH_A if path == "meshA" else box_mesh(12, seed=41)
+    kf.set_aoa(3.0 if path == "meshA" else 3.06)
+    out = {}
+    for order in ("natural", "morton"):
+        monkeypatch.setenv("KFUN3D_NODE_ORDER", order)
+        m = kf.Mesh(mesh)
+        assert m.query("visit_order_copies") == (1 if order == "morton" else 0)
+        out[order] = (m.solve(ts_max=4), m.view.q.copy())
+        m.close()
+    (h0, q0), (h1, q1) = out["natural"], out["morton"]
+    assert len(h0) == len(h1)
+    for a, b in zip(h0, h1):
+        for k in ("gmres_its", "cfl", "fnorm", "lift", "drag", "momn"):
+            assert a[k] == b[k], (path, a["step"], k)
+    assert np.array_equal(q0, q1)
+    assert kf.last_status() == 0
+
+
 def test_exact_kernel_entry_point_box(box_mesh):
     """Kernel() (the reference's constants) equals the oracle's solve."""
     kf.set_aoa(3.06)
