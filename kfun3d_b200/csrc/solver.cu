@@ -395,15 +395,15 @@ __global__ void k_jv_shift(size_t n, const double *__restrict__ scal, const doub
   w[i] = fast ? fma(a, x[i], q[i]) : a * x[i] + q[i];
 }
 
-// k_jv_shift over the visit order: w at node ord[p] and its visit-order
-// copy qv[p] in one pass (the same arithmetic)
-__global__ void k_jv_shift_visit(uint32_t N, const uint32_t *__restrict__ ord, const double *__restrict__ scal,
+// k_jv_shift with the visit-order copy of w written alongside: node i's w in
+// the mesh's order (coalesced, like x and q) and at its visit position
+// rowof[i] in qv (the same arithmetic)
+__global__ void k_jv_shift_visit(uint32_t N, const uint32_t *__restrict__ rowof, const double *__restrict__ scal,
                                  const double *__restrict__ x, const double *__restrict__ q, double *__restrict__ w,
                                  double4 *__restrict__ qv, int fast)
 {
-  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= N) return;
-  const size_t i = ord[p];
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
   const double h = JV_EPS * scal[S_QN];
   const double a = h / scal[S_XN];
   const double4 xx = reinterpret_cast<const double4 *>(x)[i], qq = reinterpret_cast<const double4 *>(q)[i];
@@ -413,7 +413,7 @@ __global__ void k_jv_shift_visit(uint32_t N, const uint32_t *__restrict__ ord, c
   o.z = fast ? fma(a, xx.z, qq.z) : a * xx.z + qq.z;
   o.w = fast ? fma(a, xx.w, qq.w) : a * xx.w + qq.w;
   reinterpret_cast<double4 *>(w)[i] = o;
-  qv[p] = o;
+  qv[rowof[i]] = o;
 }
 
 __global__ void k_set_h(double *scal)
@@ -600,7 +600,7 @@ void dev_jacvec(DevMesh &m, const Ops &o, const double *x, double *y)
   k_set_h<<<1, 1, 0, m.stream>>>(m.scal);
   if (m.visit) {
     // the shifted state and its visit-order copy in one pass
-    k_jv_shift_visit<<<nblk(m.N, 256), 256, 0, m.stream>>>(m.N, m.ord, m.scal, x, m.q, m.w, m.qv, o.fast);
+    k_jv_shift_visit<<<nblk(m.N, 256), 256, 0, m.stream>>>(m.N, m.rowof, m.scal, x, m.q, m.w, m.qv, o.fast);
     m.qv_of = m.w;
   } else {
     k_jv_shift<<<nblk(n, 256), 256, 0, m.stream>>>(n, m.scal, x, m.q, m.w, o.fast);
