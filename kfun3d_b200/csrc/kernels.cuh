@@ -1042,46 +1042,39 @@ __global__ void k_fill_boundary(uint32_t nb, const uint32_t *__restrict__ bnd_no
 
 // ------------------------------------------------------------------ ILU(0)
 
-// 4x4 inverse of matrix/inverse.cpp:195-355.
-__device__ void inv4(const double *s, double *dst)
+
+// 4x4 inverse of matrix/inverse.cpp:195-355 by the 16 lanes of a row group
+// (lane l = 4*row + col holds entry l of the block s): lane l forms the
+// cofactor d[l] as that file does, six triple products in its order and with
+// its signs, summed left to right (one table word each: sign bit 15, the
+// three entries in bits 0-3, 4-7 and 8-11, multiplied left to right), then
+// det = s0 d0 + s1 d4 + s2 d8 + s3 d12, det = 1 / det, entry l = d[l] det.
+__device__ const uint16_t kInv4Terms[96] = {0x0fa5u, 0x8eb5u, 0x8f69u, 0x0e79u, 0x0b6du, 0x8a7du, 0x8fa1u, 0x0eb1u, 0x0f29u, 0x8e39u, 0x8b2du, 0x0a3du, 0x0f61u, 0x8e71u, 0x8f25u, 0x0e35u, 0x072du, 0x863du, 0x8b61u, 0x0a71u, 0x0b25u, 0x8a35u, 0x8729u, 0x0639u, 0x8fa4u, 0x0eb4u, 0x0f68u, 0x8e78u, 0x8b6cu, 0x0a7cu, 0x0fa0u, 0x8eb0u, 0x8f28u, 0x0e38u, 0x0b2cu, 0x8a3cu, 0x8f60u, 0x0e70u, 0x0f24u, 0x8e34u, 0x872cu, 0x063cu, 0x0b60u, 0x8a70u, 0x8b24u, 0x0a34u, 0x0728u, 0x8638u, 0x0f94u, 0x8db4u, 0x8f58u, 0x0d78u, 0x0b5cu, 0x897cu, 0x8f90u, 0x0db0u, 0x0f18u, 0x8d38u, 0x8b1cu, 0x093cu, 0x0f50u, 0x8d70u, 0x8f14u, 0x0d34u, 0x071cu, 0x853cu, 0x8b50u, 0x0970u, 0x0b14u, 0x8934u, 0x8718u, 0x0538u, 0x8e94u, 0x0da4u, 0x0e58u, 0x8d68u, 0x8a5cu, 0x096cu, 0x0e90u, 0x8da0u, 0x8e18u, 0x0d28u, 0x0a1cu, 0x892cu, 0x8e50u, 0x0d60u, 0x0e14u, 0x8d24u, 0x861cu, 0x052cu, 0x0a50u, 0x8960u, 0x8a14u, 0x0924u, 0x0618u, 0x8528u};
+
+__device__ __forceinline__ double inv4_lane(double v, int lane16, unsigned mask, int base)
 {
-  double d[16];
-  d[0] = s[5] * s[10] * s[15] - s[5] * s[11] * s[14] - s[9] * s[6] * s[15]
-       + s[9] * s[7] * s[14] + s[13] * s[6] * s[11] - s[13] * s[7] * s[10];
-  d[1] = -s[1] * s[10] * s[15] + s[1] * s[11] * s[14] + s[9] * s[2] * s[15]
-       - s[9] * s[3] * s[14] - s[13] * s[2] * s[11] + s[13] * s[3] * s[10];
-  d[2] = s[1] * s[6] * s[15] - s[1] * s[7] * s[14] - s[5] * s[2] * s[15]
-       + s[5] * s[3] * s[14] + s[13] * s[2] * s[7] - s[13] * s[3] * s[6];
-  d[3] = -s[1] * s[6] * s[11] + s[1] * s[7] * s[10] + s[5] * s[2] * s[11]
-       - s[5] * s[3] * s[10] - s[9] * s[2] * s[7] + s[9] * s[3] * s[6];
-  d[4] = -s[4] * s[10] * s[15] + s[4] * s[11] * s[14] + s[8] * s[6] * s[15]
-       - s[8] * s[7] * s[14] - s[12] * s[6] * s[11] + s[12] * s[7] * s[10];
-  d[5] = s[0] * s[10] * s[15] - s[0] * s[11] * s[14] - s[8] * s[2] * s[15]
-       + s[8] * s[3] * s[14] + s[12] * s[2] * s[11] - s[12] * s[3] * s[10];
-  d[6] = -s[0] * s[6] * s[15] + s[0] * s[7] * s[14] + s[4] * s[2] * s[15]
-       - s[4] * s[3] * s[14] - s[12] * s[2] * s[7] + s[12] * s[3] * s[6];
-  d[7] = s[0] * s[6] * s[11] - s[0] * s[7] * s[10] - s[4] * s[2] * s[11]
-       + s[4] * s[3] * s[10] + s[8] * s[2] * s[7] - s[8] * s[3] * s[6];
-  d[8] = s[4] * s[9] * s[15] - s[4] * s[11] * s[13] - s[8] * s[5] * s[15]
-       + s[8] * s[7] * s[13] + s[12] * s[5] * s[11] - s[12] * s[7] * s[9];
-  d[9] = -s[0] * s[9] * s[15] + s[0] * s[11] * s[13] + s[8] * s[1] * s[15]
-       - s[8] * s[3] * s[13] - s[12] * s[1] * s[11] + s[12] * s[3] * s[9];
-  d[10] = s[0] * s[5] * s[15] - s[0] * s[7] * s[13] - s[4] * s[1] * s[15]
-        + s[4] * s[3] * s[13] + s[12] * s[1] * s[7] - s[12] * s[3] * s[5];
-  d[11] = -s[0] * s[5] * s[11] + s[0] * s[7] * s[9] + s[4] * s[1] * s[11]
-        - s[4] * s[3] * s[9] - s[8] * s[1] * s[7] + s[8] * s[3] * s[5];
-  d[12] = -s[4] * s[9] * s[14] + s[4] * s[10] * s[13] + s[8] * s[5] * s[14]
-        - s[8] * s[6] * s[13] - s[12] * s[5] * s[10] + s[12] * s[6] * s[9];
-  d[13] = s[0] * s[9] * s[14] - s[0] * s[10] * s[13] - s[8] * s[1] * s[14]
-        + s[8] * s[2] * s[13] + s[12] * s[1] * s[10] - s[12] * s[2] * s[9];
-  d[14] = -s[0] * s[5] * s[14] + s[0] * s[6] * s[13] + s[4] * s[1] * s[14]
-        - s[4] * s[2] * s[13] - s[12] * s[1] * s[6] + s[12] * s[2] * s[5];
-  d[15] = s[0] * s[5] * s[10] - s[0] * s[6] * s[9] - s[4] * s[1] * s[10]
-        + s[4] * s[2] * s[9] + s[8] * s[1] * s[6] - s[8] * s[2] * s[5];
-  double det = s[0] * d[0] + s[1] * d[4] + s[2] * d[8] + s[3] * d[12];
-  det = 1.0 / det;
+  double acc = 0.0;
 #pragma unroll
-  for (int k = 0; k < 16; k++) dst[k] = d[k] * det;
+  for (int k = 0; k < 6; k++) {
+    const uint32_t w = kInv4Terms[6 * lane16 + k];
+    const double x = __shfl_sync(mask, v, base + (int)(w & 15u));
+    const double y = __shfl_sync(mask, v, base + (int)((w >> 4) & 15u));
+    const double z = __shfl_sync(mask, v, base + (int)((w >> 8) & 15u));
+    const bool neg = (w >> 15) != 0;
+    if (k == 0) {
+      acc = ((neg ? -x : x) * y) * z;
+    } else {
+      const double p = (x * y) * z;
+      acc = neg ? acc - p : acc + p;
+    }
+  }
+  const double s0 = __shfl_sync(mask, v, base + 0), s1 = __shfl_sync(mask, v, base + 1);
+  const double s2 = __shfl_sync(mask, v, base + 2), s3 = __shfl_sync(mask, v, base + 3);
+  const double d0 = __shfl_sync(mask, acc, base + 0), d4 = __shfl_sync(mask, acc, base + 4);
+  const double d8 = __shfl_sync(mask, acc, base + 8), d12 = __shfl_sync(mask, acc, base + 12);
+  double det = s0 * d0 + s1 * d4 + s2 * d8 + s3 * d12;
+  det = 1.0 / det;
+  return acc * det;
 }
 
 // Product of two 4x4 blocks held one entry per lane of a 16-lane group
@@ -1151,19 +1144,10 @@ __global__ void __launch_bounds__(128) k_ilu_level(uint32_t nrows, const uint32_
     } else {
       A[16 * (size_t)j + l16] = a;
       if (k == i) {
-        __syncwarp(mask);
-        if (l16 == 0) {
-          double s[16], o[16];
-          for (int t = 0; t < 16; t++) s[t] = A[16 * (size_t)j + t];
-          inv4(s, o);
-          bool bad = false;
-          for (int t = 0; t < 16; t++) {
-            dinv[16 * (size_t)i + t] = o[t];
-            bad |= !isfinite(o[t]);
-          }
-          if (bad) atomicExch(status, KFUN3D_ERR_PIVOT);
-        }
-        __syncwarp(mask);
+        // the inverse of the row's diagonal block, entry l on lane l
+        const double inv = inv4_lane((double)a, l16, mask, base);
+        dinv[16 * (size_t)i + l16] = inv;
+        if (__any_sync(mask, !isfinite(inv)) && l16 == 0) atomicExch(status, KFUN3D_ERR_PIVOT);
       }
     }
   }
@@ -1224,19 +1208,10 @@ __global__ void __launch_bounds__(128) k_ilu_level_pairs(uint32_t nrows, const u
     } else {
       A[16 * (size_t)j + l16] = a;
       if (k == i) {
-        __syncwarp(mask);
-        if (l16 == 0) {
-          double s[16], o[16];
-          for (int t = 0; t < 16; t++) s[t] = A[16 * (size_t)j + t];
-          inv4(s, o);
-          bool bad = false;
-          for (int t = 0; t < 16; t++) {
-            dinv[16 * (size_t)i + t] = o[t];
-            bad |= !isfinite(o[t]);
-          }
-          if (bad) atomicExch(status, KFUN3D_ERR_PIVOT);
-        }
-        __syncwarp(mask);
+        // the inverse of the row's diagonal block, entry l on lane l
+        const double inv = inv4_lane((double)a, l16, mask, base);
+        dinv[16 * (size_t)i + l16] = inv;
+        if (__any_sync(mask, !isfinite(inv)) && l16 == 0) atomicExch(status, KFUN3D_ERR_PIVOT);
       }
     }
   }
@@ -1303,19 +1278,10 @@ __global__ void __launch_bounds__(128) k_ilu_level_f32(uint32_t nrows, const uin
     } else {
       A[16 * (size_t)j + l16] = a;
       if (k == i) {
-        __syncwarp(mask);
-        if (l16 == 0) {
-          double s[16], o[16];
-          for (int t = 0; t < 16; t++) s[t] = A[16 * (size_t)j + t];
-          inv4(s, o);
-          bool bad = false;
-          for (int t = 0; t < 16; t++) {
-            dinv[16 * (size_t)i + t] = (float)o[t];
-            bad |= !isfinite(o[t]);
-          }
-          if (bad) atomicExch(status, KFUN3D_ERR_PIVOT);
-        }
-        __syncwarp(mask);
+        // the inverse of the row's diagonal block, entry l on lane l
+        const double inv = inv4_lane((double)a, l16, mask, base);
+        dinv[16 * (size_t)i + l16] = (float)inv;
+        if (__any_sync(mask, !isfinite(inv)) && l16 == 0) atomicExch(status, KFUN3D_ERR_PIVOT);
       }
     }
   }
@@ -1368,19 +1334,10 @@ __global__ void __launch_bounds__(128) k_ilu_level_pairs_f32(uint32_t nrows, con
     } else {
       A[16 * (size_t)j + l16] = a;
       if (k == i) {
-        __syncwarp(mask);
-        if (l16 == 0) {
-          double sd[16], o[16];
-          for (int t = 0; t < 16; t++) sd[t] = A[16 * (size_t)j + t];
-          inv4(sd, o);
-          bool bad = false;
-          for (int t = 0; t < 16; t++) {
-            dinv[16 * (size_t)i + t] = (float)o[t];
-            bad |= !isfinite(o[t]);
-          }
-          if (bad) atomicExch(status, KFUN3D_ERR_PIVOT);
-        }
-        __syncwarp(mask);
+        // the inverse of the row's diagonal block, entry l on lane l
+        const double inv = inv4_lane((double)a, l16, mask, base);
+        dinv[16 * (size_t)i + l16] = (float)inv;
+        if (__any_sync(mask, !isfinite(inv)) && l16 == 0) atomicExch(status, KFUN3D_ERR_PIVOT);
       }
     }
   }
