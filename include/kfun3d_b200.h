@@ -267,6 +267,16 @@ int kfun3d_sptrsv_device_noalloc(const GEOMETRY *g, const double *d_b, double *d
 /* Release the device mirror of g (also done by CXX_Matrix_Delete). */
 void kfun3d_device_release(GEOMETRY *g);
 
+/* Self-check of the device-side bounded waits, without a fault: one thread
+   waits, the way the sync-free triangular sweep waits for a row, on a flag
+   that nothing sets, and must give up after the library's poll limit (about
+   a second at most); a second wait on a flag that is set must return at once,
+   in the same context.  Returns KFUN3D_ERR_TIMEOUT when both behave so,
+   KFUN3D_ERR_ARG when either does not, KFUN3D_ERR_CUDA / _NO_DEVICE on a
+   CUDA failure or without a device.  For tests and bring-up; no counterpart
+   in the reference. */
+int kfun3d_check_bounded_wait(void);
+
 /* Which device paths g's mirror uses (for tests and reports; builds the
    mirror on first use): key "sptrsv_schedule" -> the triangular-solve
    schedule of the active ILU(0) order (8 packed level launches, 7 four-lane

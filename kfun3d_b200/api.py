@@ -103,6 +103,7 @@ def lib():
         "kfun3d_launch_count": (C.c_ulonglong, []),
         "kfun3d_reset_launch_count": (None, []),
         "kfun3d_device_release": (None, [G]),
+        "kfun3d_check_bounded_wait": (C.c_int, []),
         "kfun3d_device_query": (C.c_long, [G, C.c_char_p]),
         "kfun3d_matrix_read": (C.c_long, [G, P(C.c_uint), P(C.c_uint), D]),
         "kfun3d_time_solve": (C.c_double, [G, P(SolverParams), C.c_int, P(Step), C.c_int, P(C.c_int)]),

@@ -404,6 +404,7 @@ void kfun3d_reset_launch_count_by(unsigned long long n);   // undo counts taken 
 #define KF_DECLARE_KERNELS(NS)                                                          \
   namespace NS {                                                                        \
   void gradient(DevMesh &m, const double *q);                                           \
+  int bounded_wait_check(cudaStream_t st);                                              \
   void residual(DevMesh &m, const double *q, double *r, int first_order, double u, double v); \
   void timestep(DevMesh &m, const double *q, double cfl);                               \
   void fill(DevMesh &m, const double *q, double u, double v, int precision);            \

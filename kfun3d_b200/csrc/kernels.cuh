@@ -2312,6 +2312,17 @@ static void packed_setup()
   done = true;
 }
 
+// The bounded wait of the sync-free sweep on a flag nothing sets: gives up
+// after KF_SPIN_LIMIT polls and records that in *err (bounded_wait_check).
+__global__ void k_wait_on_flag(const uint32_t *flag, uint32_t value, int *err)
+{
+  if (threadIdx.x != 0) return;
+  uint32_t spins = 0;
+  while (ld_acquire(flag) != value) {
+    if (++spins > KF_SPIN_LIMIT) { atomicExch(err, 1); return; }
+  }
+}
+
 // Both sweeps of the packed schedule: one launch per level, chained by
 // programmatic dependent launch (the first level of the lower sweep waits for
 // the right-hand side normally).  The chunk cut (32 or 64 rows a CTA) is the
@@ -2369,6 +2380,36 @@ bool sptrsv_permuted(DevMesh &m, const double *b, double *x, int precision)
   if (precision == 0) sptrsv_packed<double>(m, b, m.px, m.row_node, x);
   else sptrsv_packed<float>(m, b, m.px, m.row_node, x);
   return true;
+}
+
+// The device-side bounded waits at work without a fault: a wait on a flag
+// that nothing sets must give up (KFUN3D_ERR_TIMEOUT), and the same wait on a
+// set flag must return at once, in the same context.  Anything else is an
+// error code (KFUN3D_ERR_CUDA for a CUDA failure, KFUN3D_ERR_ARG if either
+// wait behaved otherwise).
+int bounded_wait_check(cudaStream_t st)
+{
+  uint32_t *flag = nullptr;
+  int *err = nullptr;
+  int h[2] = {0, 0};
+  bool ok = cudaMalloc(&flag, sizeof(uint32_t)) == cudaSuccess && cudaMalloc(&err, 2 * sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMemsetAsync(flag, 0, sizeof(uint32_t), st) == cudaSuccess &&
+       cudaMemsetAsync(err, 0, 2 * sizeof(int), st) == cudaSuccess;
+  if (ok) {
+    k_wait_on_flag<<<1, 32, 0, st>>>(flag, 1u, err);       // nothing sets it: gives up
+    k_wait_on_flag<<<1, 32, 0, st>>>(flag, 0u, err + 1);   // already set: returns at once
+    kf_count_launch(2);
+    ok = cudaGetLastError() == cudaSuccess &&
+         cudaMemcpyAsync(h, err, 2 * sizeof(int), cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+         cudaStreamSynchronize(st) == cudaSuccess;
+  }
+  if (flag) cudaFree(flag);
+  if (err) cudaFree(err);
+  if (!ok) {
+    cudaGetLastError();
+    return KFUN3D_ERR_CUDA;
+  }
+  return (h[0] == 1 && h[1] == 0) ? KFUN3D_ERR_TIMEOUT : KFUN3D_ERR_ARG;
 }
 
 void sptrsv(DevMesh &m, const double *b, double *x, int precision)

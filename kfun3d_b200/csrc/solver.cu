@@ -1575,6 +1575,17 @@ extern "C" double kfun3d_time_kernel(GEOMETRY *g, int which, int reps)
   return (double)ms / reps;
 }
 
+extern "C" int kfun3d_check_bounded_wait(void)
+{
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    kf_set_error(KFUN3D_ERR_NO_DEVICE, "no CUDA device");
+    return KFUN3D_ERR_NO_DEVICE;
+  }
+  return kf_fast::bounded_wait_check(0);
+}
+
 extern "C" long kfun3d_matrix_read(const GEOMETRY *g, unsigned int *ia, unsigned int *ja, double *blocks)
 {
   MatrixHandle *h = kf_handle(g);
