@@ -1132,6 +1132,7 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
       }
       int k = 0;
       while (k < restart) {
+        bool stepped = false;   // the step ran as a captured graph (its Gram-Schmidt and read-back too)
         if (step_net && cycle == 0 && k == 0) {
           // the network earns this solve on its first direction: both
           // candidates, z = v0 and the network's z, are mapped by
@@ -1176,18 +1177,28 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
           usez[k] = true;
           S.learned_its++;
         } else {
-          dev_jacvec(m, o, Vb(m, k), m.t);                             // src/kernel.c:123-130
-          o.sptrsv(m, m.t, Vb(m, k + 1), prec);
+          const bool pair = ps && ps->stride < 0 && (k % -ps->stride) == 0 && ps->count < ps->cap;
           usez[k] = false;
-          if (ps && ps->stride < 0 && (k % -ps->stride) == 0 && ps->count < ps->cap) {
-            // basis pair: x = v_k, y = ILU(0)^-1 J v_k (before Gram-Schmidt)
-            kf_mpnn_pair_async(m.N, Vb(m, k + 1), m.q, Vb(m, k), ps->x0 + (size_t)ps->count * 16 * m.N,
-                               ps->tgt + (size_t)ps->count * 4 * m.N, m.pscr, m.stream);
-            ps->count++;
+          if (o.fast && m.use_graphs && !pair) {
+            // without the network the step is the plain Arnoldi step: its
+            // captured graph (Gram-Schmidt and the column's read-back included)
+            arnoldi_step_graph(m, o, k, prec);
+            stepped = true;
+          } else {
+            dev_jacvec(m, o, Vb(m, k), m.t);                             // src/kernel.c:123-130
+            o.sptrsv(m, m.t, Vb(m, k + 1), prec);
+            if (pair) {
+              // basis pair: x = v_k, y = ILU(0)^-1 J v_k (before Gram-Schmidt)
+              kf_mpnn_pair_async(m.N, Vb(m, k + 1), m.q, Vb(m, k), ps->x0 + (size_t)ps->count * 16 * m.N,
+                                 ps->tgt + (size_t)ps->count * 4 * m.N, m.pscr, m.stream);
+              ps->count++;
+            }
           }
         }
-        orthogonalize(m, o, k);
-        fetch(m, 0, k + 2);
+        if (!stepped) {
+          orthogonalize(m, o, k);
+          fetch(m, 0, k + 2);
+        }
         double *hh = ghh + k * (KF_NBASIS + 1);
         for (int i = 0; i <= k + 1; i++) hh[i] = m.h_scal[i];
         const double res = givens(hh, cs, sn, rs, k);
