@@ -367,6 +367,21 @@ __global__ void k_axpy(size_t n, double a, const double *__restrict__ x, double 
   y[i] = fast ? fma(a, x[i], y[i]) : a * x[i] + y[i];
 }
 
+// y = a[0] v[0] + y, then a[1] v[1] + y, ... (k_axpy's arithmetic, vector
+// after vector in that order) in one pass: y and every v read once
+struct AxpyList {
+  const double *v[KF_NBASIS];
+  double a[KF_NBASIS];
+};
+__global__ void k_axpy_multi(size_t n, int k, AxpyList L, double *__restrict__ y, int fast)
+{
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double acc = y[i];
+  for (int v = 0; v < k; v++) acc = fast ? fma(L.a[v], L.v[v][i], acc) : L.a[v] * L.v[v][i] + acc;
+  y[i] = acc;
+}
+
 // w = a x + y (src/utils.c:89-107)
 __global__ void k_waxpy(size_t n, double a, const double *__restrict__ x, const double *__restrict__ y,
                         double *__restrict__ w, int fast)
@@ -618,6 +633,18 @@ void dev_axpy(DevMesh &m, double a, const double *x, double *y, bool fast)
 }
 
 double *Vb(DevMesh &m, int k) { return m.V + (size_t)k * 4 * m.N; }
+
+// y += sum over v < k of a[v] x[v], one launch (the sum of k dev_axpy calls,
+// in their order)
+void dev_axpy_multi(DevMesh &m, int k, const double *a, const double *const *x, double *y, bool fast)
+{
+  if (k <= 0) return;
+  const size_t n = 4 * (size_t)m.N;
+  AxpyList L{};
+  for (int v = 0; v < k && v < KF_NBASIS; v++) { L.v[v] = x[v]; L.a[v] = a[v]; }
+  k_axpy_multi<<<nblk(n, 256), 256, 0, m.stream>>>(n, std::min(k, (int)KF_NBASIS), L, y, fast);
+  kf_count_launch();
+}
 
 void dev_normalize(DevMesh &m, double *x, double *nrm, bool fast)
 {
@@ -898,7 +925,11 @@ static int solve_device(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_param
         for (int j = mm + 1; j <= k - 1; j++) tt -= ghh[j * (KF_NBASIS + 1) + mm] * rs[j];
         rs[mm] = tt / ghh[mm * (KF_NBASIS + 1) + mm];
       }
-      for (int vv = 0; vv < k; vv++) dev_axpy(m, rs[vv], Vb(m, vv), m.x, o.fast);
+      {
+        const double *vs[KF_NBASIS];
+        for (int vv = 0; vv < k; vv++) vs[vv] = Vb(m, vv);
+        dev_axpy_multi(m, k, rs, vs, m.x, o.fast);
+      }
       if (print && k == restart) fun3d_printf(5, ">> GMRES: COMPLETED ONE CYCLE\n");
       if (done) break;
     }
@@ -1221,14 +1252,22 @@ static int solve_flexible(DevMesh &m, const GEOMETRY *g, const kfun3d_solver_par
         if (ps && ps->stride > 0 && cycle == 0 && k < restart && (k % ps->stride) == 0 && ps->count < ps->cap) {
           back_substitute(ghh, rs, k, yk);
           CK(cudaMemsetAsync(m.fx, 0, n * sizeof(double), m.stream));
-          for (int vv = 0; vv < k; vv++) dev_axpy(m, yk[vv], Vb(m, vv), m.fx, o.fast);
+          {
+            const double *vs[KF_NBASIS];
+            for (int vv = 0; vv < k; vv++) vs[vv] = Vb(m, vv);
+            dev_axpy_multi(m, k, yk, vs, m.fx, o.fast);
+          }
           write_pair(m, o, prec, m.fx, *ps);
         }
       }
       if (failed || k == 0) break;
       total += k;
       back_substitute(ghh, rs, k, yk);                                  // src/kernel.c:178-190
-      for (int vv = 0; vv < k; vv++) dev_axpy(m, yk[vv], usez[vv] ? Zb(m, vv) : Vb(m, vv), m.x, o.fast);
+      {
+        const double *vs[KF_NBASIS];
+        for (int vv = 0; vv < k; vv++) vs[vv] = usez[vv] ? Zb(m, vv) : Vb(m, vv);
+        dev_axpy_multi(m, k, yk, vs, m.x, o.fast);
+      }
       if (done) break;
     }
     if (failed || !done) {
