@@ -163,6 +163,24 @@ long kfun3d_ilu_rank(const GEOMETRY *g, unsigned int *rank);
    renumbered pattern (may be NULL).  Returns 0, or -1 on bad arguments. */
 int kfun3d_ilu_order_plan(const GEOMETRY *g, unsigned int tiles, unsigned int *rank, unsigned int *nlev_lower,
                           unsigned int *nlev_upper);
+/* Additive Schwarz preconditioner without overlap (the "Schwarz" of
+   Newton-Krylov-Schwarz: PETSc's -pc_type asm -sub_pc_type ilu in
+   archive/base2/incomp/petsc.opt, the reference's partition being METIS's,
+   matrix/matrix.cpp:99-135), on one device: with parts > 1 the nodes are cut
+   into `parts` subdomains by recursive coordinate bisection
+   (kfun3d_schwarz_partition) and every Jacobian block that couples two
+   subdomains is removed before ILU(0), which then factors each subdomain on
+   its own (block-Jacobi ILU(0) in the active elimination order; the
+   triangular solves are the subdomains' own).  What one GPU per subdomain
+   would compute, without the halo exchange and the reductions across GPUs.
+   0 or 1: off (default).  Applied at the next factorisation; changes the
+   iteration counts, not the Jacobian-vector products. */
+void kfun3d_set_schwarz(unsigned int parts);
+unsigned int kfun3d_get_schwarz(void);
+/* Host only (no GPU needed): part[node] (N entries) of the `parts`
+   subdomains kfun3d_set_schwarz(parts) uses.  Returns 0, or -1 on bad
+   arguments. */
+int kfun3d_schwarz_partition(const GEOMETRY *g, unsigned int parts, unsigned int *part);
 /* 1: residual reconstructed without gradients (first-order flux). */
 void kfun3d_set_first_order(int on);
 /* 0 silences Kernel()'s per-step report. */

@@ -10,7 +10,7 @@ fails loudly when the library has not been built; there is no CPU fallback.
 """
 from .api import (  # noqa: F401
     KFUN3D_MODE_EXACT, KFUN3D_MODE_FAST, Mesh, SolverParams, Step, generate_mesh, lib,
-    set_aoa, get_aoa, freestream, set_mode, get_mode, set_precision, set_ilu_order, get_ilu_order,
+    set_aoa, get_aoa, freestream, set_mode, get_mode, set_precision, set_ilu_order, get_ilu_order, set_schwarz, get_schwarz,
     set_first_order,
     set_verbose, last_status, last_error, clear_status, set_abort_on_error,
     launch_count, reset_launch_count, LIB_PATH,

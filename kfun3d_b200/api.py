@@ -91,6 +91,9 @@ def lib():
         "kfun3d_ilu_rank": (C.c_long, [G, C.POINTER(C.c_uint)]),
         "kfun3d_ilu_order_plan": (C.c_int, [G, C.c_uint, C.POINTER(C.c_uint), C.POINTER(C.c_uint),
                                             C.POINTER(C.c_uint)]),
+        "kfun3d_set_schwarz": (None, [C.c_uint]),
+        "kfun3d_get_schwarz": (C.c_uint, []),
+        "kfun3d_schwarz_partition": (C.c_int, [G, C.c_uint, C.POINTER(C.c_uint)]),
         "kfun3d_set_first_order": (None, [C.c_int]),
         "kfun3d_set_verbose": (None, [C.c_int]),
         "kfun3d_default_params": (None, [P(SolverParams)]),
@@ -188,6 +191,16 @@ def set_ilu_order(order):
 
 def get_ilu_order():
     return lib().kfun3d_get_ilu_order()
+
+
+def set_schwarz(parts):
+    """Additive Schwarz without overlap on one device: ILU(0) of each of `parts`
+    subdomains (recursive coordinate bisection) on its own; 0 or 1 turns it off."""
+    lib().kfun3d_set_schwarz(int(parts))
+
+
+def get_schwarz():
+    return lib().kfun3d_get_schwarz()
 
 
 def set_first_order(on):
@@ -332,6 +345,13 @@ class Mesh:
         if lib().kfun3d_ilu_rank(self.g, rank.ctypes.data_as(C.POINTER(C.c_uint))) < 0:
             raise RuntimeError(f"kfun3d_ilu_rank failed: {last_error()}")
         return rank.astype(np.int64)
+
+    def schwarz_partition(self, parts):
+        """Host-only: subdomain of every node for `parts` additive Schwarz subdomains."""
+        part = np.zeros(self.view.nnodes, dtype=np.uint32)
+        if lib().kfun3d_schwarz_partition(self.g, int(parts), part.ctypes.data_as(C.POINTER(C.c_uint))) != 0:
+            raise RuntimeError(f"kfun3d_schwarz_partition failed: {last_error()}")
+        return part.astype(np.int64)
 
     def ilu_order_plan(self, tiles=148):
         """Host-only preview of the spatial ILU(0) order (no GPU): (rank, levels of the

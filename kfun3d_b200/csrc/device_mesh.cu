@@ -27,6 +27,7 @@ int g_mode = KFUN3D_MODE_EXACT;
 int g_precision = 0;
 int g_ilu_order = 0;
 int g_first_order = 0;
+unsigned g_schwarz = 0;
 std::atomic<unsigned long long> g_launches{0};
 }  // namespace
 
@@ -52,6 +53,7 @@ int kf_mode() { return g_mode; }
 int kf_precision() { return g_precision; }
 int kf_ilu_order() { return g_ilu_order; }
 int kf_first_order() { return g_first_order; }
+unsigned kf_schwarz() { return g_schwarz; }
 void kf_count_launch(unsigned n) { g_launches += n; }
 void kfun3d_reset_launch_count_by(unsigned long long n) { g_launches -= n; }
 
@@ -80,6 +82,8 @@ void kfun3d_set_precision(int p) { g_precision = p ? 1 : 0; }
 void kfun3d_set_ilu_order(int o) { g_ilu_order = o ? 1 : 0; }
 int kfun3d_get_ilu_order(void) { return g_ilu_order; }
 void kfun3d_set_first_order(int on) { g_first_order = on ? 1 : 0; }
+void kfun3d_set_schwarz(unsigned int parts) { g_schwarz = parts > 1 ? parts : 0; }
+unsigned int kfun3d_get_schwarz(void) { return g_schwarz; }
 void kfun3d_set_verbose(int on) { g_kf_verbose = on; }
 unsigned long long kfun3d_launch_count(void) { return g_launches; }
 void kfun3d_reset_launch_count(void) { g_launches = 0; }
@@ -429,7 +433,7 @@ static void release_device(MatrixHandle *h)
                   m->diag, m->tblk, m->lpos, m->last_lower, m->lev_l, m->lev_u, m->A, m->lslot, m->dinv,
                   m->Af, m->dinvf, m->q, m->r, m->gx, m->gy, m->gz, m->cdt, m->w, m->t, m->x, m->rhs, m->V,
                   m->red, m->scal, m->forces, m->dscr, m->status, m->flags, m->ticket, m->part, m->lsq_coef,
-                  m->qv, m->xyzv, m->gxv, m->gyv, m->gzv, m->inc_othv, m->n0v, m->n1v, m->inc_geo, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->n0s, m->pair_ptr, m->pairs, m->lev_ptr_d, m->bar, m->Z, m->qold, m->fy, m->fx, m->pscr, m->ord, m->rowof, m->egeo_s};
+                  m->qv, m->xyzv, m->gxv, m->gyv, m->gzv, m->inc_othv, m->n0v, m->n1v, m->inc_geo, m->desc_l, m->desc_u, m->eoff, m->n1, m->in1_ptr, m->in1_edge, m->eres, m->n0s, m->pair_ptr, m->pairs, m->lev_ptr_d, m->bar, m->Z, m->qold, m->fy, m->fx, m->pscr, m->ord, m->rowof, m->egeo_s, m->sub_part};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (m->h_scal) cudaFreeHost(m->h_scal);

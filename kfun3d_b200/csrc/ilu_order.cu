@@ -403,3 +403,81 @@ extern "C" int kfun3d_ilu_order_plan(const GEOMETRY *g, unsigned int tiles, unsi
   }
   return 0;
 }
+
+// ----------------------------------------------------------------- additive Schwarz subdomains
+
+// The nodes cut into `parts` subdomains by recursive coordinate bisection: a
+// set of nodes going to p parts is split across the longest side of its
+// bounding box into floor(p/2) and p - floor(p/2) parts, the first holding
+// floor(n * floor(p/2) / p) of its n nodes (those lowest in that coordinate,
+// ties by node index), so part sizes differ by at most one node per level of
+// the recursion.  The reference partitions its mesh with METIS
+// (matrix/matrix.cpp:99-135, src/subdomains.c:118-122) for its threads; a
+// geometric cut serves the same purpose here without the library.
+std::vector<uint32_t> kf_partition_rcb(const double *X, const double *Y, const double *Z, size_t N, uint32_t parts)
+{
+  std::vector<uint32_t> part(N, 0);
+  if (parts <= 1 || N == 0) return part;
+  std::vector<uint32_t> idx(N);
+  for (size_t i = 0; i < N; i++) idx[i] = (uint32_t)i;
+  const double *C[3] = {X, Y, Z};
+  auto split = [&](auto &&self, size_t a, size_t b, uint32_t p0, uint32_t np) -> void {
+    if (np <= 1 || b - a <= 1) {
+      for (size_t q = a; q < b; q++) part[idx[q]] = p0;
+      return;
+    }
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (size_t q = a; q < b; q++)
+      for (int d = 0; d < 3; d++) {
+        lo[d] = std::min(lo[d], C[d][idx[q]]);
+        hi[d] = std::max(hi[d], C[d][idx[q]]);
+      }
+    int ax = 0;
+    for (int d = 1; d < 3; d++)
+      if (hi[d] - lo[d] > hi[ax] - lo[ax]) ax = d;
+    const uint32_t nl = np / 2;
+    const size_t cut = a + (size_t)((unsigned long long)(b - a) * nl / np);
+    const double *c = C[ax];
+    std::nth_element(idx.begin() + a, idx.begin() + cut, idx.begin() + b,
+                     [c](uint32_t u, uint32_t v) { return c[u] < c[v] || (!(c[v] < c[u]) && u < v); });
+    self(self, a, cut, p0, nl);
+    self(self, cut, b, p0 + nl, np - nl);
+  };
+  split(split, 0, N, 0, parts);
+  return part;
+}
+
+int kf_schwarz_select(DevMesh &m, const GEOMETRY *g, unsigned parts)
+{
+  if (parts <= 1) {
+    if (m.sub_parts) m.factored = false;
+    m.sub_parts = 0;
+    return KFUN3D_OK;
+  }
+  if (parts == m.sub_parts) return KFUN3D_OK;
+  if (!g || !g->n || !g->n->xyz) {
+    kf_set_error(KFUN3D_ERR_ARG, "additive Schwarz: the GEOMETRY has no node coordinates");
+    return KFUN3D_ERR_ARG;
+  }
+  const std::vector<uint32_t> part = kf_partition_rcb(g->n->xyz->x0, g->n->xyz->x1, g->n->xyz->x2, m.N, parts);
+  if ((!m.sub_part && cudaMalloc(&m.sub_part, (size_t)m.N * sizeof(uint32_t)) != cudaSuccess) ||
+      cudaMemcpy(m.sub_part, part.data(), (size_t)m.N * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess) {
+    kf_set_error(KFUN3D_ERR_CUDA, "additive Schwarz: uploading the subdomains failed");
+    return KFUN3D_ERR_CUDA;
+  }
+  m.sub_parts = parts;
+  m.factored = false;
+  return KFUN3D_OK;
+}
+
+extern "C" int kfun3d_schwarz_partition(const GEOMETRY *g, unsigned int parts, unsigned int *part)
+{
+  if (!g || !g->n || !g->n->xyz || !part || parts < 1) {
+    kf_set_error(KFUN3D_ERR_ARG, "kfun3d_schwarz_partition: bad arguments");
+    return -1;
+  }
+  const std::vector<uint32_t> p = kf_partition_rcb(g->n->xyz->x0, g->n->xyz->x1, g->n->xyz->x2, g->n->sz, parts);
+  std::copy(p.begin(), p.end(), part);
+  return 0;
+}

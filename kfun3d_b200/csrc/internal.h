@@ -375,6 +375,10 @@ struct DevMesh {
   int graph_ilu = 0;              // ILU set the Arnoldi graphs were captured with
   uint32_t *fill_blk = nullptr, *fill_diag = nullptr, *fill_last = nullptr, *fill_lpos = nullptr;
   uint32_t *row_node = nullptr;   // active set's node of each matrix row (null: the identity)
+  // additive Schwarz subdomains (kfun3d_set_schwarz): sub_part[node] for
+  // sub_parts subdomains; 0 parts: the whole mesh is one domain
+  uint32_t *sub_part = nullptr;
+  uint32_t sub_parts = 0;
   // the state whose visit-order copy qv already holds, written together with
   // it by its producer; the next visit-order gather of that state is skipped
   // (one-shot)
@@ -396,6 +400,12 @@ int kf_ilu_order();
 // Makes the ILU(0) ordering `order` (0 the mesh's numbering, 1 spatial) the
 // active one, building set 1 on first use; KFUN3D_OK or an error code.
 int kf_ilu_select(DevMesh &m, const GEOMETRY *g, int order);
+unsigned kf_schwarz();
+// Makes `parts` additive Schwarz subdomains (0 or 1: none) the mesh's
+// current ones, computing and uploading the partition on a change.
+int kf_schwarz_select(DevMesh &m, const GEOMETRY *g, unsigned parts);
+// Recursive coordinate bisection of the nodes into `parts` subdomains.
+std::vector<uint32_t> kf_partition_rcb(const double *X, const double *Y, const double *Z, size_t N, uint32_t parts);
 
 void kf_count_launch(unsigned n = 1);
 void kfun3d_reset_launch_count_by(unsigned long long n);   // undo counts taken during graph capture

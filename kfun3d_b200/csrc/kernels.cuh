@@ -1343,6 +1343,32 @@ __global__ void __launch_bounds__(128) k_ilu_level_pairs_f32(uint32_t nrows, con
   }
 }
 
+// Additive Schwarz without overlap on one device: every block that couples
+// two subdomains (row and column nodes in different parts) is set to zero
+// before the factorisation.  ILU(0) then keeps those blocks exactly zero
+// (each of their products has a factor in another such block, and the
+// reference's last product is subtracted and added back: (0 - d) + d = 0),
+// so the factor is block-Jacobi ILU(0), one independent factor per
+// subdomain in the active elimination order, and the triangular solves are
+// the subdomains' own.  One thread per row; row_node maps a row of the
+// active numbering to its mesh node (null: the identity).
+template <typename T>
+__global__ void k_drop_coupling(uint32_t N, const uint32_t *__restrict__ ia, const uint32_t *__restrict__ ja,
+                                const uint32_t *__restrict__ row_node, const uint32_t *__restrict__ part,
+                                T *__restrict__ A)
+{
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const uint32_t pi = part[row_node ? row_node[i] : i];
+  for (uint32_t j = ia[i]; j < ia[i + 1]; j++) {
+    const uint32_t k = ja[j];
+    if (part[row_node ? row_node[k] : k] == pi) continue;
+    T *blk = A + 16 * (size_t)j;
+#pragma unroll
+    for (int e = 0; e < 16; e++) blk[e] = T(0);
+  }
+}
+
 __global__ void k_ilu_finish_f32(uint32_t N, const uint32_t *__restrict__ diag, const float *__restrict__ dinv,
                                  float *__restrict__ A)
 {
@@ -2252,6 +2278,13 @@ static void packed_setup();
 void ilu(DevMesh &m, int precision)
 {
   int *status = m.status;
+  if (m.sub_parts > 1 && m.sub_part) {
+    if (precision == 0)
+      k_drop_coupling<double><<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ia, m.ja, m.row_node, m.sub_part, m.A);
+    else
+      k_drop_coupling<float><<<blocks(m.N, 256), 256, 0, m.stream>>>(m.N, m.ia, m.ja, m.row_node, m.sub_part, m.Af);
+    kf_count_launch();
+  }
   for (uint32_t l = 0; l < m.nlev_l; l++) {
     const uint32_t r0 = m.lev_l_ptr[l], nr = m.lev_l_ptr[l + 1] - r0;
     if (precision == 0 && m.pairs)

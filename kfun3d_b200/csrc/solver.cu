@@ -1328,6 +1328,7 @@ DevMesh *dev_or_fail(const GEOMETRY *g)
 {
   DevMesh *m = kf_device(g);
   if (m && kf_ilu_select(*m, g, kf_ilu_order()) != KFUN3D_OK) return nullptr;
+  if (m && kf_schwarz_select(*m, g, kf_schwarz()) != KFUN3D_OK) return nullptr;
   return m;
 }
 

@@ -139,6 +139,13 @@ class Matrix:
     def blocks_f32(self):
         return np.ctypeslib.as_array(self.m.contents.af, shape=(self.nnz * 16,)).copy().reshape(-1, 4, 4)
 
+    def drop_coupling(self, cross):
+        """Set to zero the blocks flagged in `cross` (one flag per block of the
+        pattern), in place: the matrix an additive Schwarz preconditioner
+        without overlap factors."""
+        a = np.ctypeslib.as_array(self.m.contents.a, shape=(self.nnz * 16,)).reshape(-1, 16)
+        a[np.asarray(cross, dtype=bool)] = 0.0
+
     def fill(self, aoa, q, cdt):
         q = np.ascontiguousarray(q, dtype=np.float64)
         cdt = np.ascontiguousarray(cdt, dtype=np.float64)
